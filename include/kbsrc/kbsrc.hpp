@@ -1,0 +1,47 @@
+// KBSRC on B200 - Kaiser-Bessel sample-rate converter, public C++ API.
+//
+// Same API as HongYue1/KBSRC 1.3.0 include/kbsrc/kbsrc.hpp:8-45 (Precision, Options, Stats, resample,
+// version), so code written against the reference library builds unchanged. The block engine runs on the
+// GPU (sm_100a); its output is byte-identical to the reference CPU engines for Fast and Exact.
+#pragma once
+
+#include <vector>
+
+namespace kbsrc {
+
+enum class Precision {
+    Fast,        // float64 pipeline
+    Exact,       // double-double (~106-bit) pipeline
+    LongDouble,  // x87 80-bit in the reference; rejected here (the GPU has no 80-bit type)
+};
+
+struct Options {
+    Precision precision = Precision::Exact;
+    double length = 0.2;    // one-sided kernel length, seconds; the transition band is inversely proportional
+    double beta = 40.0;     // Kaiser window beta
+    int threads = 0;        // host threads for kernel design and LPC, 0 = automatic
+    int block = 0;          // block size factor, 0 = automatic
+    bool lpc_edges = true;  // Burg LPC extrapolation at the signal edges
+};
+
+struct Stats {
+    long long p = 0, q = 0;     // rate ratio P/Q
+    long long taps = 0;         // kernel taps at the kernel rate
+    int block = 0, threads = 0;
+    bool general_fold = false;  // near-unity ratio path
+    double design_seconds = 0, process_seconds = 0;
+    double passband = 0, stopband = 0;  // band edges in Hz
+    const char* isa = "";       // engine used: "sm_100a" (GPU), "generic" for the equal-rate copy
+};
+
+// Resamples interleaved input (frames x channels) from rate_in to rate_out and returns planar output, one
+// vector per channel of ceil(frames * rate_out / rate_in) samples. Throws std::invalid_argument on bad
+// arguments (same messages as the reference) and std::runtime_error when the GPU engine cannot run the plan.
+// Exact computes in round-to-nearest whatever the caller's mode, which is restored on return or throw.
+std::vector<std::vector<double>> resample(const double* interleaved, long long frames, int channels,
+                                          int rate_in, int rate_out, const Options& options = {},
+                                          Stats* stats = nullptr);
+
+const char* version();
+
+}  // namespace kbsrc

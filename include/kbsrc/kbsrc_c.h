@@ -1,0 +1,67 @@
+/* C form of kbsrc::resample (include/kbsrc/kbsrc.hpp), for FFI callers (ctypes, cgo, JNI).
+ * The reference (HongYue1/KBSRC 1.3.0) has only the C++ entry include/kbsrc/kbsrc.hpp:41-45; this wraps it
+ * with plain pointers and sizes. Nothing throws across it. */
+#ifndef KBSRC_C_H
+#define KBSRC_C_H
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct {
+    int precision; /* 0 fast, 1 exact (2 long double: rejected) */
+    double length; /* one-sided kernel length, seconds (reference default 0.2) */
+    double beta;   /* Kaiser beta (default 40) */
+    int threads;   /* host threads, 0 = automatic */
+    int block;     /* block size factor, 0 = automatic */
+    int lpc_edges; /* nonzero: Burg LPC edges (default) */
+} kbsrc_options_c;
+
+typedef struct {
+    long long p, q, taps;
+    int block, threads, general_fold;
+    double design_seconds, process_seconds, passband, stopband;
+    const char* isa;
+} kbsrc_stats_c;
+
+/* Output frames per channel for a conversion: ceil(frames * P / Q), or -1 on bad arguments. */
+long long kbsrc_output_frames(long long frames, int rate_in, int rate_out);
+
+/* Converts. out: planar, channels * out_cap doubles (out[c*out_cap + i]). Returns the output frames per
+ * channel (>= 0), or -1 invalid argument, -2 out_cap too small, -3 runtime (GPU) error, -4 out of memory;
+ * err (if not NULL) receives the message. */
+long long kbsrc_resample_c(const double* in, long long frames, int channels, int rate_in, int rate_out,
+                           const kbsrc_options_c* opt, double* out, long long out_cap, kbsrc_stats_c* stats,
+                           char* err, int err_len);
+
+const char* kbsrc_version_c(void);
+
+/* A planned conversion: block plan, LPC edges and the GPU engine with the kernel spectrum, built once for
+ * input of one shape (frames, channels, rates, options) and run any number of times on such input. */
+typedef struct kbsrc_conversion kbsrc_conversion;
+struct kbsrc_gpu_engine;
+
+/* Plans a conversion for `in` (its edges feed the LPC prediction). Returns 0, or -1 invalid argument,
+ * -3 runtime (GPU) error, -4 out of memory. */
+int kbsrc_prepare_c(const double* in, long long frames, int channels, int rate_in, int rate_out,
+                    const kbsrc_options_c* opt, kbsrc_conversion** out, char* err, int err_len);
+/* Runs it: in as given to kbsrc_prepare_c (interleaved), out planar channels * nout. */
+int kbsrc_conversion_run_c(kbsrc_conversion* cv, const double* in, double* out, char* err, int err_len);
+/* Output frames, LPC edge arrays (channels * edge_len each) and the engine (NULL for equal rates). */
+int kbsrc_conversion_info_c(const kbsrc_conversion* cv, long long* nout, long long* edge_len, const double** head,
+                            const double** tail, struct kbsrc_gpu_engine** engine, kbsrc_stats_c* stats);
+void kbsrc_conversion_free_c(kbsrc_conversion* cv);
+
+/* Diagnostics: the host-side steps on their own (no GPU needed).
+ * kbsrc_plan_c: the block plan of src/resampler.cpp:98-167, info[16] = P Q taps nb marg hop nblk Nb Mb pre o E
+ *   lead general up nout; returns 0, 1 (equal rates: copy) or -1 (invalid argument).
+ * kbsrc_kernel_taps_c: Kaiser taps h[0..L] of src/design.cpp:17-37 as (hi, lo) pairs.
+ * kbsrc_burg_c: the Burg LPC prediction of src/lpc.cpp:13-42. */
+int kbsrc_plan_c(long long frames, int channels, int rate_in, int rate_out, const kbsrc_options_c* opt,
+                 long long* info, char* err, int err_len);
+int kbsrc_kernel_taps_c(int L, long long a, long long b, double beta, int threads, double* out);
+int kbsrc_burg_c(const double* x, long long len, long long n, double* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

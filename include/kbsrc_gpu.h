@@ -1,0 +1,94 @@
+/*
+ * kbsrc_gpu.h - the C ABI between the host C++ library (planning, staging, kernel taps, LPC edges, WAV I/O)
+ * and the sm_100a block engine. Plain pointers and sizes, integer status codes, nothing throws.
+ *
+ * It replaces, in HongYue1/KBSRC 1.3.0:
+ *   run_engine<T,W,C>()          src/resampler.cpp:34-88   -> kbsrc_gpu_engine_create / _run_host / _run_device
+ *   kernel_spectrum()            src/design.cpp:40-49      -> kbsrc_gpu_kernel_spectrum
+ * The whole conversion kbsrc::resample() (include/kbsrc/kbsrc.hpp:41-43) is also exported in C form by
+ * libkbsrc.so as kbsrc_resample_c (include/kbsrc/kbsrc_c.h).
+ *
+ * Output is byte-identical to the reference CPU engines: the kernels execute the reference's IEEE operation
+ * sequence (f64 for fast, double-double for exact) in round-to-nearest.
+ */
+#ifndef KBSRC_GPU_H
+#define KBSRC_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define KBSRC_GPU_OK 0
+#define KBSRC_GPU_E_ARG (-1)         /* invalid argument */
+#define KBSRC_GPU_E_NOMEM (-2)       /* device or host allocation failed */
+#define KBSRC_GPU_E_CUDA (-3)        /* a CUDA call failed; kbsrc_gpu_last_error() has the text */
+#define KBSRC_GPU_E_UNSUPPORTED (-4) /* a plan this build does not run on the GPU */
+#define KBSRC_GPU_E_NODEVICE (-5)    /* no CUDA device */
+
+#define KBSRC_GPU_FAST 0  /* float64 pipeline (reference Precision::Fast) */
+#define KBSRC_GPU_EXACT 1 /* double-double pipeline (reference Precision::Exact) */
+
+typedef struct kbsrc_gpu_engine kbsrc_gpu_engine;
+
+/* One conversion plan, as computed by the host planner (reference src/resampler.cpp:98-209).
+ * Block b of channel c reads staged samples [b*hop*Q, b*hop*Q + nb*Q) where the staged channel holds
+ * `lead` zeros/edge samples before input frame 0 (lead = marg*Q + pre), and writes output samples
+ * [b*hop*P - o, (b+1)*hop*P - o) clipped to [0, nout). */
+typedef struct {
+    int precision;      /* KBSRC_GPU_FAST or KBSRC_GPU_EXACT */
+    int channels;       /* >= 1 */
+    long long P, Q;     /* reduced rate ratio rate_out/rate_in = P/Q */
+    int nb;             /* block size factor: forward FFT nb*Q points, inverse nb*P */
+    int marg;           /* margin in units of Q (input) or P (output) */
+    long long nblk;     /* blocks per channel */
+    long long lead;     /* staged-sample index of input frame 0 */
+    long long o;        /* output offset (pre/Q*P) */
+    long long frames;   /* input frames per channel */
+    long long nout;     /* output samples per channel */
+    int up;             /* rate_out > rate_in: periodic spectrum extension instead of folding */
+    int Jg;             /* general-fold bin limit (near-unity ratios), 0 otherwise */
+    long long edge_len; /* LPC samples predicted before and after the signal per channel (0: zero padding) */
+    const double* H;    /* kernel spectrum, H_len (hi, lo) pairs, host memory; copied at create */
+    long long H_len;
+} kbsrc_gpu_desc;
+
+/* Creates an engine on the current CUDA device: FFT plans, twiddle tables and the kernel spectrum on the
+ * device. Replaces the set-up half of run_engine (src/resampler.cpp:38-40). */
+int kbsrc_gpu_engine_create(const kbsrc_gpu_desc* desc, kbsrc_gpu_engine** out);
+
+/* Runs every (channel, block) task of the plan. Host buffers:
+ *   in    interleaved input, frames * channels doubles (pinned memory gives full copy bandwidth)
+ *   head  channels * edge_len doubles: head[c*edge_len + i] is the sample i+1 frames before frame 0
+ *   tail  channels * edge_len doubles: tail[c*edge_len + i] is the sample i frames after the last frame
+ *   out   planar output, channels * nout doubles (out[c*nout + i])
+ * head/tail may be NULL when edge_len is 0. Replaces the block loop of run_engine (src/resampler.cpp:41-87). */
+int kbsrc_gpu_engine_run_host(kbsrc_gpu_engine* e, const double* in, const double* head, const double* tail,
+                              double* out);
+
+/* Same with device buffers, asynchronous on `stream` (a cudaStream_t; NULL = the engine's own stream).
+ * The caller keeps the buffers alive until the stream reaches this point. */
+int kbsrc_gpu_engine_run_device(kbsrc_gpu_engine* e, const double* d_in, const double* d_head,
+                                const double* d_tail, double* d_out, void* stream);
+
+/* Number of (channel, block) tasks, kernel launches per run, and the engine's device bytes. */
+int kbsrc_gpu_engine_info(const kbsrc_gpu_engine* e, long long* tasks, long long* launches,
+                          long long* device_bytes);
+
+void kbsrc_gpu_engine_destroy(kbsrc_gpu_engine* e);
+
+/* Real spectrum of the symmetric kernel h[0..L] placed circularly in n points, divided by scale, computed on
+ * the GPU with the reference's scalar double-double real FFT (src/design.cpp:40-49, RFFT<dd,dd,dd>).
+ * taps: (L+1) (hi, lo) pairs; H: (n/2+1) (hi, lo) pairs out. n must be even. */
+int kbsrc_gpu_kernel_spectrum(const double* taps, int L, int n, double scale, double* H);
+
+/* Text of the last error on this thread ("" if none). */
+const char* kbsrc_gpu_last_error(void);
+
+/* Engine name for Stats::isa, e.g. "sm_100a". */
+const char* kbsrc_gpu_engine_name(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

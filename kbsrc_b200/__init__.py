@@ -1,0 +1,277 @@
+"""KBSRC on B200: DFT-domain rational resampling with the overlap-save block engine on the GPU (sm_100a).
+
+Python access to the in-tree native libraries through ctypes:
+  lib/libkbsrc.so      kbsrc::resample and its C form (include/kbsrc/kbsrc_c.h)
+  lib/libkbsrc_gpu.so  the engine's C ABI (include/kbsrc_gpu.h)
+The GPU path is the only path: loading fails loudly when the libraries are missing or not built.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_DIR = os.path.join(HERE, "lib")
+HOST_SO = os.path.join(LIB_DIR, "libkbsrc.so")
+GPU_SO = os.path.join(LIB_DIR, "libkbsrc_gpu.so")
+CLI = os.path.join(HERE, "bin", "kbsrc")
+
+FAST, EXACT = 0, 1
+_P = ctypes.POINTER
+_dp = _P(ctypes.c_double)
+_lp = _P(ctypes.c_longlong)
+
+# status codes of include/kbsrc_gpu.h
+GPU_OK, GPU_E_ARG, GPU_E_NOMEM, GPU_E_CUDA, GPU_E_UNSUPPORTED, GPU_E_NODEVICE = 0, -1, -2, -3, -4, -5
+
+
+class Options(ctypes.Structure):
+    _fields_ = [("precision", ctypes.c_int), ("length", ctypes.c_double), ("beta", ctypes.c_double),
+                ("threads", ctypes.c_int), ("block", ctypes.c_int), ("lpc_edges", ctypes.c_int)]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("p", ctypes.c_longlong), ("q", ctypes.c_longlong), ("taps", ctypes.c_longlong),
+                ("block", ctypes.c_int), ("threads", ctypes.c_int), ("general_fold", ctypes.c_int),
+                ("design_seconds", ctypes.c_double), ("process_seconds", ctypes.c_double),
+                ("passband", ctypes.c_double), ("stopband", ctypes.c_double), ("isa", ctypes.c_char_p)]
+
+    def as_dict(self):
+        d = {k: getattr(self, k) for k, _ in self._fields_}
+        d["isa"] = (d["isa"] or b"").decode()
+        return d
+
+
+class GpuDesc(ctypes.Structure):
+    """kbsrc_gpu_desc (include/kbsrc_gpu.h)."""
+    _fields_ = [("precision", ctypes.c_int), ("channels", ctypes.c_int), ("P", ctypes.c_longlong),
+                ("Q", ctypes.c_longlong), ("nb", ctypes.c_int), ("marg", ctypes.c_int), ("nblk", ctypes.c_longlong),
+                ("lead", ctypes.c_longlong), ("o", ctypes.c_longlong), ("frames", ctypes.c_longlong),
+                ("nout", ctypes.c_longlong), ("up", ctypes.c_int), ("Jg", ctypes.c_int),
+                ("edge_len", ctypes.c_longlong), ("H", _dp), ("H_len", ctypes.c_longlong)]
+
+
+# Every symbol the C headers declare: (library, name, restype, argtypes)
+GPU_SYMBOLS = {
+    "kbsrc_gpu_engine_create": (ctypes.c_int, [_P(GpuDesc), _P(ctypes.c_void_p)]),
+    "kbsrc_gpu_engine_run_host": (ctypes.c_int, [ctypes.c_void_p, _dp, _dp, _dp, _dp]),
+    "kbsrc_gpu_engine_run_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                                   ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "kbsrc_gpu_engine_info": (ctypes.c_int, [ctypes.c_void_p, _lp, _lp, _lp]),
+    "kbsrc_gpu_engine_destroy": (None, [ctypes.c_void_p]),
+    "kbsrc_gpu_kernel_spectrum": (ctypes.c_int, [_dp, ctypes.c_int, ctypes.c_int, ctypes.c_double, _dp]),
+    "kbsrc_gpu_last_error": (ctypes.c_char_p, []),
+    "kbsrc_gpu_engine_name": (ctypes.c_char_p, []),
+}
+HOST_SYMBOLS = {
+    "kbsrc_output_frames": (ctypes.c_longlong, [ctypes.c_longlong, ctypes.c_int, ctypes.c_int]),
+    "kbsrc_resample_c": (ctypes.c_longlong, [_dp, ctypes.c_longlong, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                             _P(Options), _dp, ctypes.c_longlong, _P(Stats), ctypes.c_char_p,
+                                             ctypes.c_int]),
+    "kbsrc_version_c": (ctypes.c_char_p, []),
+    "kbsrc_prepare_c": (ctypes.c_int, [_dp, ctypes.c_longlong, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                       _P(Options), _P(ctypes.c_void_p), ctypes.c_char_p, ctypes.c_int]),
+    "kbsrc_conversion_run_c": (ctypes.c_int, [ctypes.c_void_p, _dp, _dp, ctypes.c_char_p, ctypes.c_int]),
+    "kbsrc_conversion_info_c": (ctypes.c_int, [ctypes.c_void_p, _lp, _lp, _P(_dp), _P(_dp),
+                                               _P(ctypes.c_void_p), _P(Stats)]),
+    "kbsrc_conversion_free_c": (None, [ctypes.c_void_p]),
+    "kbsrc_plan_c": (ctypes.c_int, [ctypes.c_longlong, ctypes.c_int, ctypes.c_int, ctypes.c_int, _P(Options), _lp,
+                                    ctypes.c_char_p, ctypes.c_int]),
+    "kbsrc_kernel_taps_c": (ctypes.c_int, [ctypes.c_int, ctypes.c_longlong, ctypes.c_longlong, ctypes.c_double,
+                                           ctypes.c_int, _dp]),
+    "kbsrc_burg_c": (ctypes.c_int, [_dp, ctypes.c_longlong, ctypes.c_longlong, _dp]),
+}
+PLAN_KEYS = ["P", "Q", "taps", "nb", "marg", "hop", "nblk", "Nb", "Mb", "pre", "o", "E", "lead", "general", "up",
+             "nout"]
+
+_gpu = None
+_host = None
+
+
+def _bind(path, table):
+    if not os.path.exists(path):
+        raise RuntimeError(f"{path} is not built: run `make -C {HERE}` (or __graft_entry__.build())")
+    lib = ctypes.CDLL(path)
+    for name, (res, args) in table.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    return lib
+
+
+def gpu_lib():
+    """libkbsrc_gpu.so with its C ABI bound."""
+    global _gpu
+    if _gpu is None:
+        _gpu = _bind(GPU_SO, GPU_SYMBOLS)
+    return _gpu
+
+
+def host_lib():
+    """libkbsrc.so (loads libkbsrc_gpu.so) with its C API bound."""
+    global _host
+    if _host is None:
+        gpu_lib()
+        _host = _bind(HOST_SO, HOST_SYMBOLS)
+    return _host
+
+
+def gpu_error():
+    return (gpu_lib().kbsrc_gpu_last_error() or b"").decode()
+
+
+def _ptr(a):
+    return a.ctypes.data_as(_dp)
+
+
+def _options(mode, length, beta, block, lpc, threads):
+    prec = {"fast": 0, "exact": 1, "ld": 2}[mode] if isinstance(mode, str) else int(mode)
+    return Options(prec, float(length), float(beta), int(threads), int(block), int(bool(lpc)))
+
+
+def output_frames(frames, rate_in, rate_out):
+    return int(host_lib().kbsrc_output_frames(frames, rate_in, rate_out))
+
+
+def resample(x, rate_in, rate_out, mode="exact", length=0.2, beta=40.0, block=0, lpc=True, threads=0, stats=None):
+    """Converts x (frames, channels) float64 from rate_in to rate_out on the GPU. Returns planar (channels, nout).
+
+    Raises ValueError for rejected arguments (the reference's messages) and RuntimeError for GPU failures.
+    """
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    if x.ndim == 1:
+        x = x[:, None]
+    frames, ch = x.shape
+    n = output_frames(frames, rate_in, rate_out)
+    if n < 0:
+        raise ValueError("sample rates must be positive" if rate_in < 1 or rate_out < 1 else "input too long")
+    out = np.zeros((ch, max(n, 1)))
+    st = Stats()
+    err = ctypes.create_string_buffer(512)
+    opt = _options(mode, length, beta, block, lpc, threads)
+    r = host_lib().kbsrc_resample_c(_ptr(x), frames, ch, rate_in, rate_out, ctypes.byref(opt), _ptr(out),
+                                    out.shape[1], ctypes.byref(st), err, 512)
+    if r == -1:
+        raise ValueError(err.value.decode())
+    if r < 0:
+        raise RuntimeError(err.value.decode())
+    if stats is not None:
+        stats.update(st.as_dict())
+    return out[:, :r]
+
+
+class Conversion:
+    """A planned conversion (kbsrc_prepare_c): plan, LPC edges, kernel spectrum and GPU engine, built once for
+    input of one shape and run many times."""
+
+    def __init__(self, x, rate_in, rate_out, mode="exact", length=0.2, beta=40.0, block=0, lpc=True, threads=0):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        if x.ndim == 1:
+            x = x[:, None]
+        self.frames, self.channels = x.shape
+        self._h = ctypes.c_void_p()
+        err = ctypes.create_string_buffer(512)
+        opt = _options(mode, length, beta, block, lpc, threads)
+        r = host_lib().kbsrc_prepare_c(_ptr(x), self.frames, self.channels, rate_in, rate_out, ctypes.byref(opt),
+                                       ctypes.byref(self._h), err, 512)
+        if r == -1:
+            raise ValueError(err.value.decode())
+        if r < 0:
+            raise RuntimeError(err.value.decode())
+        nout, elen = ctypes.c_longlong(), ctypes.c_longlong()
+        head, tail = _dp(), _dp()
+        eng = ctypes.c_void_p()
+        st = Stats()
+        host_lib().kbsrc_conversion_info_c(self._h, ctypes.byref(nout), ctypes.byref(elen), ctypes.byref(head),
+                                           ctypes.byref(tail), ctypes.byref(eng), ctypes.byref(st))
+        self.nout, self.edge_len, self.engine = nout.value, elen.value, eng.value
+        n = self.edge_len * self.channels
+        self.head = np.ctypeslib.as_array(head, (n,)).copy() if n else np.zeros(0)
+        self.tail = np.ctypeslib.as_array(tail, (n,)).copy() if n else np.zeros(0)
+        self.stats = st.as_dict()
+
+    def run(self, x, out=None):
+        """Runs on interleaved input x (frames, channels) host memory; returns planar (channels, nout)."""
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        if out is None:
+            out = np.zeros((self.channels, max(self.nout, 1)))
+        err = ctypes.create_string_buffer(512)
+        if host_lib().kbsrc_conversion_run_c(self._h, _ptr(x), _ptr(out), err, 512):
+            raise RuntimeError(err.value.decode())
+        return out[:, :self.nout]
+
+    def engine_info(self):
+        t, l, b = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_longlong()
+        gpu_lib().kbsrc_gpu_engine_info(self.engine, ctypes.byref(t), ctypes.byref(l), ctypes.byref(b))
+        return {"tasks": t.value, "launches": l.value, "device_bytes": b.value}
+
+    def run_device(self, d_in, d_head, d_tail, d_out, stream=0):
+        """Engine run on device pointers (ints), asynchronous on `stream` (a cudaStream_t as int, 0 = engine's)."""
+        rc = gpu_lib().kbsrc_gpu_engine_run_device(self.engine, d_in, d_head, d_tail, d_out, stream or None)
+        if rc:
+            raise RuntimeError(f"kbsrc_gpu_engine_run_device: {rc} {gpu_error()}")
+
+    def run_host_raw(self, x_ptr, head_ptr, tail_ptr, out_ptr):
+        """Engine run on host pointers (ints), e.g. pinned buffers; synchronous."""
+        rc = gpu_lib().kbsrc_gpu_engine_run_host(self.engine, ctypes.cast(x_ptr, _dp), ctypes.cast(head_ptr, _dp),
+                                                 ctypes.cast(tail_ptr, _dp), ctypes.cast(out_ptr, _dp))
+        if rc:
+            raise RuntimeError(f"kbsrc_gpu_engine_run_host: {rc} {gpu_error()}")
+
+    def close(self):
+        if self._h:
+            host_lib().kbsrc_conversion_free_c(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def plan(frames, channels, rate_in, rate_out, mode="exact", length=0.2, beta=40.0, block=0):
+    """The host block plan as a dict (PLAN_KEYS; "copy" True for equal rates). ValueError on rejection."""
+    info = np.zeros(16, dtype=np.int64)
+    err = ctypes.create_string_buffer(512)
+    opt = _options(mode, length, beta, block, True, 0)
+    r = host_lib().kbsrc_plan_c(frames, channels, rate_in, rate_out, ctypes.byref(opt), info.ctypes.data_as(_lp),
+                                err, 512)
+    if r < 0:
+        raise ValueError(err.value.decode())
+    d = dict(zip(PLAN_KEYS, info.tolist()))
+    d["copy"] = r == 1
+    return d
+
+
+def kernel_taps(L, a, b, beta, threads=1):
+    out = np.zeros((L + 1, 2))
+    if host_lib().kbsrc_kernel_taps_c(L, a, b, beta, threads, _ptr(out)):
+        raise ValueError("bad tap arguments")
+    return out
+
+
+def burg(x, n):
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    out = np.zeros(n)
+    if host_lib().kbsrc_burg_c(_ptr(x), len(x), n, _ptr(out)):
+        raise ValueError("bad arguments")
+    return out
+
+
+def kernel_spectrum(taps, n, scale):
+    """GPU kernel design (kbsrc_gpu_kernel_spectrum): taps (L+1, 2) (hi, lo) -> H (n/2+1, 2)."""
+    taps = np.ascontiguousarray(taps, dtype=np.float64)
+    H = np.zeros((n // 2 + 1, 2))
+    rc = gpu_lib().kbsrc_gpu_kernel_spectrum(_ptr(taps), taps.shape[0] - 1, n, scale, _ptr(H))
+    if rc:
+        raise RuntimeError(f"kbsrc_gpu_kernel_spectrum: {rc} {gpu_error()}")
+    return H
+
+
+def build(verbose=False):
+    """Compiles the native libraries in place (make -C kbsrc_b200)."""
+    import subprocess
+    r = subprocess.run(["make", "-C", HERE, "-j4"], capture_output=not verbose, text=True)
+    if r.returncode:
+        raise RuntimeError(f"build failed:\n{r.stdout}\n{r.stderr}")

@@ -1,0 +1,940 @@
+// sm_100a block engine of the DFT-domain resampler, and its C ABI (include/kbsrc_gpu.h).
+//
+// One run processes every (channel, block) task of a conversion plan: the overlap-save loop of the
+// reference's run_engine (HongYue1/KBSRC src/resampler.cpp:34-88). Per task:
+//   forward real FFT of nb*Q points  = gather (staged input + LPC edges) -> complex FFT of h = nb*Q/2 points
+//                                      -> split into h+1 real-spectrum bins          (fft.hpp:362-409)
+//   spectrum multiply with the kernel, fold (down) or periodic extension (up)        (resampler.cpp:53-78)
+//   inverse real FFT of nb*P points  = merge into h' = nb*P/2 complex points -> complex FFT (fft.hpp:411-461)
+//   discard the margins and write hop*P output samples                               (resampler.cpp:80-84)
+// Complex FFTs of more than 2048 points use the reference's four-step split n = N1*N2 (fft.hpp:267-313):
+// a column pass (N2 sequences of N1, stride N2, then the w_n^{k1 n2} twiddle) and a row pass (N1 sequences
+// of N2, stored transposed). Each pass is one launch over all tasks of a wave; the sub-FFTs run in shared
+// memory (fft.cuh). Smaller FFTs run whole in one CTA.
+//
+// Arithmetic (dd.cuh): fast = f64; exact = short-add dd in the four-step sub-FFTs and accurate-add dd
+// elsewhere, exactly as the reference instantiates its templates, so the output is byte-identical.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../host/ddh.hpp"
+#include "dd.cuh"
+#include "fft.cuh"
+#include "kbsrc_gpu.h"
+
+using namespace kbsrc::dev;
+namespace hd = kbsrc::host;
+
+namespace {
+
+thread_local std::string g_error;
+
+int fail(int code, const std::string& msg) {
+    g_error = msg;
+    return code;
+}
+
+#define KB_CUDA(call)                                                                                   \
+    do {                                                                                                \
+        cudaError_t err_ = (call);                                                                      \
+        if (err_ != cudaSuccess) return fail(KBSRC_GPU_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(err_)); \
+    } while (0)
+
+// ------------------------------------------------------------------------------------------------------
+// kernel parameter blocks
+// ------------------------------------------------------------------------------------------------------
+
+// The staged channel of the reference (resampler.cpp:168-186) without materialising it: zeros, the LPC head,
+// the interleaved input, the LPC tail, zeros.
+struct Signal {
+    const double* in;
+    const double* head;
+    const double* tail;
+    long long frames, edge, lead, hopQ, nblk;
+    int ch;
+};
+
+__device__ __forceinline__ double signal_at(const Signal& s, int c, long long g) {
+    const long long t = g - s.lead;
+    if (t >= 0 && t < s.frames) return __ldg(s.in + t * s.ch + c);
+    if (t < 0 && t >= -s.edge) return __ldg(s.head + c * s.edge + (-1 - t));
+    if (t >= s.frames && t < s.frames + s.edge) return __ldg(s.tail + c * s.edge + (t - s.frames));
+    return 0.0;
+}
+
+// Discard and copy (resampler.cpp:80-84): sample e of block b's inverse FFT lands at b*hopP + e - margP - o
+struct Output {
+    double* out;
+    long long nout, o, hopP, margP, nblk;
+};
+
+__device__ __forceinline__ void emit(const Output& o, int c, long long b, long long e, double v) {
+    const long long k = e - o.margP;
+    if (k < 0 || k >= o.hopP) return;
+    const long long d = b * o.hopP + k - o.o;
+    if (d >= 0 && d < o.nout) o.out[c * o.nout + d] = v;
+}
+
+enum Src { kSrcSignal = 0, kSrcComplex = 1, kSrcDDReal = 2 };
+enum Dst { kDstComplex = 0, kDstOutput = 1 };
+
+template <class Ar>
+struct PassParams {
+    SubPlan sp;                   // the sub-FFT
+    int N1, N2, F;                // four-step shape; F sequences per CTA
+    const CxW<Ar>* tw_stage;      // stage twiddles of sp
+    const CxW<Ar>* tw4;           // four-step twiddles [k1*N2 + n2] (column pass)
+    OddRoots<typename Ar::W> odd; // radix 3/5/7 constants
+    CxR<Ar>* src;                 // complex input (or output of the column pass), per task `stride`
+    CxR<Ar>* dst;
+    long long stride;             // complex elements between task slots
+    long long task0;              // first task of this launch (blockIdx.y adds)
+    Signal sig;                   // kSrcSignal
+    const double* ddreal;         // kSrcDDReal: (hi, lo) pairs
+    Output out;                   // kDstOutput
+};
+
+template <class Ar>
+__device__ __forceinline__ CxR<Ar> load_input(const PassParams<Ar>& P, int src_kind, const CxR<Ar>* src, long long i,
+                                              long long task) {
+    using R = typename Ar::R;
+    if (src_kind == kSrcSignal) {
+        const int c = (int)(task / P.sig.nblk);
+        const long long b = task % P.sig.nblk, g = b * P.sig.hopQ + 2 * i;
+        return CxR<Ar>{Ar::from_f64(signal_at(P.sig, c, g)), Ar::from_f64(signal_at(P.sig, c, g + 1))};
+    }
+    if (src_kind == kSrcComplex) return src[i];
+    if constexpr (Ar::kDD) {
+        const double2 a = __ldg(reinterpret_cast<const double2*>(P.ddreal) + 2 * i);
+        const double2 b = __ldg(reinterpret_cast<const double2*>(P.ddreal) + 2 * i + 1);
+        return CxR<Ar>{R{a.x, a.y}, R{b.x, b.y}};
+    } else {
+        return CxR<Ar>{P.ddreal[4 * i], P.ddreal[4 * i + 2]};
+    }
+}
+
+template <class Ar>
+__device__ __forceinline__ CxR<Ar> czero() {
+    return CxR<Ar>{Ar::zero(), Ar::zero()};
+}
+
+// Column pass: sequences n2 in [c0, c0+F) of length N1 (stride N2), twiddle, store in place
+// (fft.hpp:283-299). blockIdx.x: column group; blockIdx.y: task slot.
+template <class Ar, int SRC>
+__global__ void __launch_bounds__(256) k_column(const __grid_constant__ PassParams<Ar> P) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    using C = CxR<Ar>;
+    const int F = P.F, N1 = P.N1, N2 = P.N2;
+    C* A = reinterpret_cast<C*>(smem);
+    C* B = A + N1 * F;
+    const long long task = P.task0 + blockIdx.y;
+    const int c0 = blockIdx.x * F;
+    const C* src = P.src + blockIdx.y * P.stride;
+    C* dst = P.dst + blockIdx.y * P.stride;
+    for (int e = threadIdx.x; e < N1 * F; e += blockDim.x) {
+        const int r = e / F, f = e - r * F, n2 = c0 + f;
+        A[r * F + f] = n2 < N2 ? load_input<Ar>(P, SRC, src, (long long)r * N2 + n2, task) : czero<Ar>();
+    }
+    __syncthreads();
+    const C* res = stockham<Ar>(P.sp, A, B, F, P.tw_stage, P.odd);
+    for (int e = threadIdx.x; e < N1 * F; e += blockDim.x) {
+        const int k1 = e / F, f = e - k1 * F, n2 = c0 + f;
+        if (n2 >= N2) continue;
+        C v = res[k1 * F + f];
+        if (k1 && (Ar::kLanes || n2)) v = c_mulw<Ar>(v, ld_tw(P.tw4 + (long long)k1 * N2 + n2));
+        if (Ar::kLaneRenorm) v = c_renorm<Ar>(v);
+        dst[(long long)k1 * N2 + n2] = v;
+    }
+}
+
+// Row pass: rows r in [r0, r0+F) of length N2 (contiguous), stored transposed to [N1*k2 + r]
+// (fft.hpp:300-311), or written straight to the output as real samples (fft.hpp:459-460).
+template <class Ar, int DST>
+__global__ void __launch_bounds__(256) k_row(const __grid_constant__ PassParams<Ar> P) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    using C = CxR<Ar>;
+    const int F = P.F, N1 = P.N1, N2 = P.N2;
+    C* A = reinterpret_cast<C*>(smem);
+    C* B = A + N2 * F;
+    const long long task = P.task0 + blockIdx.y;
+    const int r0 = blockIdx.x * F;
+    const C* src = P.src + blockIdx.y * P.stride;
+    for (int e = threadIdx.x; e < N2 * F; e += blockDim.x) {
+        const int f = e / N2, i = e - f * N2, row = r0 + f;
+        A[i * F + f] = row < N1 ? src[(long long)row * N2 + i] : czero<Ar>();
+    }
+    __syncthreads();
+    const C* res = stockham<Ar>(P.sp, A, B, F, P.tw_stage, P.odd);
+    C* dst = P.dst + blockIdx.y * P.stride;
+    const int c = DST == kDstOutput ? (int)(task / P.out.nblk) : 0;
+    const long long b = DST == kDstOutput ? task % P.out.nblk : 0;
+    for (int e = threadIdx.x; e < N2 * F; e += blockDim.x) {
+        const int k2 = e / F, f = e - k2 * F, row = r0 + f;
+        if (row >= N1) continue;
+        C v = res[k2 * F + f];
+        if (Ar::kLaneRenorm) v = c_renorm<Ar>(v);
+        const long long iz = (long long)N1 * k2 + row;
+        if (DST == kDstComplex) {
+            dst[iz] = v;
+        } else {
+            emit(P.out, c, b, 2 * iz, Ar::to_f64(v.re));
+            emit(P.out, c, b, 2 * iz + 1, Ar::to_f64(Ar::neg(v.im)));
+        }
+    }
+}
+
+// Whole FFT of n <= 2048 points in one CTA (the reference's direct SFFT path, fft.hpp:241-244,279).
+template <class Ar, int SRC, int DST>
+__global__ void __launch_bounds__(256) k_direct(const __grid_constant__ PassParams<Ar> P) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    using C = CxR<Ar>;
+    const int n = P.sp.n;
+    C* A = reinterpret_cast<C*>(smem);
+    C* B = A + n;
+    const long long task = P.task0 + blockIdx.y;
+    const C* src = P.src + blockIdx.y * P.stride;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) A[i] = load_input<Ar>(P, SRC, src, i, task);
+    __syncthreads();
+    const C* res = stockham<Ar>(P.sp, A, B, 1, P.tw_stage, P.odd);
+    C* dst = P.dst + blockIdx.y * P.stride;
+    const int c = DST == kDstOutput ? (int)(task / P.out.nblk) : 0;
+    const long long b = DST == kDstOutput ? task % P.out.nblk : 0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const C v = res[i];
+        if (DST == kDstComplex) {
+            dst[i] = v;
+        } else {
+            emit(P.out, c, b, 2LL * i, Ar::to_f64(v.re));
+            emit(P.out, c, b, 2LL * i + 1, Ar::to_f64(Ar::neg(v.im)));
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------------------------
+// real-FFT split, spectrum, real-FFT merge
+// ------------------------------------------------------------------------------------------------------
+template <class Ar>
+struct SpecParams {
+    const CxR<Ar>* Z;    // forward complex FFT output, h per task
+    CxR<Ar>* X;          // forward spectrum, h+1 per task
+    CxR<Ar>* Zi;         // inverse complex FFT input, hi per task
+    long long stride;
+    const CxW<Ar>* w_fw; // e^{-2 pi i k/Nb}, k <= h
+    const CxW<Ar>* w_iv; // e^{-2 pi i k/Mb}, k <= hi
+    const typename Ar::W* H;
+    int h, hi;           // Nb/2 and Mb/2
+    int Nb, Mb, up;
+    double scale;        // kernel design: H = X.re / scale
+    typename Ar::W* Hout;
+};
+
+// X[k] = (E + O w[k]) / 2 with E = z[k] + conj z[h-k], O = -i (z[k] - conj z[h-k]) (fft.hpp:365-408).
+// Double-double computes conjugate pairs together (one E, O for k and h-k); f64 computes each k alone.
+template <class Ar>
+__global__ void k_split(const __grid_constant__ SpecParams<Ar> P) {
+    using C = CxR<Ar>;
+    const C* Z = P.Z + blockIdx.y * P.stride;
+    C* X = P.X + blockIdx.y * P.stride;
+    const int h = P.h;
+    const typename Ar::R half = Ar::from_f64(0.5);
+    const int last = Ar::kDD ? h / 2 : h - 1;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k <= last; k += gridDim.x * blockDim.x) {
+        if (k == 0) {
+            const C z0 = Z[0];
+            X[0] = C{Ar::add(z0.re, z0.im), Ar::zero()};
+            X[h] = C{Ar::sub(z0.re, z0.im), Ar::zero()};
+            continue;
+        }
+        const int j = h - k;
+        const C a = Z[k], bb = c_conj<Ar>(Z[j]);
+        const C E = c_add<Ar>(a, bb), O = c_mul_mi<Ar>(c_sub<Ar>(a, bb));
+        const C v = c_add<Ar>(E, c_mulw<Ar>(O, ld_tw(P.w_fw + k)));
+        X[k] = c_scale<Ar>(v, half);
+        if (Ar::kDD && j != k) {
+            const C u = c_add<Ar>(c_conj<Ar>(E), c_mulw<Ar>(c_conj<Ar>(O), ld_tw(P.w_fw + j)));
+            X[j] = c_scale<Ar>(u, half);
+        }
+    }
+}
+
+template <class W>
+__device__ __forceinline__ W ld_w(const W* p) {
+    return __ldg(p);
+}
+template <>
+__device__ __forceinline__ dd ld_w<dd>(const dd* p) {
+    const double2 a = __ldg(reinterpret_cast<const double2*>(p));
+    return dd{a.x, a.y};
+}
+
+// Y[k]: spectrum multiply with fold (down) or periodic extension (up) (resampler.cpp:64-78)
+template <class Ar>
+__device__ __forceinline__ CxR<Ar> spectrum_bin(const SpecParams<Ar>& P, const CxR<Ar>* X, int k) {
+    using C = CxR<Ar>;
+    const int Nb = P.Nb, Mb = P.Mb;
+    if (P.up) {
+        const int kk = k % Nb;
+        const C v = kk <= Nb / 2 ? X[kk] : c_conj<Ar>(X[Nb - kk]);
+        C y = c_scale<Ar>(v, Ar::from_w(ld_w(P.H + k)));
+        if (2 * k == Mb) y.im = Ar::zero();
+        return y;
+    }
+    if (2 * k == Mb)
+        return C{Ar::mul(Ar::mul(Ar::from_f64(2.0), X[k].re), Ar::from_w(ld_w(P.H + k))), Ar::zero()};
+    C y = c_scale<Ar>(X[k], Ar::from_w(ld_w(P.H + k)));
+    const int j = Mb - k, jmax = min(Nb / 2, Mb - 1);
+    if (k >= 1 && j <= jmax) {  // j >= Mb/2 + 1 = K holds for every k < Mb/2
+        const C v = c_scale<Ar>(X[j], Ar::from_w(ld_w(P.H + j)));
+        y = c_add<Ar>(y, c_conj<Ar>(v));
+    }
+    return y;
+}
+
+// Inverse merge z[k] = conj(E + i D), E = Y[k] + conj Y[hi-k], D = (Y[k] - conj Y[hi-k]) conj w[k]
+// (fft.hpp:411-458); pairs in dd, each k alone in f64.
+template <class Ar>
+__global__ void k_merge(const __grid_constant__ SpecParams<Ar> P) {
+    using C = CxR<Ar>;
+    const C* X = P.X + blockIdx.y * P.stride;
+    C* Zi = P.Zi + blockIdx.y * P.stride;
+    const int hi = P.hi;
+    const int last = Ar::kDD ? hi / 2 : hi - 1;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k <= last; k += gridDim.x * blockDim.x) {
+        const int j = hi - k;
+        const C a = spectrum_bin<Ar>(P, X, k), bb = c_conj<Ar>(spectrum_bin<Ar>(P, X, j));
+        const C E = c_add<Ar>(a, bb), split = c_sub<Ar>(a, bb);
+        const CxW<Ar> wk = ld_tw(P.w_iv + k);
+        const C D = c_mulw<Ar>(split, CxW<Ar>{wk.re, w_neg(wk.im)});
+        const C v = {Ar::sub(E.re, D.im), Ar::add(E.im, D.re)};
+        Zi[k] = c_conj<Ar>(v);
+        if (Ar::kDD && k && j != k) {
+            const C Ej = c_conj<Ar>(E);
+            const CxW<Ar> wj = ld_tw(P.w_iv + j);
+            const C Dj = c_mulw<Ar>(C{Ar::neg(split.re), split.im}, CxW<Ar>{wj.re, w_neg(wj.im)});
+            const C u = {Ar::sub(Ej.re, Dj.im), Ar::add(Ej.im, Dj.re)};
+            Zi[j] = c_conj<Ar>(u);
+        }
+    }
+}
+
+// dd / double (double_double.hpp:80-84) with IEEE division
+__device__ __forceinline__ dd div_dd_f64(dd a, double b) {
+    auto mul_f64 = [](dd x, double y) {
+        const double p = __dmul_rn(x.hi, y);
+        double e = __fma_rn(x.hi, y, -p);
+        e = __dadd_rn(e, __dmul_rn(x.lo, y));
+        return qts(p, e);
+    };
+    const double q1 = __ddiv_rn(a.hi, b);
+    dd r = add_accurate(a, dd_neg(mul_f64(dd{b, 0.0}, q1)));
+    const double q2 = __ddiv_rn(r.hi, b);
+    r = add_accurate(r, dd_neg(mul_f64(dd{b, 0.0}, q2)));
+    const double q3 = __ddiv_rn(r.hi, b);
+    return add_accurate(qts(q1, q2), dd{q3, 0.0});
+}
+
+// Kernel design: H[k] = X[k].re / scale (design.cpp:46-47)
+__global__ void k_design_out(const __grid_constant__ SpecParams<ArDDAccurate> P) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k <= P.h; k += gridDim.x * blockDim.x)
+        P.Hout[k] = div_dd_f64(P.X[k].re, P.scale);
+}
+
+// ------------------------------------------------------------------------------------------------------
+// host side: FFT plans and tables (built in dd on the host, as the reference builds them)
+// ------------------------------------------------------------------------------------------------------
+struct HostCx {
+    hd::dd re, im;
+};
+
+// Stockham plan of n points: radices 4,..,4,2,..,2,3,..,5,..,7,.. (fft.hpp:93-97); stage twiddles
+// w_n^{s p u} appended to `tw` (fft.hpp:98-107).
+int build_sub(int n, std::vector<HostCx>& tw, SubPlan& sp) {
+    int rs[64], ns = 0, t = n;
+    while (t % 4 == 0) { rs[ns++] = 4; t /= 4; }
+    while (t % 2 == 0) { rs[ns++] = 2; t /= 2; }
+    for (int p : {3, 5, 7})
+        while (t % p == 0) { rs[ns++] = p; t /= p; }
+    if (t != 1) return fail(KBSRC_GPU_E_UNSUPPORTED, "FFT length not 7-smooth");
+    if (ns > kMaxStages) return fail(KBSRC_GPU_E_UNSUPPORTED, "FFT length has too many stages");
+    std::memset(&sp, 0, sizeof sp);
+    sp.n = n;
+    sp.nst = ns;
+    hd::RootTable rt(n);
+    int rem = n, s = 1;
+    for (int g = 0; g < ns; g++) {
+        const int r = rs[g], m = rem / r;
+        sp.st[g] = Stage{r, m, s, (int)tw.size()};
+        for (int p = 0; p < m; p++)
+            for (int u = 1; u < r; u++) {
+                HostCx w;
+                rt.get(-(long long)s * p * u, w.re, w.im);
+                tw.push_back(w);
+            }
+        rem /= r;
+        s *= r;
+    }
+    if (tw.empty()) tw.push_back(HostCx{});  // keep the table pointer valid for n = 1
+    return KBSRC_GPU_OK;
+}
+
+struct HostCfft {
+    int n = 0, four = 0, N1 = 0, N2 = 0;
+    SubPlan s1{}, s2{}, sd{};
+    std::vector<HostCx> tw_stage, tw4;
+};
+
+// Complex FFT of n points (fft.hpp:226-265): direct up to 2048 points, else four-step with N1 the largest
+// divisor <= sqrt(n) (falling back to direct when N1 < 8).
+int build_cfft(int n, HostCfft& c) {
+    c.n = n;
+    if (!hd::smooth7(n)) return fail(KBSRC_GPU_E_UNSUPPORTED, "FFT length not 7-smooth (Bluestein)");
+    c.four = n > 2048;
+    if (c.four) {
+        int best = 1;
+        for (int d = 1; (long long)d * d <= n; d++)
+            if (n % d == 0) best = d;
+        c.N1 = best;
+        c.N2 = n / best;
+        if (c.N1 < 8) c.four = 0;
+    }
+    if (!c.four) return build_sub(n, c.tw_stage, c.sd);
+    int rc = build_sub(c.N1, c.tw_stage, c.s1);
+    if (rc) return rc;
+    if ((rc = build_sub(c.N2, c.tw_stage, c.s2)) != KBSRC_GPU_OK) return rc;
+    c.tw4.resize((size_t)n);
+    hd::RootTable rt(n);
+    for (int k1 = 0; k1 < c.N1; k1++)
+        for (int n2 = 0; n2 < c.N2; n2++) {
+            HostCx& w = c.tw4[(size_t)k1 * c.N2 + n2];
+            rt.get(-(long long)k1 * n2, w.re, w.im);
+        }
+    return KBSRC_GPU_OK;
+}
+
+// w[k] = e^{-2 pi i k/N}, k <= N/2 (fft.hpp:356-357)
+std::vector<HostCx> split_roots(int N) {
+    std::vector<HostCx> w((size_t)N / 2 + 1);
+    hd::RootTable rt(N);
+    for (int k = 0; k <= N / 2; k++) rt.get(-k, w[k].re, w[k].im);
+    return w;
+}
+
+// Device copy of a table: dd pairs for double-double, the high parts for f64 (fft.hpp:16)
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    ~DevBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    int alloc(size_t n) {
+        release();
+        if (n == 0) n = 16;
+        cudaError_t e = cudaMalloc(&p, n);
+        if (e != cudaSuccess) {
+            p = nullptr;
+            return fail(e == cudaErrorMemoryAllocation ? KBSRC_GPU_E_NOMEM : KBSRC_GPU_E_CUDA,
+                        std::string("cudaMalloc: ") + cudaGetErrorString(e));
+        }
+        bytes = n;
+        return KBSRC_GPU_OK;
+    }
+};
+
+int upload_cx(const std::vector<HostCx>& v, bool dd_tables, DevBuf& out) {
+    std::vector<double> flat;
+    if (dd_tables) {
+        flat.resize(v.size() * 4);
+        for (size_t i = 0; i < v.size(); i++) {
+            flat[4 * i] = v[i].re.hi; flat[4 * i + 1] = v[i].re.lo;
+            flat[4 * i + 2] = v[i].im.hi; flat[4 * i + 3] = v[i].im.lo;
+        }
+    } else {
+        flat.resize(v.size() * 2);
+        for (size_t i = 0; i < v.size(); i++) { flat[2 * i] = v[i].re.hi; flat[2 * i + 1] = v[i].im.hi; }
+    }
+    int rc = out.alloc(flat.size() * sizeof(double));
+    if (rc) return rc;
+    KB_CUDA(cudaMemcpy(out.p, flat.data(), flat.size() * sizeof(double), cudaMemcpyHostToDevice));
+    return KBSRC_GPU_OK;
+}
+
+template <class W>
+OddRoots<W> odd_roots() {
+    OddRoots<W> o{};
+    const int rr[3] = {3, 5, 7};
+    for (int i = 0; i < 3; i++)
+        for (int k = 0; k < rr[i]; k++) {
+            hd::dd c, s;
+            hd::unit_root(k, rr[i], c, s);
+            if constexpr (sizeof(W) == sizeof(double)) {
+                o.c[i][k] = c.hi;
+                o.s[i][k] = s.hi;
+            } else {
+                o.c[i][k] = W{c.hi, c.lo};
+                o.s[i][k] = W{s.hi, s.lo};
+            }
+        }
+    return o;
+}
+
+// A complex FFT resident on the device
+struct DevCfft {
+    HostCfft host;  // shapes and sub-plans (tables released after upload)
+    DevBuf tw_stage, tw4;
+};
+
+int make_dev_cfft(int n, bool dd_tables, DevCfft& d) {
+    int rc = build_cfft(n, d.host);
+    if (rc) return rc;
+    if ((rc = upload_cx(d.host.tw_stage, dd_tables, d.tw_stage)) != KBSRC_GPU_OK) return rc;
+    if (d.host.four && (rc = upload_cx(d.host.tw4, dd_tables, d.tw4)) != KBSRC_GPU_OK) return rc;
+    std::vector<HostCx>().swap(d.host.tw_stage);
+    std::vector<HostCx>().swap(d.host.tw4);
+    return KBSRC_GPU_OK;
+}
+
+// Launch shape of a shared-memory pass over sequences of length n: F sequences per CTA, T threads.
+struct Shape {
+    int F, T;
+    size_t smem;
+};
+
+int max_bfly(const SubPlan& sp) {
+    int b = 1;
+    for (int g = 0; g < sp.nst; g++) b = std::max(b, sp.st[g].m * sp.st[g].s);
+    return b;
+}
+
+Shape pick_shape(const SubPlan& sp, int count, size_t esize, int fmax) {
+    const size_t budget = 100 * 1024;
+    int F = 1;
+    for (int f = fmax; f >= 1; f--) {
+        if (2 * (size_t)sp.n * f * esize > budget) continue;
+        if (F == 1) F = f;
+        if (count % f == 0) { F = f; break; }
+    }
+    int T = ((max_bfly(sp) * F + 31) / 32) * 32;
+    T = std::max(64, std::min(256, T));
+    return Shape{F, T, 2 * (size_t)sp.n * F * esize};
+}
+
+int env_int(const char* name, int dflt) {
+    const char* v = std::getenv(name);
+    return v && *v ? std::atoi(v) : dflt;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------------------------------------------
+// the engine
+// ------------------------------------------------------------------------------------------------------
+struct kbsrc_gpu_engine {
+    kbsrc_gpu_desc d{};
+    bool exact = false;
+    int device = 0;
+    int Nb = 0, Mb = 0, hf = 0, hi = 0, hop = 0;
+    long long tasks = 0, wave = 0, stride = 0, launches = 0;
+    cudaStream_t stream = nullptr;
+    DevCfft fw, iv;
+    DevBuf w_fw, w_iv, H;
+    DevBuf bufA, bufB;
+    DevBuf d_in, d_head, d_tail, d_out;
+    Shape col_fw{}, row_fw{}, col_iv{}, row_iv{}, dir_fw{}, dir_iv{};
+    OddRoots<dd> odd_dd{};
+    OddRoots<double> odd_f64{};
+    ~kbsrc_gpu_engine() {
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+namespace {
+
+template <class W>
+const OddRoots<W>& odd_of(const kbsrc_gpu_engine* e);
+template <>
+const OddRoots<dd>& odd_of<dd>(const kbsrc_gpu_engine* e) { return e->odd_dd; }
+template <>
+const OddRoots<double>& odd_of<double>(const kbsrc_gpu_engine* e) { return e->odd_f64; }
+
+// Lets every pass kernel use up to the device's shared memory per block (once per device).
+int allow_large_smem() {
+    static bool done[64] = {};
+    int dev = 0;
+    KB_CUDA(cudaGetDevice(&dev));
+    if (dev < 64 && done[dev]) return KBSRC_GPU_OK;
+    int mx = 0;
+    KB_CUDA(cudaDeviceGetAttribute(&mx, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+#define KB_SMEM(k) KB_CUDA(cudaFuncSetAttribute((const void*)(k), cudaFuncAttributeMaxDynamicSharedMemorySize, mx))
+    KB_SMEM((k_column<ArF64, kSrcSignal>));
+    KB_SMEM((k_column<ArF64, kSrcComplex>));
+    KB_SMEM((k_column<ArDDShort, kSrcSignal>));
+    KB_SMEM((k_column<ArDDShort, kSrcComplex>));
+    KB_SMEM((k_column<ArDDAccurate, kSrcDDReal>));
+    KB_SMEM((k_row<ArF64, kDstComplex>));
+    KB_SMEM((k_row<ArF64, kDstOutput>));
+    KB_SMEM((k_row<ArDDShort, kDstComplex>));
+    KB_SMEM((k_row<ArDDShort, kDstOutput>));
+    KB_SMEM((k_row<ArDDAccurate, kDstComplex>));
+    KB_SMEM((k_direct<ArF64, kSrcSignal, kDstComplex>));
+    KB_SMEM((k_direct<ArF64, kSrcComplex, kDstOutput>));
+    KB_SMEM((k_direct<ArDDAccurate, kSrcSignal, kDstComplex>));
+    KB_SMEM((k_direct<ArDDAccurate, kSrcComplex, kDstOutput>));
+    KB_SMEM((k_direct<ArDDAccurate, kSrcDDReal, kDstComplex>));
+#undef KB_SMEM
+    if (dev < 64) done[dev] = true;
+    return KBSRC_GPU_OK;
+}
+
+unsigned grid_for(long long n, int threads) {
+    long long b = (n + threads - 1) / threads;
+    return (unsigned)std::max(1LL, std::min(b, 65535LL));
+}
+
+// Enqueues all passes for every wave of tasks. ArL: four-step sub-FFT arithmetic, ArS: everything else.
+template <class ArL, class ArS>
+int enqueue(kbsrc_gpu_engine* e, const double* in, const double* head, const double* tail, double* out,
+            cudaStream_t st) {
+    using CL = CxR<ArL>;
+    using CS = CxR<ArS>;
+    static_assert(sizeof(CL) == sizeof(CS), "one element size per mode");
+    using WL = typename ArL::W;
+    using WS = typename ArS::W;
+    const kbsrc_gpu_desc& d = e->d;
+    const Signal sig{in, head, tail, d.frames, d.edge_len, d.lead, (long long)e->hop * d.Q, d.nblk, d.channels};
+    const Output o{out, d.nout, d.o, (long long)e->hop * d.P, (long long)d.marg * d.P, d.nblk};
+    CL* AL = static_cast<CL*>(e->bufA.p);
+    CL* BL = static_cast<CL*>(e->bufB.p);
+    CS* AS = static_cast<CS*>(e->bufA.p);
+    CS* BS = static_cast<CS*>(e->bufB.p);
+    long long launches = 0;
+    for (long long t0 = 0; t0 < e->tasks; t0 += e->wave) {
+        const unsigned nt = (unsigned)std::min(e->wave, e->tasks - t0);
+        // forward real FFT: gather + complex FFT into B (natural order)
+        if (e->fw.host.four) {
+            const HostCfft& c = e->fw.host;
+            PassParams<ArL> p{};
+            p.sp = c.s1; p.N1 = c.N1; p.N2 = c.N2; p.F = e->col_fw.F;
+            p.tw_stage = static_cast<const CxW<ArL>*>(e->fw.tw_stage.p);
+            p.tw4 = static_cast<const CxW<ArL>*>(e->fw.tw4.p);
+            p.odd = odd_of<WL>(e);
+            p.src = AL; p.dst = AL; p.stride = e->stride; p.task0 = t0; p.sig = sig;
+            k_column<ArL, kSrcSignal><<<dim3((c.N2 + p.F - 1) / p.F, nt), e->col_fw.T, e->col_fw.smem, st>>>(p);
+            p.sp = c.s2; p.F = e->row_fw.F; p.src = AL; p.dst = BL;
+            k_row<ArL, kDstComplex><<<dim3((c.N1 + p.F - 1) / p.F, nt), e->row_fw.T, e->row_fw.smem, st>>>(p);
+            launches += 2;
+        } else {
+            PassParams<ArS> p{};
+            p.sp = e->fw.host.sd; p.F = 1;
+            p.tw_stage = static_cast<const CxW<ArS>*>(e->fw.tw_stage.p);
+            p.odd = odd_of<WS>(e);
+            p.src = AS; p.dst = BS; p.stride = e->stride; p.task0 = t0; p.sig = sig;
+            k_direct<ArS, kSrcSignal, kDstComplex><<<dim3(1, nt), e->dir_fw.T, e->dir_fw.smem, st>>>(p);
+            launches += 1;
+        }
+        // split into the real spectrum (B -> A), multiply/fold and merge (A -> B)
+        SpecParams<ArS> s{};
+        s.Z = BS; s.X = AS; s.Zi = BS; s.stride = e->stride;
+        s.w_fw = static_cast<const CxW<ArS>*>(e->w_fw.p);
+        s.w_iv = static_cast<const CxW<ArS>*>(e->w_iv.p);
+        s.H = static_cast<const WS*>(e->H.p);
+        s.h = e->hf; s.hi = e->hi; s.Nb = e->Nb; s.Mb = e->Mb; s.up = d.up;
+        k_split<ArS><<<dim3(grid_for(e->hf / 2 + 1 + (ArS::kDD ? 0 : e->hf / 2), 256), nt), 256, 0, st>>>(s);
+        k_merge<ArS><<<dim3(grid_for(e->hi / 2 + 1 + (ArS::kDD ? 0 : e->hi / 2), 256), nt), 256, 0, st>>>(s);
+        launches += 2;
+        // inverse complex FFT of B and the output epilogue
+        if (e->iv.host.four) {
+            const HostCfft& c = e->iv.host;
+            PassParams<ArL> p{};
+            p.sp = c.s1; p.N1 = c.N1; p.N2 = c.N2; p.F = e->col_iv.F;
+            p.tw_stage = static_cast<const CxW<ArL>*>(e->iv.tw_stage.p);
+            p.tw4 = static_cast<const CxW<ArL>*>(e->iv.tw4.p);
+            p.odd = odd_of<WL>(e);
+            p.src = BL; p.dst = BL; p.stride = e->stride; p.task0 = t0; p.out = o;
+            k_column<ArL, kSrcComplex><<<dim3((c.N2 + p.F - 1) / p.F, nt), e->col_iv.T, e->col_iv.smem, st>>>(p);
+            p.sp = c.s2; p.F = e->row_iv.F;
+            k_row<ArL, kDstOutput><<<dim3((c.N1 + p.F - 1) / p.F, nt), e->row_iv.T, e->row_iv.smem, st>>>(p);
+            launches += 2;
+        } else {
+            PassParams<ArS> p{};
+            p.sp = e->iv.host.sd; p.F = 1;
+            p.tw_stage = static_cast<const CxW<ArS>*>(e->iv.tw_stage.p);
+            p.odd = odd_of<WS>(e);
+            p.src = BS; p.dst = BS; p.stride = e->stride; p.task0 = t0; p.out = o;
+            k_direct<ArS, kSrcComplex, kDstOutput><<<dim3(1, nt), e->dir_iv.T, e->dir_iv.smem, st>>>(p);
+            launches += 1;
+        }
+    }
+    e->launches = launches;
+    KB_CUDA(cudaGetLastError());
+    return KBSRC_GPU_OK;
+}
+
+Shape direct_shape(const SubPlan& sp, size_t esize) {
+    int T = ((max_bfly(sp) + 31) / 32) * 32;
+    T = std::max(64, std::min(256, T));
+    return Shape{1, T, 2 * (size_t)sp.n * esize};
+}
+
+int check_desc(const kbsrc_gpu_desc* d) {
+    if (!d) return fail(KBSRC_GPU_E_ARG, "null descriptor");
+    if (d->precision != KBSRC_GPU_FAST && d->precision != KBSRC_GPU_EXACT) return fail(KBSRC_GPU_E_ARG, "precision");
+    if (d->channels < 1 || d->P < 1 || d->Q < 1 || d->nb < 2 || d->nb % 2 || d->marg < 0 || d->nb <= 2 * d->marg)
+        return fail(KBSRC_GPU_E_ARG, "bad plan shape");
+    if (d->frames < 0 || d->nout < 0 || d->nblk < 0 || d->edge_len < 0 || d->lead < 0)
+        return fail(KBSRC_GPU_E_ARG, "bad plan sizes");
+    if ((long long)d->nb * std::max(d->P, d->Q) > (1LL << 30)) return fail(KBSRC_GPU_E_ARG, "transform too large");
+    const long long need = d->Jg ? (long long)d->Jg + 1 : (d->up ? d->nb * d->P / 2 + 1 : d->nb * d->Q / 2 + 1);
+    if (!d->H || d->H_len < need) return fail(KBSRC_GPU_E_ARG, "kernel spectrum too short");
+    if (d->Jg) return fail(KBSRC_GPU_E_UNSUPPORTED, "general fold (near-unity ratio) is not on the GPU yet");
+    return KBSRC_GPU_OK;
+}
+
+int upload_real(const double* hilo, long long n, bool dd_tables, DevBuf& out) {
+    std::vector<double> v;
+    if (dd_tables) v.assign(hilo, hilo + 2 * n);
+    else {
+        v.resize((size_t)n);
+        for (long long i = 0; i < n; i++) v[i] = hilo[2 * i];
+    }
+    int rc = out.alloc(v.size() * sizeof(double));
+    if (rc) return rc;
+    KB_CUDA(cudaMemcpy(out.p, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice));
+    return KBSRC_GPU_OK;
+}
+
+int create_impl(const kbsrc_gpu_desc* desc, kbsrc_gpu_engine** out) {
+    int rc = check_desc(desc);
+    if (rc) return rc;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) {
+        cudaGetLastError();
+        return fail(KBSRC_GPU_E_NODEVICE, "no CUDA device");
+    }
+    if ((rc = allow_large_smem()) != KBSRC_GPU_OK) return rc;
+    auto* e = new kbsrc_gpu_engine();
+    struct Guard {
+        kbsrc_gpu_engine* p;
+        ~Guard() { delete p; }
+    } guard{e};
+    e->d = *desc;
+    e->d.H = nullptr;
+    e->exact = desc->precision == KBSRC_GPU_EXACT;
+    KB_CUDA(cudaGetDevice(&e->device));
+    e->Nb = (int)(desc->nb * desc->Q);
+    e->Mb = (int)(desc->nb * desc->P);
+    e->hf = e->Nb / 2;
+    e->hi = e->Mb / 2;
+    e->hop = desc->nb - 2 * desc->marg;
+    e->tasks = (long long)desc->channels * desc->nblk;
+    e->odd_dd = odd_roots<dd>();
+    e->odd_f64 = odd_roots<double>();
+    KB_CUDA(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
+    if ((rc = make_dev_cfft(e->hf, e->exact, e->fw)) != KBSRC_GPU_OK) return rc;
+    if ((rc = make_dev_cfft(e->hi, e->exact, e->iv)) != KBSRC_GPU_OK) return rc;
+    if ((rc = upload_cx(split_roots(e->Nb), e->exact, e->w_fw)) != KBSRC_GPU_OK) return rc;
+    if ((rc = upload_cx(split_roots(e->Mb), e->exact, e->w_iv)) != KBSRC_GPU_OK) return rc;
+    if ((rc = upload_real(desc->H, desc->H_len, e->exact, e->H)) != KBSRC_GPU_OK) return rc;
+    const size_t esize = e->exact ? 32 : 16;
+    const int fmax = env_int("KBSRC_GPU_FMAX", e->exact ? 4 : 8);
+    const HostCfft &f = e->fw.host, &v = e->iv.host;
+    if (f.four) {
+        e->col_fw = pick_shape(f.s1, f.N2, esize, fmax);
+        e->row_fw = pick_shape(f.s2, f.N1, esize, fmax);
+    } else {
+        e->dir_fw = direct_shape(f.sd, esize);
+    }
+    if (v.four) {
+        e->col_iv = pick_shape(v.s1, v.N2, esize, fmax);
+        e->row_iv = pick_shape(v.s2, v.N1, esize, fmax);
+    } else {
+        e->dir_iv = direct_shape(v.sd, esize);
+    }
+    // task slots: each holds max(h+1, h'+1) complex values, rounded to 8
+    e->stride = ((std::max(e->hf, e->hi) + 1 + 7) / 8) * 8;
+    const long long budget = (long long)env_int("KBSRC_GPU_WAVE_MB", 4096) << 20;
+    const long long per_task = 2 * e->stride * (long long)esize;
+    e->wave = std::max(1LL, std::min({e->tasks, budget / per_task, 65535LL}));
+    if (e->tasks > 0) {
+        if ((rc = e->bufA.alloc((size_t)(e->wave * e->stride * esize))) != KBSRC_GPU_OK) return rc;
+        if ((rc = e->bufB.alloc((size_t)(e->wave * e->stride * esize))) != KBSRC_GPU_OK) return rc;
+    }
+    guard.p = nullptr;
+    *out = e;
+    return KBSRC_GPU_OK;
+}
+
+int run_device_impl(kbsrc_gpu_engine* e, const double* in, const double* head, const double* tail, double* out,
+                    cudaStream_t st) {
+    const kbsrc_gpu_desc& d = e->d;
+    if (d.nout > 0) KB_CUDA(cudaMemsetAsync(out, 0, (size_t)d.nout * d.channels * sizeof(double), st));
+    if (e->tasks == 0 || d.nout == 0) return KBSRC_GPU_OK;
+    if (d.frames > 0 && !in) return fail(KBSRC_GPU_E_ARG, "null input");
+    if (d.edge_len > 0 && (!head || !tail)) return fail(KBSRC_GPU_E_ARG, "null edge buffers");
+    if (e->exact) return enqueue<ArDDShort, ArDDAccurate>(e, in, head, tail, out, st);
+    return enqueue<ArF64, ArF64>(e, in, head, tail, out, st);
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------------------------------------------
+// C ABI
+// ------------------------------------------------------------------------------------------------------
+extern "C" {
+
+int kbsrc_gpu_engine_create(const kbsrc_gpu_desc* desc, kbsrc_gpu_engine** out) {
+    if (!out) return fail(KBSRC_GPU_E_ARG, "null output pointer");
+    *out = nullptr;
+    try {
+        return create_impl(desc, out);
+    } catch (const std::bad_alloc&) {
+        return fail(KBSRC_GPU_E_NOMEM, "host allocation failed");
+    } catch (const std::exception& x) {
+        return fail(KBSRC_GPU_E_ARG, x.what());
+    }
+}
+
+int kbsrc_gpu_engine_run_device(kbsrc_gpu_engine* e, const double* d_in, const double* d_head, const double* d_tail,
+                                double* d_out, void* stream) {
+    if (!e) return fail(KBSRC_GPU_E_ARG, "null engine");
+    if (!d_out && e->d.nout > 0) return fail(KBSRC_GPU_E_ARG, "null output");
+    try {
+        return run_device_impl(e, d_in, d_head, d_tail, d_out, stream ? (cudaStream_t)stream : e->stream);
+    } catch (const std::exception& x) {
+        return fail(KBSRC_GPU_E_CUDA, x.what());
+    }
+}
+
+int kbsrc_gpu_engine_run_host(kbsrc_gpu_engine* e, const double* in, const double* head, const double* tail,
+                              double* out) {
+    if (!e) return fail(KBSRC_GPU_E_ARG, "null engine");
+    const kbsrc_gpu_desc& d = e->d;
+    if ((d.frames > 0 && !in) || (d.nout > 0 && !out) || (d.edge_len > 0 && (!head || !tail)))
+        return fail(KBSRC_GPU_E_ARG, "null buffer");
+    try {
+        int rc;
+        const size_t nin = (size_t)d.frames * d.channels, ne = (size_t)d.edge_len * d.channels,
+                     no = (size_t)d.nout * d.channels;
+        if (!e->d_in.p && (rc = e->d_in.alloc(nin * 8)) != KBSRC_GPU_OK) return rc;
+        if (!e->d_head.p && (rc = e->d_head.alloc(ne * 8)) != KBSRC_GPU_OK) return rc;
+        if (!e->d_tail.p && (rc = e->d_tail.alloc(ne * 8)) != KBSRC_GPU_OK) return rc;
+        if (!e->d_out.p && (rc = e->d_out.alloc(no * 8)) != KBSRC_GPU_OK) return rc;
+        cudaStream_t st = e->stream;
+        if (nin) KB_CUDA(cudaMemcpyAsync(e->d_in.p, in, nin * 8, cudaMemcpyHostToDevice, st));
+        if (ne) {
+            KB_CUDA(cudaMemcpyAsync(e->d_head.p, head, ne * 8, cudaMemcpyHostToDevice, st));
+            KB_CUDA(cudaMemcpyAsync(e->d_tail.p, tail, ne * 8, cudaMemcpyHostToDevice, st));
+        }
+        rc = run_device_impl(e, (const double*)e->d_in.p, (const double*)e->d_head.p, (const double*)e->d_tail.p,
+                             (double*)e->d_out.p, st);
+        if (rc) return rc;
+        if (no) KB_CUDA(cudaMemcpyAsync(out, e->d_out.p, no * 8, cudaMemcpyDeviceToHost, st));
+        KB_CUDA(cudaStreamSynchronize(st));
+        return KBSRC_GPU_OK;
+    } catch (const std::exception& x) {
+        return fail(KBSRC_GPU_E_CUDA, x.what());
+    }
+}
+
+int kbsrc_gpu_engine_info(const kbsrc_gpu_engine* e, long long* tasks, long long* launches, long long* device_bytes) {
+    if (!e) return fail(KBSRC_GPU_E_ARG, "null engine");
+    if (tasks) *tasks = e->tasks;
+    if (launches) {
+        long long per_wave = (e->fw.host.four ? 2 : 1) + 2 + (e->iv.host.four ? 2 : 1);
+        *launches = e->tasks ? per_wave * ((e->tasks + e->wave - 1) / e->wave) : 0;
+    }
+    if (device_bytes) {
+        *device_bytes = (long long)(e->fw.tw_stage.bytes + e->fw.tw4.bytes + e->iv.tw_stage.bytes + e->iv.tw4.bytes +
+                                    e->w_fw.bytes + e->w_iv.bytes + e->H.bytes + e->bufA.bytes + e->bufB.bytes +
+                                    e->d_in.bytes + e->d_head.bytes + e->d_tail.bytes + e->d_out.bytes);
+    }
+    return KBSRC_GPU_OK;
+}
+
+void kbsrc_gpu_engine_destroy(kbsrc_gpu_engine* e) { delete e; }
+
+int kbsrc_gpu_kernel_spectrum(const double* taps, int L, int n, double scale, double* H) {
+    if (!taps || !H || L < 0 || n < 2 || n % 2 || 2LL * L >= n)
+        return fail(KBSRC_GPU_E_ARG, "bad kernel spectrum arguments");
+    try {
+        int ndev = 0;
+        if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) {
+            cudaGetLastError();
+            return fail(KBSRC_GPU_E_NODEVICE, "no CUDA device");
+        }
+        int rc = allow_large_smem();
+        if (rc) return rc;
+        // the symmetric kernel placed circularly (design.cpp:42-43)
+        std::vector<double> r((size_t)2 * n, 0.0);
+        r[0] = taps[0];
+        r[1] = taps[1];
+        for (int m = 1; m <= L; m++) {
+            r[2 * (size_t)m] = taps[2 * m]; r[2 * (size_t)m + 1] = taps[2 * m + 1];
+            r[2 * (size_t)(n - m)] = taps[2 * m]; r[2 * (size_t)(n - m) + 1] = taps[2 * m + 1];
+        }
+        const int h = n / 2;
+        DevCfft c;
+        if ((rc = make_dev_cfft(h, true, c)) != KBSRC_GPU_OK) return rc;
+        DevBuf w, rin, A, B, Hd;
+        if ((rc = upload_cx(split_roots(n), true, w)) != KBSRC_GPU_OK) return rc;
+        if ((rc = rin.alloc(r.size() * 8)) != KBSRC_GPU_OK) return rc;
+        const size_t esize = 32;
+        if ((rc = A.alloc((size_t)(h + 1) * esize)) || (rc = B.alloc((size_t)(h + 1) * esize)) != KBSRC_GPU_OK) return rc;
+        if ((rc = Hd.alloc((size_t)(h + 1) * 16)) != KBSRC_GPU_OK) return rc;
+        cudaStream_t st = nullptr;
+        KB_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        struct StreamGuard {
+            cudaStream_t s;
+            ~StreamGuard() { cudaStreamDestroy(s); }
+        } sg{st};
+        KB_CUDA(cudaMemcpyAsync(rin.p, r.data(), r.size() * 8, cudaMemcpyHostToDevice, st));
+        using C = CxR<ArDDAccurate>;
+        const OddRoots<dd> odd = odd_roots<dd>();
+        PassParams<ArDDAccurate> p{};
+        p.tw_stage = static_cast<const CxW<ArDDAccurate>*>(c.tw_stage.p);
+        p.odd = odd;
+        p.ddreal = static_cast<const double*>(rin.p);
+        p.stride = 0;
+        if (c.host.four) {
+            const Shape sc = pick_shape(c.host.s1, c.host.N2, esize, 4), sr = pick_shape(c.host.s2, c.host.N1, esize, 4);
+            p.sp = c.host.s1; p.N1 = c.host.N1; p.N2 = c.host.N2; p.F = sc.F;
+            p.tw4 = static_cast<const CxW<ArDDAccurate>*>(c.tw4.p);
+            p.src = static_cast<C*>(A.p); p.dst = static_cast<C*>(A.p);
+            k_column<ArDDAccurate, kSrcDDReal><<<dim3((c.host.N2 + sc.F - 1) / sc.F, 1), sc.T, sc.smem, st>>>(p);
+            p.sp = c.host.s2; p.F = sr.F; p.src = static_cast<C*>(A.p); p.dst = static_cast<C*>(B.p);
+            k_row<ArDDAccurate, kDstComplex><<<dim3((c.host.N1 + sr.F - 1) / sr.F, 1), sr.T, sr.smem, st>>>(p);
+        } else {
+            const Shape sd = direct_shape(c.host.sd, esize);
+            p.sp = c.host.sd; p.F = 1; p.dst = static_cast<C*>(B.p);
+            k_direct<ArDDAccurate, kSrcDDReal, kDstComplex><<<dim3(1, 1), sd.T, sd.smem, st>>>(p);
+        }
+        SpecParams<ArDDAccurate> s{};
+        s.Z = static_cast<C*>(B.p); s.X = static_cast<C*>(A.p);
+        s.w_fw = static_cast<const CxW<ArDDAccurate>*>(w.p);
+        s.h = h; s.scale = scale; s.Hout = static_cast<dd*>(Hd.p);
+        k_split<ArDDAccurate><<<grid_for(h / 2 + 1, 256), 256, 0, st>>>(s);
+        k_design_out<<<grid_for(h + 1, 256), 256, 0, st>>>(s);
+        KB_CUDA(cudaGetLastError());
+        KB_CUDA(cudaMemcpyAsync(H, Hd.p, (size_t)(h + 1) * 16, cudaMemcpyDeviceToHost, st));
+        KB_CUDA(cudaStreamSynchronize(st));
+        return KBSRC_GPU_OK;
+    } catch (const std::bad_alloc&) {
+        return fail(KBSRC_GPU_E_NOMEM, "host allocation failed");
+    } catch (const std::exception& x) {
+        return fail(KBSRC_GPU_E_CUDA, x.what());
+    }
+}
+
+const char* kbsrc_gpu_last_error(void) { return g_error.c_str(); }
+
+const char* kbsrc_gpu_engine_name(void) { return "sm_100a"; }
+
+}  // extern "C"

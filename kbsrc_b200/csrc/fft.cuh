@@ -1,0 +1,142 @@
+// Mixed-radix Stockham DFT passes in shared memory.
+//
+// A CTA transforms F independent sequences of length n at once. Element j of sequence f lives at
+// smem[j*F + f], so consecutive threads (consecutive f) touch consecutive addresses. Each stage walks its
+// (f, butterfly) pairs in a block-stride loop and ping-pongs between two buffers.
+//
+// The butterflies and the stage/twiddle indexing are the reference's (HongYue1/KBSRC src/dsp/fft.hpp:62-151):
+// radix order 4s, 2s, then 3, 5, 7; stage twiddles skipped for p == 0; the odd-radix sums accumulated for
+// t = 1..H in that order. Rounding is part of the output definition, so none of this may be reordered.
+#pragma once
+#include "dd.cuh"
+
+namespace kbsrc::dev {
+
+constexpr int kMaxStages = 16;
+
+struct Stage {
+    int r, m, s;  // radix, butterflies per (p) group count m = n_left/r, output stride s
+    int tw;       // offset of this stage's twiddles (complex table entries), laid out [p*(r-1) + u-1]
+};
+struct SubPlan {
+    int n, nst;
+    Stage st[kMaxStages];
+};
+
+// cos / sin of 2 pi k / r for r = 3, 5, 7 (rows 0, 1, 2)
+template <class W>
+struct OddRoots {
+    W c[3][7], s[3][7];
+};
+
+template <class W>
+__device__ __forceinline__ cx<W> ld_tw(const cx<W>* p);
+template <>
+__device__ __forceinline__ cx<double> ld_tw<double>(const cx<double>* p) {
+    const double2 a = __ldg(reinterpret_cast<const double2*>(p));
+    return cx<double>{a.x, a.y};
+}
+template <>
+__device__ __forceinline__ cx<dd> ld_tw<dd>(const cx<dd>* p) {
+    const double2* q = reinterpret_cast<const double2*>(p);
+    const double2 a = __ldg(q), b = __ldg(q + 1);
+    return cx<dd>{dd{a.x, a.y}, dd{b.x, b.y}};
+}
+
+template <class Ar>
+__device__ __forceinline__ void bfly2(const CxR<Ar>* src, int sin, CxR<Ar>* dst, int sout, const CxW<Ar>* tw,
+                                      bool p0) {
+    const CxR<Ar> a0 = src[0], a1 = src[sin];
+    dst[0] = c_add<Ar>(a0, a1);
+    dst[sout] = p0 ? c_sub<Ar>(a0, a1) : c_mulw<Ar>(c_sub<Ar>(a0, a1), ld_tw(tw));
+}
+
+template <class Ar>
+__device__ __forceinline__ void bfly4(const CxR<Ar>* src, int sin, CxR<Ar>* dst, int sout, const CxW<Ar>* tw,
+                                      bool p0) {
+    using C = CxR<Ar>;
+    const C a0 = src[0], a1 = src[sin], a2 = src[2 * sin], a3 = src[3 * sin];
+    const C t0 = c_add<Ar>(a0, a2), t1 = c_sub<Ar>(a0, a2), t2 = c_add<Ar>(a1, a3);
+    const C t3 = c_mul_mi<Ar>(c_sub<Ar>(a1, a3));
+    dst[0] = c_add<Ar>(t0, t2);
+    if (p0) {
+        dst[sout] = c_add<Ar>(t1, t3);
+        dst[2 * sout] = c_sub<Ar>(t0, t2);
+        dst[3 * sout] = c_sub<Ar>(t1, t3);
+    } else {
+        dst[sout] = c_mulw<Ar>(c_add<Ar>(t1, t3), ld_tw(tw));
+        dst[2 * sout] = c_mulw<Ar>(c_sub<Ar>(t0, t2), ld_tw(tw + 1));
+        dst[3 * sout] = c_mulw<Ar>(c_sub<Ar>(t1, t3), ld_tw(tw + 2));
+    }
+}
+
+// Odd radix R: x_u = a0 + sum_t S_t cos(2pi tu/R) -/+ i sum_t D_t sin(2pi tu/R) (fft.hpp:62-84)
+template <class Ar, int R>
+__device__ __forceinline__ void bfly_odd(const CxR<Ar>* src, int sin, CxR<Ar>* dst, int sout, const CxW<Ar>* tw,
+                                         bool p0, const typename Ar::W* cr, const typename Ar::W* sr) {
+    using C = CxR<Ar>;
+    constexpr int H = (R - 1) / 2;
+    const C a0 = src[0];
+    C S[H], Df[H];
+#pragma unroll
+    for (int t = 1; t <= H; t++) {
+        const C x = src[t * sin], y = src[(R - t) * sin];
+        S[t - 1] = c_add<Ar>(x, y);
+        Df[t - 1] = c_sub<Ar>(x, y);
+    }
+    C sum = a0;
+#pragma unroll
+    for (int t = 0; t < H; t++) sum = c_add<Ar>(sum, S[t]);
+    dst[0] = sum;
+#pragma unroll
+    for (int u = 1; u <= H; u++) {
+        C A = a0, B = {Ar::zero(), Ar::zero()};
+#pragma unroll
+        for (int t = 1; t <= H; t++) {
+            const int m = (t * u) % R;
+            const typename Ar::R c = Ar::from_w(cr[m]), sn = Ar::from_w(sr[m]);
+            A = {Ar::add(A.re, Ar::mul(S[t - 1].re, c)), Ar::add(A.im, Ar::mul(S[t - 1].im, c))};
+            B = {Ar::add(B.re, Ar::mul(Df[t - 1].re, sn)), Ar::add(B.im, Ar::mul(Df[t - 1].im, sn))};
+        }
+        const C xu = {Ar::add(A.re, B.im), Ar::sub(A.im, B.re)};
+        const C xr = {Ar::sub(A.re, B.im), Ar::add(A.im, B.re)};
+        if (p0) {
+            dst[u * sout] = xu;
+            dst[(R - u) * sout] = xr;
+        } else {
+            dst[u * sout] = c_mulw<Ar>(xu, ld_tw(tw + u - 1));
+            dst[(R - u) * sout] = c_mulw<Ar>(xr, ld_tw(tw + R - u - 1));
+        }
+    }
+}
+
+// Runs every stage of `sp` on F sequences held in `a` (layout [j*F + f]); `b` is the other buffer.
+// Returns the buffer that holds the result. Ends with the CTA synchronised.
+template <class Ar>
+__device__ CxR<Ar>* stockham(const SubPlan& sp, CxR<Ar>* a, CxR<Ar>* b, int F, const CxW<Ar>* __restrict__ tw,
+                             const OddRoots<typename Ar::W>& odd) {
+    for (int g = 0; g < sp.nst; g++) {
+        const int r = sp.st[g].r, m = sp.st[g].m, s = sp.st[g].s;
+        const CxW<Ar>* twg = tw + sp.st[g].tw;
+        const int total = m * s * F, sin = s * m * F, sout = s * F;
+        for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
+            const int f = idx % F, bf = idx / F, q = bf % s, p = bf / s;
+            const CxR<Ar>* src = a + (s * p + q) * F + f;
+            CxR<Ar>* dst = b + (s * r * p + q) * F + f;
+            const CxW<Ar>* t = twg + p * (r - 1);
+            const bool p0 = p == 0;
+            if (r == 4) bfly4<Ar>(src, sin, dst, sout, t, p0);
+            else if (r == 2) bfly2<Ar>(src, sin, dst, sout, t, p0);
+            else if (r == 3) bfly_odd<Ar, 3>(src, sin, dst, sout, t, p0, odd.c[0], odd.s[0]);
+            else if (r == 5) bfly_odd<Ar, 5>(src, sin, dst, sout, t, p0, odd.c[1], odd.s[1]);
+            else bfly_odd<Ar, 7>(src, sin, dst, sout, t, p0, odd.c[2], odd.s[2]);
+        }
+        __syncthreads();
+        CxR<Ar>* t = a;
+        a = b;
+        b = t;
+    }
+    return a;
+}
+
+}  // namespace kbsrc::dev

@@ -1,0 +1,573 @@
+// Host side of the converter: argument checks, block planning, Burg LPC edges, Kaiser taps, and the calls into
+// the GPU engine through the C ABI (include/kbsrc_gpu.h). Replaces HongYue1/KBSRC src/resampler.cpp:92-228
+// (resample_impl), src/design.cpp:17-37 (kernel_taps), src/lpc.cpp:13-42 (burg_extrap) and src/dispatch.cpp
+// (the round-to-nearest guard). The block loop itself (resampler.cpp:34-88) runs on the GPU.
+//
+// Block planning, tap values and LPC edges are part of the output definition: the integer formulas, the
+// double-double operation order and the 16-task shrink rule are the reference's, so the engine sees the
+// same blocks and kernel and the output is byte-identical.
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <climits>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <numeric>
+#include <stdexcept>
+#include <string>
+#include <thread>
+#include <vector>
+#if defined(__x86_64__) || defined(__i386__)
+#include <xmmintrin.h>
+#else
+#include <cfenv>
+#endif
+
+#include "ddh.hpp"
+#include "kbsrc/kbsrc.hpp"
+#include "kbsrc/kbsrc_c.h"
+#include "kbsrc_gpu.h"
+
+#ifndef KBSRC_VERSION
+#define KBSRC_VERSION "1.3.0-b200"
+#endif
+
+namespace kbsrc {
+namespace {
+
+using host::dd;
+
+double now() { return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count(); }
+
+// Runs Exact's host arithmetic in round-to-nearest and restores the caller's rounding mode on exit; only the
+// SSE rounding-control bits are touched on x86 (the reference's dispatch.cpp:37-67 contract).
+class RoundToNearest {
+public:
+    explicit RoundToNearest(bool on) {
+        if (!on) return;
+#if defined(__x86_64__) || defined(__i386__)
+        saved_ = _mm_getcsr() & kRC;
+        if (saved_) _mm_setcsr(_mm_getcsr() & ~kRC);
+#else
+        const int m = std::fegetround();
+        if (m >= 0 && m != FE_TONEAREST && std::fesetround(FE_TONEAREST) == 0) saved_ = m;
+#endif
+    }
+    ~RoundToNearest() {
+#if defined(__x86_64__) || defined(__i386__)
+        if (saved_) _mm_setcsr((_mm_getcsr() & ~kRC) | saved_);
+#else
+        if (saved_ != kNone) std::fesetround(saved_);
+#endif
+    }
+    RoundToNearest(const RoundToNearest&) = delete;
+    RoundToNearest& operator=(const RoundToNearest&) = delete;
+
+private:
+#if defined(__x86_64__) || defined(__i386__)
+    static constexpr unsigned kRC = 0x6000;
+    unsigned saved_ = 0;
+#else
+    static constexpr int kNone = -1;
+    int saved_ = kNone;
+#endif
+};
+
+// Runs body(i) for i in [0, n) on up to `threads` threads, each taking indices from a shared counter.
+template <class F>
+void parallel_for(int threads, long long n, long long chunk, F body) {
+    std::atomic<long long> next(0);
+    auto work = [&] {
+        for (long long c; (c = next.fetch_add(chunk)) < n;)
+            for (long long i = c; i < std::min(n, c + chunk); i++) body(i);
+    };
+    threads = (int)std::max<long long>(1, std::min<long long>(threads, (n + chunk - 1) / chunk));
+    std::vector<std::thread> pool;
+    try {
+        for (int t = 1; t < threads; t++) pool.emplace_back(work);
+    } catch (...) {
+        // fewer threads: the ones started and this one share the work
+    }
+    work();
+    for (auto& t : pool) t.join();
+}
+
+bool block_ok(int v, bool avoid7) { return v % 2 == 0 && host::smooth7(v / 2) && !(avoid7 && (v / 2) % 7 == 0); }
+
+// The overlap-save plan of one conversion (resampler.cpp:98-209).
+struct Plan {
+    long long P = 0, Q = 0, nout = 0, Lk = 0, E = 0, pre = 0, nblk = 0, base = 0, c2 = 0, fk = 0, mn = 0;
+    long long fi = 0, fo = 0;
+    int nb = 0, marg = 0, hop = 0;
+    bool up = false, general = false, copy = false;
+    double fml = 0;
+};
+
+Plan make_plan(const double* in, long long frames, int ch, int rate_in, int rate_out, const Options& opt) {
+    if (ch < 1 || frames < 0 || (frames > 0 && !in)) throw std::invalid_argument("bad input buffer");
+    if (rate_in < 1 || rate_out < 1) throw std::invalid_argument("sample rates must be positive");
+    if (!(opt.length > 0 && opt.length <= 10) || !(opt.beta > 0 && opt.beta <= 200) || opt.threads < 0 ||
+        opt.block < 0)
+        throw std::invalid_argument("option out of range");
+    Plan pl;
+    pl.fi = rate_in;
+    pl.fo = rate_out;
+    const long long g = std::gcd(pl.fi, pl.fo);
+    pl.P = pl.fo / g;
+    pl.Q = pl.fi / g;
+    pl.up = pl.fo > pl.fi;
+    const long long cap = LLONG_MAX / 16;
+    const __int128 n128 = ((__int128)frames * pl.P + pl.Q - 1) / pl.Q;
+    if (frames > cap || n128 > cap) throw std::invalid_argument("input too long");
+    pl.nout = (long long)n128;
+    if (pl.fo == pl.fi) {
+        pl.copy = true;
+        return pl;
+    }
+    const long long P = pl.P, Q = pl.Q;
+    pl.fk = pl.up ? pl.fo : pl.fi;
+    pl.mn = std::min(pl.fi, pl.fo);
+    const double lk = std::floor(opt.length * (double)pl.fk);
+    if (!(lk >= 1 && lk <= INT_MAX)) throw std::invalid_argument("option out of range");
+    pl.Lk = (long long)lk;
+    // transition band 2*fml wide; its top edge must fit below the lower Nyquist frequency
+    pl.fml = std::sqrt(opt.beta * opt.beta + 9.8696044010893586) / (2 * 3.14159265358979323846 * opt.length);
+    const double drop = std::ceil(2 * pl.fml);
+    if (!((double)pl.mn - drop > 2 * pl.fml)) throw std::invalid_argument("length too short for these sample rates");
+    pl.c2 = pl.mn - (long long)drop;
+    const long long reach = (pl.Lk * pl.fi + pl.fk - 1) / pl.fk + 1;
+    const long long margl = std::max((reach + Q + Q - 1) / Q, pl.up ? (pl.Lk + P + P - 1) / P : 0LL);
+    if ((opt.block ? opt.block : 10 * margl) > INT_MAX / 2 / std::max(P, Q))
+        throw std::invalid_argument("block, rates or length too large");
+    pl.E = reach + Q;
+    pl.pre = (pl.E + 64 + Q - 1) / Q * Q;
+    const long long span = pl.pre + frames + pl.E + 64;
+    // Fast's automatic block: about 51200 points in the larger transform, 4..10 margins, no factor 7
+    const bool fast_auto = !opt.block && opt.precision == Precision::Fast;
+    auto next_block = [](int v, bool avoid7) {
+        while (!block_ok(v, avoid7)) v++;
+        return v;
+    };
+    int nb = opt.block ? next_block(opt.block, false)
+                       : next_block((int)(fast_auto ? std::clamp(51200 / std::max(P, Q), 4 * margl, 10 * margl)
+                                                    : 10 * margl),
+                                    fast_auto);
+    if (nb <= 2 * margl) throw std::invalid_argument("option out of range");
+    const int marg = (int)margl;
+    // Short inputs: smaller blocks until there are at least 16 quarter-block task groups. Machine-independent
+    // by design, since the block size sets the rounding.
+    while (!opt.block && nb > 4 * marg) {
+        const long long hq = (long long)(nb - 2 * marg) * Q;
+        const long long nbk = (span + hq - 1) / hq;
+        if ((long long)ch * ((nbk + 3) / 4) >= 16) break;
+        const int nn = next_block(std::max(4 * marg, nb * 3 / 4), fast_auto);
+        if (nn >= nb) break;
+        nb = nn;
+    }
+    pl.nb = nb;
+    pl.marg = marg;
+    pl.hop = nb - 2 * marg;
+    pl.nblk = (span + (long long)pl.hop * Q - 1) / ((long long)pl.hop * Q);
+    pl.base = (long long)marg * Q;
+    pl.general = (double)(std::max(pl.fi, pl.fo) - pl.mn) / 2 < 3 * pl.fml;
+    return pl;
+}
+
+// One-sided Kaiser-windowed sinc taps h[0..L], relative cutoff a/b, in dd (design.cpp:17-37). The sinc
+// argument is reduced exactly: sin(pi n a/b) from the root e^{2 pi i (n a mod 2b) / 2b}.
+std::vector<dd> kaiser_taps(int L, long long a, long long b, double beta, int threads) {
+    std::vector<dd> h((size_t)L + 1);
+    const dd i0b = host::bessel_i0(dd(beta)), ab = dd((double)a) / (double)b;
+    parallel_for(threads, (long long)L + 1, 256, [&](long long n) {
+        dd s(1.0);
+        if (n) {
+            const long long m = (long long)(((__int128)n * a) % (2 * (__int128)b));
+            dd c, sn;
+            host::unit_root(m, 2 * b, c, sn);
+            s = sn / (host::kPi * (dd((double)n) * (double)a) / (double)b);
+        }
+        const dd u = dd((double)n) / (double)L;
+        const dd w = host::bessel_i0(dd(beta) * host::sqrt_dd(dd(1.0) - u * u)) / i0b;
+        h[n] = ab * s * w;
+    });
+    return h;
+}
+
+// Burg LPC (order 32, trained on the last 4096 samples) predicting n samples after x[0..len) (lpc.cpp:13-42).
+// Zeros when the segment is too short, silent, or the prediction leaves 4x the segment's peak.
+std::vector<double> burg_predict(const double* x, long long len, long long n) {
+    constexpr int order = 32, train = 4096;
+    std::vector<double> out((size_t)n, 0.0);
+    const long long m = std::min<long long>(len, train);
+    const double* seg = x + len - m;
+    if (m < 2 * order + 8) return out;
+    bool nonzero = false;
+    double peak = 0;
+    for (long long i = 0; i < m; i++) {
+        nonzero |= seg[i] != 0;
+        peak = std::max(peak, std::fabs(seg[i]));
+    }
+    if (!nonzero) return out;
+    std::vector<dd> fw(seg + 1, seg + m), bw(seg, seg + m - 1), a{dd(1.0)};
+    for (int it = 0; it < order; it++) {
+        dd num(0.0), den(0.0);
+        for (size_t i = 0; i < fw.size(); i++) {
+            num = num + fw[i] * bw[i];
+            den = den + (fw[i] * fw[i] + bw[i] * bw[i]);
+        }
+        if (den.hi <= 0) break;
+        const dd k = -(num * 2.0) / den;
+        a.push_back(dd(0.0));
+        const std::vector<dd> rev(a.rbegin(), a.rend());
+        for (size_t i = 0; i < a.size(); i++) a[i] = a[i] + k * rev[i];
+        for (size_t i = 0; i + 1 < fw.size(); i++) {  // in place: reads i and i+1 before they change
+            const dd f2 = fw[i + 1] + k * bw[i + 1], b2 = bw[i] + k * fw[i];
+            fw[i] = f2;
+            bw[i] = b2;
+        }
+        fw.pop_back();
+        bw.pop_back();
+    }
+    const int p = (int)a.size() - 1;
+    std::vector<double> c(p), buf((size_t)(p + n));
+    for (int i = 0; i < p; i++) c[i] = -(a[p - i].hi + a[p - i].lo);
+    for (int i = 0; i < p; i++) buf[i] = seg[m - p + i];
+    for (long long i = 0; i < n; i++) {
+        double s = 0;
+        for (int j = 0; j < p; j++) s += c[j] * buf[i + j];
+        buf[p + i] = s;
+    }
+    const double lim = 4 * peak;
+    for (long long i = 0; i < n; i++)
+        if (!std::isfinite(buf[p + i]) || std::fabs(buf[p + i]) > lim) return out;
+    std::copy(buf.begin() + p, buf.end(), out.begin());
+    return out;
+}
+
+void gpu_check(int rc, const char* what) {
+    if (rc == KBSRC_GPU_OK) return;
+    if (rc == KBSRC_GPU_E_NOMEM) throw std::bad_alloc();
+    throw std::runtime_error(std::string(what) + ": " + kbsrc_gpu_last_error());
+}
+
+struct EngineHandle {
+    kbsrc_gpu_engine* e = nullptr;
+    EngineHandle() = default;
+    EngineHandle(const EngineHandle&) = delete;
+    EngineHandle& operator=(const EngineHandle&) = delete;
+    ~EngineHandle() { kbsrc_gpu_engine_destroy(e); }
+};
+
+// A planned conversion: everything but the block loop, ready to run on new input of the same shape.
+struct Conversion {
+    Plan pl;
+    Options opt;
+    int ch = 0;
+    long long frames = 0;
+    std::vector<double> head, tail;  // LPC edges, ch * ext each
+    long long ext = 0;
+    EngineHandle eng;
+    double design_seconds = 0;
+};
+
+std::unique_ptr<Conversion> prepare(const double* in, long long frames, int ch, int rate_in, int rate_out,
+                                    const Options& opt) {
+    auto cv = std::make_unique<Conversion>();
+    cv->pl = make_plan(in, frames, ch, rate_in, rate_out, opt);
+    cv->opt = opt;
+    cv->ch = ch;
+    cv->frames = frames;
+    const Plan& pl = cv->pl;
+    if (pl.copy) return cv;
+    if (opt.precision == Precision::LongDouble)
+        throw std::runtime_error("mode ld (x87 long double) is not available on the GPU engine");
+    if (pl.general) throw std::runtime_error("near-unity ratios (general fold) are not available on the GPU engine");
+    const double t0 = now();
+    const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
+    const int threads = opt.threads ? opt.threads : std::min(hw, 8);
+    const long long Q = pl.Q, P = pl.P, Nb = (long long)pl.nb * Q, Mb = (long long)pl.nb * P;
+    // LPC edges: the tail predicted from the last 4096 samples, the head from the first 4096 reversed, each
+    // faded out over its last 32 samples (resampler.cpp:168-186)
+    const long long ext = opt.lpc_edges ? pl.E + 32 : 0;
+    cv->ext = ext;
+    cv->head.assign((size_t)(ext * ch), 0.0);
+    cv->tail.assign((size_t)(ext * ch), 0.0);
+    if (ext) {
+        double fade[32];
+        for (int i = 0; i < 32; i++) {
+            dd co, sn;
+            host::unit_root(i, 64, co, sn);
+            fade[i] = ((dd(1.0) + co) * 0.5).hi;
+        }
+        parallel_for(threads, 2LL * ch, 1, [&](long long job) {
+            const int c = (int)(job / 2);
+            const long long m = std::min<long long>(frames, 4096);
+            std::vector<double> seg((size_t)m);
+            if (job % 2 == 0)  // tail: the channel's last m samples in order
+                for (long long i = 0; i < m; i++) seg[i] = in[(frames - m + i) * ch + c];
+            else  // head: the first m samples reversed
+                for (long long i = 0; i < m; i++) seg[i] = in[(m - 1 - i) * ch + c];
+            std::vector<double> pred = burg_predict(seg.data(), m, ext);
+            for (int i = 0; i < 32; i++) pred[ext - 32 + i] *= fade[i];
+            std::copy(pred.begin(), pred.end(), (job % 2 == 0 ? cv->tail : cv->head).begin() + c * ext);
+        });
+    }
+    // kernel: taps on the host, spectrum on the GPU (design.cpp:40-49)
+    const long long gc = std::gcd(pl.c2, pl.fk);
+    const std::vector<dd> taps = kaiser_taps((int)pl.Lk, pl.c2 / gc, pl.fk / gc, opt.beta, threads);
+    const int nspec = (int)(pl.up ? Mb : Nb);
+    std::vector<double> H((size_t)(nspec / 2 + 1) * 2);
+    gpu_check(kbsrc_gpu_kernel_spectrum(reinterpret_cast<const double*>(taps.data()), (int)pl.Lk, nspec, (double)Nb,
+                                        H.data()),
+              "kernel spectrum");
+    kbsrc_gpu_desc d{};
+    d.precision = opt.precision == Precision::Fast ? KBSRC_GPU_FAST : KBSRC_GPU_EXACT;
+    d.channels = ch;
+    d.P = P;
+    d.Q = Q;
+    d.nb = pl.nb;
+    d.marg = pl.marg;
+    d.nblk = pl.nblk;
+    d.lead = pl.base + pl.pre;
+    d.o = pl.pre / Q * P;
+    d.frames = frames;
+    d.nout = pl.nout;
+    d.up = pl.up;
+    d.Jg = 0;
+    d.edge_len = ext;
+    d.H = H.data();
+    d.H_len = (long long)H.size() / 2;
+    gpu_check(kbsrc_gpu_engine_create(&d, &cv->eng.e), "GPU engine");
+    cv->design_seconds = now() - t0;
+    return cv;
+}
+
+void fill_stats(const Conversion& cv, Stats* stats, double process_seconds) {
+    if (!stats) return;
+    const Plan& pl = cv.pl;
+    stats->p = pl.P;
+    stats->q = pl.Q;
+    if (pl.copy) {
+        stats->isa = "generic";
+        stats->threads = 1;
+        return;
+    }
+    stats->isa = kbsrc_gpu_engine_name();
+    stats->taps = 2 * pl.Lk + 1;
+    stats->block = pl.nb;
+    stats->threads = 1;
+    stats->general_fold = false;
+    stats->design_seconds = cv.design_seconds;
+    stats->process_seconds = process_seconds;
+    stats->passband = (double)pl.c2 / 2 - pl.fml;
+    stats->stopband = (double)pl.c2 / 2 + pl.fml;
+}
+
+// Runs a prepared conversion on input of its shape; out: planar ch * nout.
+void run_conversion(Conversion& cv, const double* in, double* out) {
+    const Plan& pl = cv.pl;
+    if (pl.copy) {
+        for (int c = 0; c < cv.ch; c++)
+            for (long long i = 0; i < cv.frames; i++) out[c * pl.nout + i] = in[i * cv.ch + c];
+        return;
+    }
+    gpu_check(kbsrc_gpu_engine_run_host(cv.eng.e, in, cv.head.data(), cv.tail.data(), out), "GPU engine");
+}
+
+std::vector<std::vector<double>> resample_gpu(const double* in, long long frames, int ch, int rate_in, int rate_out,
+                                              const Options& opt, Stats* stats) {
+    auto cv = prepare(in, frames, ch, rate_in, rate_out, opt);
+    const double t1 = now();
+    const long long nout = cv->pl.nout;
+    std::vector<double> planar((size_t)(nout * ch));
+    run_conversion(*cv, in, planar.data());
+    std::vector<std::vector<double>> out(ch);
+    for (int c = 0; c < ch; c++) out[c].assign(planar.begin() + c * nout, planar.begin() + (c + 1) * nout);
+    fill_stats(*cv, stats, now() - t1);
+    return out;
+}
+
+}  // namespace
+
+std::vector<std::vector<double>> resample(const double* in, long long frames, int channels, int rate_in, int rate_out,
+                                          const Options& opt, Stats* stats) {
+    RoundToNearest rn(opt.precision == Precision::Exact);
+    return resample_gpu(in, frames, channels, rate_in, rate_out, opt, stats);
+}
+
+const char* version() { return KBSRC_VERSION; }
+
+}  // namespace kbsrc
+
+// ---- C form -----------------------------------------------------------------------------------------------
+namespace {
+long long report(const char* msg, long long code, char* err, int err_len) {
+    if (err && err_len > 0) {
+        std::strncpy(err, msg, (size_t)err_len - 1);
+        err[err_len - 1] = 0;
+    }
+    return code;
+}
+}  // namespace
+
+extern "C" long long kbsrc_output_frames(long long frames, int rate_in, int rate_out) {
+    if (frames < 0 || rate_in < 1 || rate_out < 1) return -1;
+    const long long g = std::gcd((long long)rate_in, (long long)rate_out), P = rate_out / g, Q = rate_in / g;
+    const __int128 n = ((__int128)frames * P + Q - 1) / Q;
+    return n > LLONG_MAX / 16 ? -1 : (long long)n;
+}
+
+extern "C" long long kbsrc_resample_c(const double* in, long long frames, int channels, int rate_in, int rate_out,
+                                      const kbsrc_options_c* copt, double* out, long long out_cap,
+                                      kbsrc_stats_c* cst, char* err, int err_len) {
+    try {
+        kbsrc::Options o;
+        if (copt) {
+            o.precision = copt->precision == 0   ? kbsrc::Precision::Fast
+                          : copt->precision == 2 ? kbsrc::Precision::LongDouble
+                                                 : kbsrc::Precision::Exact;
+            o.length = copt->length;
+            o.beta = copt->beta;
+            o.threads = copt->threads;
+            o.block = copt->block;
+            o.lpc_edges = copt->lpc_edges != 0;
+        }
+        kbsrc::Stats st;
+        auto y = kbsrc::resample(in, frames, channels, rate_in, rate_out, o, &st);
+        const long long n = y.empty() ? 0 : (long long)y[0].size();
+        if (n > out_cap || (n > 0 && !out)) return report("output buffer too small", -2, err, err_len);
+        for (int c = 0; c < channels; c++)
+            if (n) std::memcpy(out + (size_t)c * out_cap, y[c].data(), (size_t)n * sizeof(double));
+        if (cst) {
+            cst->p = st.p; cst->q = st.q; cst->taps = st.taps; cst->block = st.block; cst->threads = st.threads;
+            cst->general_fold = st.general_fold; cst->design_seconds = st.design_seconds;
+            cst->process_seconds = st.process_seconds; cst->passband = st.passband; cst->stopband = st.stopband;
+            cst->isa = st.isa;
+        }
+        return n;
+    } catch (const std::invalid_argument& x) {
+        return report(x.what(), -1, err, err_len);
+    } catch (const std::bad_alloc&) {
+        return report("out of memory", -4, err, err_len);
+    } catch (const std::exception& x) {
+        return report(x.what(), -3, err, err_len);
+    }
+}
+
+extern "C" const char* kbsrc_version_c(void) { return kbsrc::version(); }
+
+namespace {
+kbsrc::Options options_from_c(const kbsrc_options_c* copt) {
+    kbsrc::Options o;
+    if (copt) {
+        o.precision = copt->precision == 0   ? kbsrc::Precision::Fast
+                      : copt->precision == 2 ? kbsrc::Precision::LongDouble
+                                             : kbsrc::Precision::Exact;
+        o.length = copt->length;
+        o.beta = copt->beta;
+        o.threads = copt->threads;
+        o.block = copt->block;
+        o.lpc_edges = copt->lpc_edges != 0;
+    }
+    return o;
+}
+}  // namespace
+
+extern "C" int kbsrc_prepare_c(const double* in, long long frames, int channels, int rate_in, int rate_out,
+                               const kbsrc_options_c* copt, kbsrc_conversion** out, char* err, int err_len) {
+    if (!out) return (int)report("null output pointer", -1, err, err_len);
+    *out = nullptr;
+    try {
+        const kbsrc::Options o = options_from_c(copt);
+        kbsrc::RoundToNearest rn(o.precision == kbsrc::Precision::Exact);
+        *out = reinterpret_cast<kbsrc_conversion*>(kbsrc::prepare(in, frames, channels, rate_in, rate_out, o).release());
+        return 0;
+    } catch (const std::invalid_argument& x) {
+        return (int)report(x.what(), -1, err, err_len);
+    } catch (const std::bad_alloc&) {
+        return (int)report("out of memory", -4, err, err_len);
+    } catch (const std::exception& x) {
+        return (int)report(x.what(), -3, err, err_len);
+    }
+}
+
+extern "C" int kbsrc_conversion_run_c(kbsrc_conversion* cv, const double* in, double* out, char* err, int err_len) {
+    if (!cv) return (int)report("null conversion", -1, err, err_len);
+    try {
+        kbsrc::run_conversion(*reinterpret_cast<kbsrc::Conversion*>(cv), in, out);
+        return 0;
+    } catch (const std::bad_alloc&) {
+        return (int)report("out of memory", -4, err, err_len);
+    } catch (const std::exception& x) {
+        return (int)report(x.what(), -3, err, err_len);
+    }
+}
+
+extern "C" int kbsrc_conversion_info_c(const kbsrc_conversion* cvp, long long* nout, long long* edge_len,
+                                       const double** head, const double** tail, kbsrc_gpu_engine** engine,
+                                       kbsrc_stats_c* st) {
+    if (!cvp) return -1;
+    const auto& cv = *reinterpret_cast<const kbsrc::Conversion*>(cvp);
+    if (nout) *nout = cv.pl.nout;
+    if (edge_len) *edge_len = cv.ext;
+    if (head) *head = cv.head.data();
+    if (tail) *tail = cv.tail.data();
+    if (engine) *engine = cv.eng.e;
+    if (st) {
+        kbsrc::Stats s;
+        kbsrc::fill_stats(cv, &s, 0);
+        st->p = s.p; st->q = s.q; st->taps = s.taps; st->block = s.block; st->threads = s.threads;
+        st->general_fold = s.general_fold; st->design_seconds = s.design_seconds; st->process_seconds = 0;
+        st->passband = s.passband; st->stopband = s.stopband; st->isa = s.isa;
+    }
+    return 0;
+}
+
+extern "C" void kbsrc_conversion_free_c(kbsrc_conversion* cv) { delete reinterpret_cast<kbsrc::Conversion*>(cv); }
+
+// ---- diagnostics: the host-side pieces on their own ---------------------------------------------------------
+
+// Block plan: info[16] = P Q taps nb marg hop nblk Nb Mb pre o E lead general up nout. Returns 0, 1 (equal rates)
+// or -1 (invalid argument, message in err).
+extern "C" int kbsrc_plan_c(long long frames, int channels, int rate_in, int rate_out, const kbsrc_options_c* copt,
+                            long long* info, char* err, int err_len) {
+    try {
+        static const double dummy = 0;
+        const kbsrc::Options o = options_from_c(copt);
+        const kbsrc::Plan pl = kbsrc::make_plan(frames ? &dummy : nullptr, frames, channels, rate_in, rate_out, o);
+        const long long v[16] = {pl.P, pl.Q, 2 * pl.Lk + 1, pl.nb, pl.marg, pl.hop, pl.nblk, (long long)pl.nb * pl.Q,
+                                 (long long)pl.nb * pl.P, pl.pre, pl.Q ? pl.pre / pl.Q * pl.P : 0, pl.E,
+                                 pl.base + pl.pre, pl.general, pl.up, pl.nout};
+        if (info) std::memcpy(info, v, sizeof v);
+        return pl.copy ? 1 : 0;
+    } catch (const std::exception& x) {
+        return (int)report(x.what(), -1, err, err_len);
+    }
+}
+
+// Kaiser taps h[0..L] as (hi, lo) pairs (2L+2 doubles)
+extern "C" int kbsrc_kernel_taps_c(int L, long long a, long long b, double beta, int threads, double* out) {
+    if (L < 1 || a < 1 || b < 1 || !out) return -1;
+    try {
+        kbsrc::RoundToNearest rn(true);
+        const auto h = kbsrc::kaiser_taps(L, a, b, beta, threads < 1 ? 1 : threads);
+        std::memcpy(out, h.data(), h.size() * sizeof(kbsrc::host::dd));
+        return 0;
+    } catch (...) {
+        return -4;
+    }
+}
+
+// Burg LPC prediction of n samples following x[0..len)
+extern "C" int kbsrc_burg_c(const double* x, long long len, long long n, double* out) {
+    if (len < 0 || n < 0 || (len > 0 && !x) || (n > 0 && !out)) return -1;
+    try {
+        kbsrc::RoundToNearest rn(true);
+        const auto p = kbsrc::burg_predict(x, len, n);
+        std::copy(p.begin(), p.end(), out);
+        return 0;
+    } catch (...) {
+        return -4;
+    }
+}

@@ -1,0 +1,27 @@
+// WAV reading and writing for the kbsrc command-line tool (PCM 8/16/24/32, IEEE float 32/64,
+// WAVE_FORMAT_EXTENSIBLE). Same formats, header layout and error messages as HongYue1/KBSRC src/io/wav.hpp,
+// since the tool's output file is compared byte for byte.
+#pragma once
+
+#include <string>
+#include <vector>
+
+namespace kbsrc::io {
+
+struct Audio {
+    int rate = 0, ch = 0;
+    long long frames = 0;
+    std::vector<double> d;  // interleaved
+    int fmt_bits = 0;
+    bool fmt_float = false;
+};
+
+Audio read_wav(const char* path);
+// Fails when a WAV header in `format` cannot describe ch channels at this rate.
+void check_wav_output(int ch, int rate, const std::string& format);
+// y: planar samples. Integer formats are scaled, optionally TPDF-dithered (two uniform draws per sample from
+// std::mt19937_64 seeded 12345, frame-major order), rounded in the current rounding mode and clipped.
+void write_wav(const char* path, const std::vector<std::vector<double>>& y, int ch, long long frames, int rate,
+               const std::string& format, bool dither, long long& clipped);
+
+}  // namespace kbsrc::io

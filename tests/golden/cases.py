@@ -1,0 +1,73 @@
+"""Seeded synthetic inputs and the parity case list shared by the golden-fixture generator and the tests.
+
+The workloads stand in for the configurations the engine is measured on (uniform noise in [-0.5, 0.5) from
+numpy's default_rng, a log sine sweep); no external data is involved.
+"""
+import numpy as np
+
+
+def noise(seed, seconds, rate, channels):
+    """i.i.d. uniform [-0.5, 0.5) f64 samples, (frames, channels), from default_rng(seed)."""
+    return np.random.default_rng(seed).uniform(-0.5, 0.5, (int(round(seconds * rate)), channels))
+
+
+def sweep(seconds, rate, channels=2, f0=20.0, f1=20000.0, amp=0.5):
+    """Log sine sweep f0 -> f1 Hz over `seconds`, the same on every channel."""
+    T = float(seconds)
+    t = np.arange(int(round(seconds * rate))) / rate
+    k = np.log(f1 / f0)
+    x = amp * np.sin(2 * np.pi * f0 * T / k * (np.exp(t / T * k) - 1))
+    return np.repeat(x[:, None], channels, axis=1)
+
+
+# name -> (input recipe, rate_in, rate_out, options). Recipes: ("noise", seed, seconds, rate, ch),
+# ("sweep", seconds, rate, ch), ("frames", seed, frames, ch).
+CASES = {
+    # configurations of the benchmark
+    "c1_96k_44k1_exact": (("noise", 1, 10, 96000, 2), 96000, 44100, {"mode": "exact"}),
+    "c2_96k_44k1_exact": (("noise", 2, 180, 96000, 2), 96000, 44100, {"mode": "exact"}),
+    "c2_96k_44k1_fast": (("noise", 2, 180, 96000, 2), 96000, 44100, {"mode": "fast"}),
+    "c3_sweep_44k1_48k_exact": (("sweep", 60, 44100, 2), 44100, 48000, {"mode": "exact"}),
+    "c3_sweep_44k1_48k_fast": (("sweep", 60, 44100, 2), 44100, 48000, {"mode": "fast"}),
+    # small cases: down/up, both modes, direct and four-step transforms, options, channel counts, edges
+    "s_48k_96k_exact_97": (("frames", 11, 97, 2), 48000, 96000, {"mode": "exact"}),
+    "s_48k_96k_fast_97": (("frames", 11, 97, 2), 48000, 96000, {"mode": "fast"}),
+    "s_48k_44k1_exact_97": (("frames", 12, 97, 2), 48000, 44100, {"mode": "exact"}),
+    "s_48k_44k1_fast_97": (("frames", 12, 97, 2), 48000, 44100, {"mode": "fast"}),
+    "s_8k_16k_exact_1_len001": (("frames", 13, 1, 2), 8000, 16000, {"mode": "exact", "length": 0.01}),
+    "s_8k_16k_fast_50_len001": (("frames", 13, 50, 1), 8000, 16000, {"mode": "fast", "length": 0.01}),
+    "s_16k_8k_exact_300_len001": (("frames", 14, 300, 1), 16000, 8000, {"mode": "exact", "length": 0.01}),
+    "s_96k_44k1_exact_20000": (("frames", 15, 20000, 2), 96000, 44100, {"mode": "exact"}),
+    "s_96k_44k1_fast_20000": (("frames", 15, 20000, 2), 96000, 44100, {"mode": "fast"}),
+    "s_44k1_48k_exact_30000": (("frames", 16, 30000, 1), 44100, 48000, {"mode": "exact"}),
+    "s_44k1_48k_fast_30000": (("frames", 16, 30000, 3), 44100, 48000, {"mode": "fast"}),
+    "s_192k_44k1_exact_40000": (("frames", 17, 40000, 2), 192000, 44100, {"mode": "exact"}),
+    "s_44k1_96k_exact_10000": (("frames", 18, 10000, 2), 44100, 96000, {"mode": "exact"}),
+    "s_44k1_8k_fast_20000": (("frames", 19, 20000, 1), 44100, 8000, {"mode": "fast"}),
+    "s_8k_44k1_exact_3000": (("frames", 20, 3000, 1), 8000, 44100, {"mode": "exact"}),
+    "s_48k_192k_fast_5000": (("frames", 21, 5000, 2), 48000, 192000, {"mode": "fast"}),
+    "s_96k_48k_exact_nolpc": (("frames", 22, 15000, 2), 96000, 48000, {"mode": "exact", "lpc": False}),
+    "s_44k1_48k_exact_block": (("frames", 23, 20000, 1), 44100, 48000, {"mode": "exact", "block": 700}),
+    "s_96k_44k1_exact_len05_beta60": (("frames", 24, 30000, 1), 96000, 44100,
+                                      {"mode": "exact", "length": 0.05, "beta": 60.0}),
+    "s_48k_96k_exact_6ch": (("frames", 25, 4000, 6), 48000, 96000, {"mode": "exact"}),
+    "s_48k_44k1_exact_10frames": (("frames", 26, 10, 1), 48000, 44100, {"mode": "exact"}),
+    "s_48k_44k1_exact_empty": (("frames", 27, 0, 1), 48000, 44100, {"mode": "exact"}),
+    "s_22k05_48k_fast_len002": (("frames", 28, 3000, 1), 22050, 48000, {"mode": "fast", "length": 0.02}),
+}
+
+
+def make_input(recipe):
+    kind = recipe[0]
+    if kind == "noise":
+        _, seed, seconds, rate, ch = recipe
+        return noise(seed, seconds, rate, ch)
+    if kind == "sweep":
+        _, seconds, rate, ch = recipe
+        return sweep(seconds, rate, ch)
+    _, seed, frames, ch = recipe
+    return np.random.default_rng(seed).uniform(-0.5, 0.5, (frames, ch))
+
+
+def is_small(name):
+    return name.startswith("s_")
