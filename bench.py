@@ -1,0 +1,369 @@
+#!/usr/bin/env python
+"""Throughput of the DFT-domain resampling block engine on B200: output Msamples/s.
+
+Workload (default): 180 s of stereo 96 kHz float64 noise (uniform [-0.5, 0.5), numpy default_rng(2)) converted
+to 44.1 kHz in exact (double-double) mode with the defaults (--len 0.2, --beta 40, LPC edges, automatic block):
+107 blocks x 2 channels of a 201600-point forward and 92610-point inverse real FFT. One step = the whole
+block loop of that conversion (every (channel, block) task), output byte-identical to the reference.
+
+  value  device-resident: input, LPC edges and output in HBM; the engine's launches only (CUDA events)
+  e2e    the same through the C ABI with host buffers: kbsrc_gpu_engine_run_host on pinned memory, the H2D copy
+         of the input and edges and the D2H copy of the output inside the timed region
+  --impl reference: the reference's own engine (HongYue1/KBSRC built from source, oracle/_ref) on the host
+         cores, its Stats::process_seconds (the block loop run_engine) per conversion
+
+Multi-GPU (torchrun): every rank converts its own file of the workload (independent conversions, no
+collective on the data path; weak scaling). Timing is the max over ranks.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+
+WORKLOADS = {
+    "c2_exact": dict(seed=2, seconds=180, rate_in=96000, rate_out=44100, channels=2, mode="exact"),
+    "c2_fast": dict(seed=2, seconds=180, rate_in=96000, rate_out=44100, channels=2, mode="fast"),
+    "c1_exact": dict(seed=1, seconds=10, rate_in=96000, rate_out=44100, channels=2, mode="exact"),
+    "c3_exact": dict(sweep=True, seconds=60, rate_in=44100, rate_out=48000, channels=2, mode="exact"),
+}
+METRIC = "out Msamples/s 96k->44.1k exact (180 s stereo f64, byte-identical to the reference)"
+
+
+def make_input(w):
+    from cases import noise, sweep
+    if w.get("sweep"):
+        return sweep(w["seconds"], w["rate_in"], w["channels"])
+    return noise(w["seed"], w["seconds"], w["rate_in"], w["channels"])
+
+
+class ClockSampler:
+    """Samples SM clock and clock-event reasons through NVML every 20 ms while running."""
+
+    REASONS = {"gpu_idle": 0x1, "applications_clocks_setting": 0x2, "sw_power_cap": 0x4, "hw_slowdown": 0x8,
+               "sync_boost": 0x10, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40,
+               "hw_power_brake_slowdown": 0x80, "display_clock_setting": 0x100}
+
+    def __init__(self, index):
+        self.samples, self.reasons, self.ok = [], set(), False
+        self.max_mhz = None
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+            self.ok = True
+        except Exception:
+            pass
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                mhz = self.nv.nvmlDeviceGetClockInfo(self.h, self.nv.NVML_CLOCK_SM)
+                r = self.nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                util = self.nv.nvmlDeviceGetUtilizationRates(self.h).gpu
+                self.samples.append((mhz, util))
+                for k, bit in self.REASONS.items():
+                    if r & bit and k != "gpu_idle":
+                        self.reasons.add(k)
+            except Exception:
+                pass
+            time.sleep(0.02)
+
+    def __enter__(self):
+        if self.ok:
+            self._t = threading.Thread(target=self._run, daemon=True)
+            self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._t:
+            self._t.join()
+
+    def summary(self):
+        loaded = [m for m, u in self.samples if u > 50] or [m for m, _ in self.samples]
+        return {"sm_mhz": statistics.median(loaded) if loaded else None, "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(self.reasons), "samples": len(self.samples)}
+
+
+def fp64_peak():
+    """Measured FP64 instruction rate of this GPU (ops/s, one DFMA/DADD/DMUL = 1), max over the three kinds."""
+    import ctypes
+    lib = ctypes.CDLL(os.path.join(ROOT, "kbsrc_b200", "lib", "libkbsrc_probe.so"))
+    lib.kbsrc_probe_fp64.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+    rates = {}
+    for kind, name in ((0, "dfma"), (1, "dadd"), (2, "dmul")):
+        v = ctypes.c_double()
+        if lib.kbsrc_probe_fp64(kind, ctypes.byref(v)) == 0:
+            rates[name] = v.value
+    return rates
+
+
+def measured_hbm_gbs():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def load_traffic():
+    """dram bytes per launch from the committed ncu summary, if any: {workload: {pass: bytes}}."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+def cpu_reference(x, w, threads, runs=1):
+    """The reference engine on the host (oracle/_ref): output Msamples/s from its process_seconds."""
+    from oracle import oracle
+    if not oracle.ref_available():
+        return None
+    n_out, secs, walls = 0, 0.0, 0.0
+    for _ in range(runs):
+        st = {}
+        t = time.perf_counter()
+        y = oracle.ref_resample(x, w["rate_in"], w["rate_out"], fast=w["mode"] == "fast", threads=threads, stats=st)
+        walls += time.perf_counter() - t
+        n_out += y.size
+        secs += st["process_seconds"]
+    return {"engine_msps": n_out / secs / 1e6, "wall_msps": n_out / walls / 1e6, "threads": st["threads"],
+            "process_seconds": secs / runs, "wall_seconds": walls / runs, "samples": n_out // runs}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        backend = "gloo" if args.impl == "reference" else "nccl"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    return world, rank, local, pg
+
+
+def reference_arm(args, w, world, rank, pg):
+    if rank != 0:
+        if pg:
+            pg.barrier()
+            pg.destroy_process_group()
+        return
+    x = make_input(w)
+    threads = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        cpu_reference(x, w, threads)
+    n_out, secs, walls = 0, 0.0, 0.0
+    for _ in range(args.steps):
+        r = cpu_reference(x, w, threads)
+        n_out += r["samples"]
+        secs += r["process_seconds"]
+        walls += r["wall_seconds"]
+    value = n_out / secs / 1e6
+    line = {"impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": "Msamples/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(secs / args.steps * 1e3, 3), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if w["mode"] == "fast" else "dd (double-double f64 pairs)",
+            "data": "synthetic", "config": {"workload": args.workload, **{k: v for k, v in w.items()}},
+            "whole_call_msps": round(n_out / walls / 1e6, 3),
+            "cpu_baseline": {"value": round(value, 3), "unit": "Msamples/s", "cores": threads, "kind": "reference",
+                             "sample": f"{args.steps} full conversions of the workload, engine time "
+                                       "(Stats::process_seconds) with all host threads"},
+            "e2e": {"value": round(value, 3), "unit": "Msamples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+def product_arm(args, w, world, rank, local, pg):
+    import torch
+    import kbsrc_b200
+    from kbsrc_b200 import roofline
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    exact = w["mode"] == "exact"
+    x = make_input(w)
+    frames, ch = x.shape
+    cv = kbsrc_b200.Conversion(x, w["rate_in"], w["rate_out"], mode=w["mode"])
+    plan = kbsrc_b200.plan(frames, ch, w["rate_in"], w["rate_out"], w["mode"])
+    work = roofline.conversion_work(plan, ch, exact)
+    info = cv.engine_info()
+    nout = cv.nout
+    d_in = torch.from_numpy(x).to(dev)
+    d_head = torch.from_numpy(cv.head).to(dev) if cv.head.size else torch.zeros(1, dtype=torch.float64, device=dev)
+    d_tail = torch.from_numpy(cv.tail).to(dev) if cv.tail.size else torch.zeros(1, dtype=torch.float64, device=dev)
+    d_out = torch.empty(ch * max(nout, 1), dtype=torch.float64, device=dev)
+    # a dedicated stream: the engine runs and the CUDA events are recorded on it (handle 0 would mean the
+    # engine's own stream in the C ABI)
+    side = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(side)
+    stream = side.cuda_stream
+    ptrs = (d_in.data_ptr(), d_head.data_ptr(), d_tail.data_ptr(), d_out.data_ptr())
+
+    def step():
+        cv.run_device(*ptrs, stream=stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",")
+    phys = vis[local] if local < len(vis) and vis[local].strip().isdigit() else str(local)
+    sampler = ClockSampler(int(phys))
+    with sampler:
+        # value: K back-to-back block loops on resident data (inputs 276 MB > L2, so no flush is needed)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(args.steps):
+            step()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        # per-pass device time over K more steps (an event after every launch, same stream)
+        pass_ms = {}
+        for _ in range(args.steps):
+            for k, (t, n) in cv.run_device_timed(*ptrs, stream=stream).items():
+                a = pass_ms.setdefault(k, [0.0, 0])
+                a[0] += t
+                a[1] += n
+        # e2e: through the C ABI with pinned host buffers, copies inside the timed region
+        hx = torch.from_numpy(x).pin_memory()
+        hh = torch.from_numpy(cv.head.copy() if cv.head.size else np.zeros(1)).pin_memory()
+        ht = torch.from_numpy(cv.tail.copy() if cv.tail.size else np.zeros(1)).pin_memory()
+        ho = torch.empty(ch * max(nout, 1), dtype=torch.float64).pin_memory()
+        cv.run_host_raw(hx.data_ptr(), hh.data_ptr(), ht.data_ptr(), ho.data_ptr())
+        e2e_steps = max(3, args.steps // 2)
+        if pg:
+            pg.barrier()
+        t = time.perf_counter()
+        for _ in range(e2e_steps):
+            cv.run_host_raw(hx.data_ptr(), hh.data_ptr(), ht.data_ptr(), ho.data_ptr())
+        e2e_s = time.perf_counter() - t
+    if pg:
+        import torch.distributed as dist
+        tt = torch.tensor([ms, e2e_s], dtype=torch.float64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms, e2e_s = tt.tolist()
+    # byte-identity of what was timed, against the reference's hash for this workload
+    got = ho[:ch * nout].numpy().reshape(ch, nout)
+    import hashlib
+    digest = hashlib.sha256(got.astype("<f8").tobytes()).hexdigest()
+    golden_sha = None
+    try:
+        with open(os.path.join(ROOT, "tests", "golden", "golden.json")) as f:
+            gold = json.load(f)["cases"]
+        key = {"c2_exact": "c2_96k_44k1_exact", "c2_fast": "c2_96k_44k1_fast", "c1_exact": "c1_96k_44k1_exact",
+               "c3_exact": "c3_sweep_44k1_48k_exact"}.get(args.workload)
+        golden_sha = gold.get(key, {}).get("sha256")
+    except Exception:
+        pass
+    if rank != 0:
+        if pg:
+            pg.barrier()
+            pg.destroy_process_group()
+        return
+    samples = ch * nout * world
+    value = samples * args.steps / (ms * 1e-3) / 1e6
+    e2e = samples * e2e_steps / e2e_s / 1e6
+    # roofline of the dominant kernel
+    launches_per_step = {k: v[1] / args.steps for k, v in pass_ms.items()}
+    avg_ms = {k: v[0] / v[1] for k, v in pass_ms.items() if v[1]}
+    share = {k: v[0] / sum(a[0] for a in pass_ms.values()) for k, v in pass_ms.items() if v[1]}
+    top = max(avg_ms, key=lambda k: pass_ms[k][0])
+    waves = max(1, int(round(launches_per_step[top])))
+    tasks_per_launch = work["tasks"] / waves
+    traffic = load_traffic().get(args.workload, {}).get(top)
+    if exact:
+        peaks = fp64_peak()
+        peak = max(peaks.values()) if peaks else None
+        achieved = work["ops_per_task"][top] * tasks_per_launch / (avg_ms[top] * 1e-3)
+        roof = {"bound": "fp64", "achieved": round(achieved / 1e12, 3), "peak": round(peak / 1e12, 3) if peak else None,
+                "unit": "TFLOP/s", "frac": round(achieved / peak, 4) if peak else None,
+                "traffic": traffic, "kernel": top,
+                "note": "FP64 instructions/s (add, mul, fma each 1) of the reference operation sequence; peak = "
+                        "measured DFMA/DADD/DMUL issue rate of this GPU (of measured)",
+                "peak_by_kind_tflops": {k: round(v / 1e12, 3) for k, v in peaks.items()}}
+    else:
+        peak, how = measured_hbm_gbs()
+        b = roofline.pass_bytes(plan, exact)[top] * tasks_per_launch
+        achieved = b / (avg_ms[top] * 1e-3) / 1e9
+        roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "traffic": traffic, "kernel": top, "peak_source": how}
+    whole_ops = work["ops_total"] / (ms * 1e-3 / args.steps)
+    cpu = None
+    if world == 1 and not args.no_cpu:
+        c_all = cpu_reference(x, w, os.cpu_count() or 1)
+        c_8 = cpu_reference(x, w, 8)
+        if c_all:
+            cpu = {"value": round(c_all["engine_msps"], 3), "unit": "Msamples/s", "cores": c_all["threads"],
+                   "kind": "reference",
+                   "sample": "one full conversion of the workload by the reference built from source, engine "
+                             "time (Stats::process_seconds), all host threads",
+                   "value_t8": round(c_8["engine_msps"], 3), "whole_call_msps": round(c_all["wall_msps"], 3)}
+    line = {
+        "metric": METRIC, "value": round(value, 3), "unit": "Msamples/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "dd (double-double f64 pairs)" if exact else "f64", "data": "synthetic",
+        "config": {"workload": args.workload, **w, "tasks": work["tasks"], "block": plan["nb"],
+                   "fft_points": [plan["Nb"], plan["Mb"]], "l2": "inputs larger than L2 (276 MB)",
+                   "parallelism": f"independent conversions x{world}"},
+        "e2e": {"value": round(e2e, 3), "unit": "Msamples/s", "h2d_bytes_per_step": int(8 * (x.size + cv.head.size
+                                                                                                 + cv.tail.size)),
+                "d2h_bytes_per_step": int(8 * ch * nout), "path": "kbsrc_gpu_engine_run_host (C ABI), pinned"},
+        "gpu_launches": int(info["launches"] * args.steps),
+        "roofline": roof,
+        "passes": {k: {"ms": round(avg_ms[k], 4), "share": round(share[k], 4),
+                       "launches_per_step": launches_per_step[k]} for k in avg_ms},
+        "fp64_ops_per_step": work["ops_total"], "whole_step_tflops": round(whole_ops / 1e12, 3),
+        "cpu_baseline": cpu,
+        "clocks": sampler.summary(),
+        "output_sha256_matches_reference": golden_sha == digest if golden_sha else None,
+    }
+    print(json.dumps(line), flush=True)
+    cv.close()
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="product", choices=["product", "reference"])
+    ap.add_argument("--workload", default="c2_exact", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    args = ap.parse_args()
+    w = WORKLOADS[args.workload]
+    world, rank, local, pg = dist_setup(args)
+    if args.impl == "reference":
+        reference_arm(args, w, world, rank, pg)
+    else:
+        product_arm(args, w, world, rank, local, pg)
+
+
+if __name__ == "__main__":
+    main()

@@ -71,6 +71,13 @@ int kbsrc_gpu_engine_run_host(kbsrc_gpu_engine* e, const double* in, const doubl
 int kbsrc_gpu_engine_run_device(kbsrc_gpu_engine* e, const double* d_in, const double* d_head,
                                 const double* d_tail, double* d_out, void* stream);
 
+/* kbsrc_gpu_engine_run_device, recording an event after every launch; waits for the run, then returns the
+ * summed device time of each pass kind in pass_ms[6] (forward column or direct, forward row, spectrum split,
+ * multiply+merge, inverse column or direct, inverse row + output) and their launch counts (may be NULL). */
+int kbsrc_gpu_engine_run_device_timed(kbsrc_gpu_engine* e, const double* d_in, const double* d_head,
+                                      const double* d_tail, double* d_out, void* stream, float* pass_ms,
+                                      int* pass_launches);
+
 /* Number of (channel, block) tasks, kernel launches per run, and the engine's device bytes. */
 int kbsrc_gpu_engine_info(const kbsrc_gpu_engine* e, long long* tasks, long long* launches,
                           long long* device_bytes);

@@ -57,6 +57,9 @@ GPU_SYMBOLS = {
     "kbsrc_gpu_engine_run_host": (ctypes.c_int, [ctypes.c_void_p, _dp, _dp, _dp, _dp]),
     "kbsrc_gpu_engine_run_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                                    ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "kbsrc_gpu_engine_run_device_timed": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                                         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                                         _P(ctypes.c_float), _P(ctypes.c_int)]),
     "kbsrc_gpu_engine_info": (ctypes.c_int, [ctypes.c_void_p, _lp, _lp, _lp]),
     "kbsrc_gpu_engine_destroy": (None, [ctypes.c_void_p]),
     "kbsrc_gpu_kernel_spectrum": (ctypes.c_int, [_dp, ctypes.c_int, ctypes.c_int, ctypes.c_double, _dp]),
@@ -210,6 +213,18 @@ class Conversion:
         rc = gpu_lib().kbsrc_gpu_engine_run_device(self.engine, d_in, d_head, d_tail, d_out, stream or None)
         if rc:
             raise RuntimeError(f"kbsrc_gpu_engine_run_device: {rc} {gpu_error()}")
+
+    PASSES = ["fwd_column", "fwd_row", "split", "merge", "inv_column", "inv_row"]
+
+    def run_device_timed(self, d_in, d_head, d_tail, d_out, stream=0):
+        """run_device with an event after every launch; returns {pass: (ms, launches)} (synchronises)."""
+        ms = (ctypes.c_float * 6)()
+        n = (ctypes.c_int * 6)()
+        rc = gpu_lib().kbsrc_gpu_engine_run_device_timed(self.engine, d_in, d_head, d_tail, d_out, stream or None,
+                                                         ms, n)
+        if rc:
+            raise RuntimeError(f"kbsrc_gpu_engine_run_device_timed: {rc} {gpu_error()}")
+        return {k: (ms[i], n[i]) for i, k in enumerate(self.PASSES)}
 
     def run_host_raw(self, x_ptr, head_ptr, tail_ptr, out_ptr):
         """Engine run on host pointers (ints), e.g. pinned buffers; synchronous."""

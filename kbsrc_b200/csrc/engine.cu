@@ -551,7 +551,9 @@ struct kbsrc_gpu_engine {
     Shape col_fw{}, row_fw{}, col_iv{}, row_iv{}, dir_fw{}, dir_iv{};
     OddRoots<dd> odd_dd{};
     OddRoots<double> odd_f64{};
+    std::vector<cudaEvent_t> events;  // per-pass timing trail, created on first use
     ~kbsrc_gpu_engine() {
+        for (cudaEvent_t x : events) cudaEventDestroy(x);
         if (stream) cudaStreamDestroy(stream);
     }
 };
@@ -600,9 +602,34 @@ unsigned grid_for(long long n, int threads) {
 }
 
 // Enqueues all passes for every wave of tasks. ArL: four-step sub-FFT arithmetic, ArS: everything else.
+// Pass kinds for per-pass timing (kbsrc_gpu_engine_run_device_timed)
+enum PassKind { kFwdA = 0, kFwdB, kSplit, kMerge, kInvA, kInvB, kPassKinds };
+
+// Optional per-launch event trail: marks[0] before the first launch, then one event after each launch.
+struct Trail {
+    std::vector<cudaEvent_t>* ev = nullptr;
+    std::vector<int>* kind = nullptr;
+    size_t n = 0;
+    int mark(cudaStream_t st, int k) {
+        if (!ev) return KBSRC_GPU_OK;
+        if (n >= ev->size()) {
+            cudaEvent_t x;
+            KB_CUDA(cudaEventCreate(&x));
+            ev->push_back(x);
+        }
+        KB_CUDA(cudaEventRecord((*ev)[n], st));
+        if (kind) kind->push_back(k);
+        n++;
+        return KBSRC_GPU_OK;
+    }
+};
+
 template <class ArL, class ArS>
 int enqueue(kbsrc_gpu_engine* e, const double* in, const double* head, const double* tail, double* out,
-            cudaStream_t st) {
+            cudaStream_t st, Trail* trail) {
+    Trail none;
+    Trail& tr = trail ? *trail : none;
+    int rc;
     using CL = CxR<ArL>;
     using CS = CxR<ArS>;
     static_assert(sizeof(CL) == sizeof(CS), "one element size per mode");
@@ -616,6 +643,7 @@ int enqueue(kbsrc_gpu_engine* e, const double* in, const double* head, const dou
     CS* AS = static_cast<CS*>(e->bufA.p);
     CS* BS = static_cast<CS*>(e->bufB.p);
     long long launches = 0;
+    if ((rc = tr.mark(st, -1)) != KBSRC_GPU_OK) return rc;
     for (long long t0 = 0; t0 < e->tasks; t0 += e->wave) {
         const unsigned nt = (unsigned)std::min(e->wave, e->tasks - t0);
         // forward real FFT: gather + complex FFT into B (natural order)
@@ -628,8 +656,10 @@ int enqueue(kbsrc_gpu_engine* e, const double* in, const double* head, const dou
             p.odd = odd_of<WL>(e);
             p.src = AL; p.dst = AL; p.stride = e->stride; p.task0 = t0; p.sig = sig;
             k_column<ArL, kSrcSignal><<<dim3((c.N2 + p.F - 1) / p.F, nt), e->col_fw.T, e->col_fw.smem, st>>>(p);
+            if ((rc = tr.mark(st, kFwdA)) != KBSRC_GPU_OK) return rc;
             p.sp = c.s2; p.F = e->row_fw.F; p.src = AL; p.dst = BL;
             k_row<ArL, kDstComplex><<<dim3((c.N1 + p.F - 1) / p.F, nt), e->row_fw.T, e->row_fw.smem, st>>>(p);
+            if ((rc = tr.mark(st, kFwdB)) != KBSRC_GPU_OK) return rc;
             launches += 2;
         } else {
             PassParams<ArS> p{};
@@ -638,6 +668,7 @@ int enqueue(kbsrc_gpu_engine* e, const double* in, const double* head, const dou
             p.odd = odd_of<WS>(e);
             p.src = AS; p.dst = BS; p.stride = e->stride; p.task0 = t0; p.sig = sig;
             k_direct<ArS, kSrcSignal, kDstComplex><<<dim3(1, nt), e->dir_fw.T, e->dir_fw.smem, st>>>(p);
+            if ((rc = tr.mark(st, kFwdA)) != KBSRC_GPU_OK) return rc;
             launches += 1;
         }
         // split into the real spectrum (B -> A), multiply/fold and merge (A -> B)
@@ -648,7 +679,9 @@ int enqueue(kbsrc_gpu_engine* e, const double* in, const double* head, const dou
         s.H = static_cast<const WS*>(e->H.p);
         s.h = e->hf; s.hi = e->hi; s.Nb = e->Nb; s.Mb = e->Mb; s.up = d.up;
         k_split<ArS><<<dim3(grid_for(e->hf / 2 + 1 + (ArS::kDD ? 0 : e->hf / 2), 256), nt), 256, 0, st>>>(s);
+        if ((rc = tr.mark(st, kSplit)) != KBSRC_GPU_OK) return rc;
         k_merge<ArS><<<dim3(grid_for(e->hi / 2 + 1 + (ArS::kDD ? 0 : e->hi / 2), 256), nt), 256, 0, st>>>(s);
+        if ((rc = tr.mark(st, kMerge)) != KBSRC_GPU_OK) return rc;
         launches += 2;
         // inverse complex FFT of B and the output epilogue
         if (e->iv.host.four) {
@@ -660,8 +693,10 @@ int enqueue(kbsrc_gpu_engine* e, const double* in, const double* head, const dou
             p.odd = odd_of<WL>(e);
             p.src = BL; p.dst = BL; p.stride = e->stride; p.task0 = t0; p.out = o;
             k_column<ArL, kSrcComplex><<<dim3((c.N2 + p.F - 1) / p.F, nt), e->col_iv.T, e->col_iv.smem, st>>>(p);
+            if ((rc = tr.mark(st, kInvA)) != KBSRC_GPU_OK) return rc;
             p.sp = c.s2; p.F = e->row_iv.F;
             k_row<ArL, kDstOutput><<<dim3((c.N1 + p.F - 1) / p.F, nt), e->row_iv.T, e->row_iv.smem, st>>>(p);
+            if ((rc = tr.mark(st, kInvB)) != KBSRC_GPU_OK) return rc;
             launches += 2;
         } else {
             PassParams<ArS> p{};
@@ -670,6 +705,7 @@ int enqueue(kbsrc_gpu_engine* e, const double* in, const double* head, const dou
             p.odd = odd_of<WS>(e);
             p.src = BS; p.dst = BS; p.stride = e->stride; p.task0 = t0; p.out = o;
             k_direct<ArS, kSrcComplex, kDstOutput><<<dim3(1, nt), e->dir_iv.T, e->dir_iv.smem, st>>>(p);
+            if ((rc = tr.mark(st, kInvA)) != KBSRC_GPU_OK) return rc;
             launches += 1;
         }
     }
@@ -773,14 +809,14 @@ int create_impl(const kbsrc_gpu_desc* desc, kbsrc_gpu_engine** out) {
 }
 
 int run_device_impl(kbsrc_gpu_engine* e, const double* in, const double* head, const double* tail, double* out,
-                    cudaStream_t st) {
+                    cudaStream_t st, Trail* trail = nullptr) {
     const kbsrc_gpu_desc& d = e->d;
     if (d.nout > 0) KB_CUDA(cudaMemsetAsync(out, 0, (size_t)d.nout * d.channels * sizeof(double), st));
     if (e->tasks == 0 || d.nout == 0) return KBSRC_GPU_OK;
     if (d.frames > 0 && !in) return fail(KBSRC_GPU_E_ARG, "null input");
     if (d.edge_len > 0 && (!head || !tail)) return fail(KBSRC_GPU_E_ARG, "null edge buffers");
-    if (e->exact) return enqueue<ArDDShort, ArDDAccurate>(e, in, head, tail, out, st);
-    return enqueue<ArF64, ArF64>(e, in, head, tail, out, st);
+    if (e->exact) return enqueue<ArDDShort, ArDDAccurate>(e, in, head, tail, out, st, trail);
+    return enqueue<ArF64, ArF64>(e, in, head, tail, out, st, trail);
 }
 
 }  // namespace
@@ -808,6 +844,37 @@ int kbsrc_gpu_engine_run_device(kbsrc_gpu_engine* e, const double* d_in, const d
     if (!d_out && e->d.nout > 0) return fail(KBSRC_GPU_E_ARG, "null output");
     try {
         return run_device_impl(e, d_in, d_head, d_tail, d_out, stream ? (cudaStream_t)stream : e->stream);
+    } catch (const std::exception& x) {
+        return fail(KBSRC_GPU_E_CUDA, x.what());
+    }
+}
+
+int kbsrc_gpu_engine_run_device_timed(kbsrc_gpu_engine* e, const double* d_in, const double* d_head,
+                                      const double* d_tail, double* d_out, void* stream, float* pass_ms,
+                                      int* pass_launches) {
+    if (!e || !pass_ms) return fail(KBSRC_GPU_E_ARG, "null engine or timing array");
+    if (!d_out && e->d.nout > 0) return fail(KBSRC_GPU_E_ARG, "null output");
+    try {
+        cudaStream_t st = stream ? (cudaStream_t)stream : e->stream;
+        std::vector<int> kinds;
+        Trail tr{&e->events, &kinds, 0};
+        int rc = run_device_impl(e, d_in, d_head, d_tail, d_out, st, &tr);
+        if (rc) return rc;
+        for (int k = 0; k < kPassKinds; k++) {
+            pass_ms[k] = 0;
+            if (pass_launches) pass_launches[k] = 0;
+        }
+        if (tr.n > 0) KB_CUDA(cudaEventSynchronize(e->events[tr.n - 1]));
+        for (size_t i = 1; i < tr.n; i++) {
+            float ms = 0;
+            KB_CUDA(cudaEventElapsedTime(&ms, e->events[i - 1], e->events[i]));
+            const int k = kinds[i];
+            if (k >= 0 && k < kPassKinds) {
+                pass_ms[k] += ms;
+                if (pass_launches) pass_launches[k] += 1;
+            }
+        }
+        return KBSRC_GPU_OK;
     } catch (const std::exception& x) {
         return fail(KBSRC_GPU_E_CUDA, x.what());
     }
