@@ -11,10 +11,11 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_DIR = os.path.join(HERE, "lib")
+# KBSRC_B200_LIB selects another build of the same libraries (a directory holding lib/ and bin/)
+LIB_DIR = os.path.join(os.environ.get("KBSRC_B200_LIB", HERE), "lib")
 HOST_SO = os.path.join(LIB_DIR, "libkbsrc.so")
 GPU_SO = os.path.join(LIB_DIR, "libkbsrc_gpu.so")
-CLI = os.path.join(HERE, "bin", "kbsrc")
+CLI = os.path.join(os.path.dirname(LIB_DIR), "bin", "kbsrc")
 
 FAST, EXACT = 0, 1
 _P = ctypes.POINTER

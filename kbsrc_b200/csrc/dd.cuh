@@ -7,6 +7,15 @@
 #pragma once
 #include <cuda_runtime.h>
 
+// Occupancy targets of the shared-memory passes (256-thread CTAs per SM): they cap registers at 64K/(256*n).
+// Double-double butterflies need about 128 registers (2 CTAs); f64 ones fit 3.
+#ifndef KB_MINB_DD
+#define KB_MINB_DD 2
+#endif
+#ifndef KB_MINB_F64
+#define KB_MINB_F64 3
+#endif
+
 namespace kbsrc::dev {
 
 struct dd {
@@ -70,6 +79,7 @@ struct ArF64 {  // Precision::Fast: float64 everywhere (V4 lanes and scalar alik
     using R = double;
     using W = double;
     static constexpr bool kLanes = true, kLaneRenorm = false, kDD = false;
+    static constexpr int kMinBlocks = KB_MINB_F64;  // resident 256-thread CTAs per SM the passes are built for
     static __device__ __forceinline__ R add(R a, R b) { return __dadd_rn(a, b); }
     static __device__ __forceinline__ R sub(R a, R b) { return __dsub_rn(a, b); }
     static __device__ __forceinline__ R mul(R a, R b) { return __dmul_rn(a, b); }
@@ -84,6 +94,7 @@ struct ArDDShort {  // four-step sub-FFTs of Precision::Exact (DD4 lanes)
     using R = dd;
     using W = dd;
     static constexpr bool kLanes = true, kLaneRenorm = true, kDD = true;
+    static constexpr int kMinBlocks = KB_MINB_DD;
     static __device__ __forceinline__ R add(R a, R b) { return add_short(a, b); }
     static __device__ __forceinline__ R sub(R a, R b) { return add_short(a, dd_neg(b)); }
     static __device__ __forceinline__ R mul(R a, R b) { return mul_dd(a, b); }
@@ -99,6 +110,7 @@ struct ArDDAccurate {  // scalar dd: direct SFFT, Bluestein, RFFT split/merge, s
     using R = dd;
     using W = dd;
     static constexpr bool kLanes = false, kLaneRenorm = false, kDD = true;
+    static constexpr int kMinBlocks = KB_MINB_DD;
     static __device__ __forceinline__ R add(R a, R b) { return add_accurate(a, b); }
     static __device__ __forceinline__ R sub(R a, R b) { return add_accurate(a, dd_neg(b)); }
     static __device__ __forceinline__ R mul(R a, R b) { return mul_dd(a, b); }

@@ -124,10 +124,16 @@ __device__ __forceinline__ CxR<Ar> czero() {
     return CxR<Ar>{Ar::zero(), Ar::zero()};
 }
 
+// Shared memory of a pass: two sequence buffers of n*F values, then the sub-FFT's stage twiddles.
+template <class Ar>
+__device__ __forceinline__ CxW<Ar>* twiddle_smem(unsigned char* smem, int n, int F) {
+    return reinterpret_cast<CxW<Ar>*>(smem + 2 * (size_t)n * F * sizeof(CxR<Ar>));
+}
+
 // Column pass: sequences n2 in [c0, c0+F) of length N1 (stride N2), twiddle, store in place
 // (fft.hpp:283-299). blockIdx.x: column group; blockIdx.y: task slot.
 template <class Ar, int SRC>
-__global__ void __launch_bounds__(256) k_column(const __grid_constant__ PassParams<Ar> P) {
+__global__ void __launch_bounds__(256, Ar::kMinBlocks) k_column(const __grid_constant__ PassParams<Ar> P) {
     extern __shared__ __align__(16) unsigned char smem[];
     using C = CxR<Ar>;
     const int F = P.F, N1 = P.N1, N2 = P.N2;
@@ -137,26 +143,38 @@ __global__ void __launch_bounds__(256) k_column(const __grid_constant__ PassPara
     const int c0 = blockIdx.x * F;
     const C* src = P.src + blockIdx.y * P.stride;
     C* dst = P.dst + blockIdx.y * P.stride;
+    const CxW<Ar>* tws = stage_twiddles<Ar>(P.sp, P.tw_stage, twiddle_smem<Ar>(smem, N1, F));
     for (int e = threadIdx.x; e < N1 * F; e += blockDim.x) {
         const int r = e / F, f = e - r * F, n2 = c0 + f;
         A[r * F + f] = n2 < N2 ? load_input<Ar>(P, SRC, src, (long long)r * N2 + n2, task) : czero<Ar>();
     }
     __syncthreads();
-    const C* res = stockham<Ar>(P.sp, A, B, F, P.tw_stage, P.odd);
-    for (int e = threadIdx.x; e < N1 * F; e += blockDim.x) {
-        const int k1 = e / F, f = e - k1 * F, n2 = c0 + f;
-        if (n2 >= N2) continue;
-        C v = res[k1 * F + f];
-        if (k1 && (Ar::kLanes || n2)) v = c_mulw<Ar>(v, ld_tw(P.tw4 + (long long)k1 * N2 + n2));
-        if (Ar::kLaneRenorm) v = c_renorm<Ar>(v);
-        dst[(long long)k1 * N2 + n2] = v;
+    const C* res = stockham<Ar>(P.sp, A, B, F, tws, P.odd);
+    // four-step twiddle and store; the table loads of a chunk are issued before any of its products
+    constexpr int kChunk = 4;
+    for (int e0 = threadIdx.x; e0 < N1 * F; e0 += kChunk * blockDim.x) {
+        CxW<Ar> w[kChunk];
+#pragma unroll
+        for (int j = 0; j < kChunk; j++) {
+            const int e = e0 + j * blockDim.x, k1 = e / F, n2 = c0 + (e - k1 * F);
+            if (e < N1 * F && n2 < N2 && k1 && (Ar::kLanes || n2)) w[j] = ld_tw(P.tw4 + (long long)k1 * N2 + n2);
+        }
+#pragma unroll
+        for (int j = 0; j < kChunk; j++) {
+            const int e = e0 + j * blockDim.x, k1 = e / F, f = e - k1 * F, n2 = c0 + f;
+            if (e >= N1 * F || n2 >= N2) continue;
+            C v = res[k1 * F + f];
+            if (k1 && (Ar::kLanes || n2)) v = c_mulw<Ar>(v, w[j]);
+            if (Ar::kLaneRenorm) v = c_renorm<Ar>(v);
+            dst[(long long)k1 * N2 + n2] = v;
+        }
     }
 }
 
 // Row pass: rows r in [r0, r0+F) of length N2 (contiguous), stored transposed to [N1*k2 + r]
 // (fft.hpp:300-311), or written straight to the output as real samples (fft.hpp:459-460).
 template <class Ar, int DST>
-__global__ void __launch_bounds__(256) k_row(const __grid_constant__ PassParams<Ar> P) {
+__global__ void __launch_bounds__(256, Ar::kMinBlocks) k_row(const __grid_constant__ PassParams<Ar> P) {
     extern __shared__ __align__(16) unsigned char smem[];
     using C = CxR<Ar>;
     const int F = P.F, N1 = P.N1, N2 = P.N2;
@@ -165,12 +183,13 @@ __global__ void __launch_bounds__(256) k_row(const __grid_constant__ PassParams<
     const long long task = P.task0 + blockIdx.y;
     const int r0 = blockIdx.x * F;
     const C* src = P.src + blockIdx.y * P.stride;
+    const CxW<Ar>* tws = stage_twiddles<Ar>(P.sp, P.tw_stage, twiddle_smem<Ar>(smem, N2, F));
     for (int e = threadIdx.x; e < N2 * F; e += blockDim.x) {
         const int f = e / N2, i = e - f * N2, row = r0 + f;
         A[i * F + f] = row < N1 ? src[(long long)row * N2 + i] : czero<Ar>();
     }
     __syncthreads();
-    const C* res = stockham<Ar>(P.sp, A, B, F, P.tw_stage, P.odd);
+    const C* res = stockham<Ar>(P.sp, A, B, F, tws, P.odd);
     C* dst = P.dst + blockIdx.y * P.stride;
     const int c = DST == kDstOutput ? (int)(task / P.out.nblk) : 0;
     const long long b = DST == kDstOutput ? task % P.out.nblk : 0;
@@ -191,7 +210,7 @@ __global__ void __launch_bounds__(256) k_row(const __grid_constant__ PassParams<
 
 // Whole FFT of n <= 2048 points in one CTA (the reference's direct SFFT path, fft.hpp:241-244,279).
 template <class Ar, int SRC, int DST>
-__global__ void __launch_bounds__(256) k_direct(const __grid_constant__ PassParams<Ar> P) {
+__global__ void __launch_bounds__(256, Ar::kMinBlocks) k_direct(const __grid_constant__ PassParams<Ar> P) {
     extern __shared__ __align__(16) unsigned char smem[];
     using C = CxR<Ar>;
     const int n = P.sp.n;
@@ -199,9 +218,10 @@ __global__ void __launch_bounds__(256) k_direct(const __grid_constant__ PassPara
     C* B = A + n;
     const long long task = P.task0 + blockIdx.y;
     const C* src = P.src + blockIdx.y * P.stride;
+    const CxW<Ar>* tws = stage_twiddles<Ar>(P.sp, P.tw_stage, twiddle_smem<Ar>(smem, n, 1));
     for (int i = threadIdx.x; i < n; i += blockDim.x) A[i] = load_input<Ar>(P, SRC, src, i, task);
     __syncthreads();
-    const C* res = stockham<Ar>(P.sp, A, B, 1, P.tw_stage, P.odd);
+    const C* res = stockham<Ar>(P.sp, A, B, 1, tws, P.odd);
     C* dst = P.dst + blockIdx.y * P.stride;
     const int c = DST == kDstOutput ? (int)(task / P.out.nblk) : 0;
     const long long b = DST == kDstOutput ? task % P.out.nblk : 0;
@@ -365,6 +385,7 @@ int build_sub(int n, std::vector<HostCx>& tw, SubPlan& sp) {
     std::memset(&sp, 0, sizeof sp);
     sp.n = n;
     sp.nst = ns;
+    sp.tw0 = (int)tw.size();
     hd::RootTable rt(n);
     int rem = n, s = 1;
     for (int g = 0; g < ns; g++) {
@@ -380,6 +401,7 @@ int build_sub(int n, std::vector<HostCx>& tw, SubPlan& sp) {
         s *= r;
     }
     if (tw.empty()) tw.push_back(HostCx{});  // keep the table pointer valid for n = 1
+    sp.twn = (int)tw.size() - sp.tw0;
     return KBSRC_GPU_OK;
 }
 
@@ -514,17 +536,22 @@ int max_bfly(const SubPlan& sp) {
     return b;
 }
 
+int env_int(const char* name, int dflt);
+
+// F sequences per CTA (a divisor of `count` when one fits) and T threads, within a shared-memory budget; the
+// block also holds the sub-FFT's twiddles.
 Shape pick_shape(const SubPlan& sp, int count, size_t esize, int fmax) {
-    const size_t budget = 100 * 1024;
+    const size_t budget = (size_t)env_int("KBSRC_GPU_SMEM_KB", 100) * 1024;
+    const size_t tw = esize == 32 ? (size_t)sp.twn * esize : 0;  // double-double stages its twiddles
     int F = 1;
     for (int f = fmax; f >= 1; f--) {
-        if (2 * (size_t)sp.n * f * esize > budget) continue;
+        if (2 * (size_t)sp.n * f * esize + tw > budget) continue;
         if (F == 1) F = f;
         if (count % f == 0) { F = f; break; }
     }
     int T = ((max_bfly(sp) * F + 31) / 32) * 32;
-    T = std::max(64, std::min(256, T));
-    return Shape{F, T, 2 * (size_t)sp.n * F * esize};
+    T = std::max(64, std::min(env_int("KBSRC_GPU_THREADS", 256), T));
+    return Shape{F, T, 2 * (size_t)sp.n * F * esize + tw};
 }
 
 int env_int(const char* name, int dflt) {
@@ -593,6 +620,18 @@ int allow_large_smem() {
     KB_SMEM((k_direct<ArDDAccurate, kSrcDDReal, kDstComplex>));
 #undef KB_SMEM
     if (dev < 64) done[dev] = true;
+    return KBSRC_GPU_OK;
+}
+
+// A usable CUDA device, or KBSRC_GPU_E_NODEVICE with the runtime's reason.
+int require_device() {
+    int ndev = 0;
+    const cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev < 1) {
+        cudaGetLastError();
+        return fail(KBSRC_GPU_E_NODEVICE, std::string("no usable CUDA device: ") +
+                                              (e != cudaSuccess ? cudaGetErrorString(e) : "none found"));
+    }
     return KBSRC_GPU_OK;
 }
 
@@ -717,7 +756,7 @@ int enqueue(kbsrc_gpu_engine* e, const double* in, const double* head, const dou
 Shape direct_shape(const SubPlan& sp, size_t esize) {
     int T = ((max_bfly(sp) + 31) / 32) * 32;
     T = std::max(64, std::min(256, T));
-    return Shape{1, T, 2 * (size_t)sp.n * esize};
+    return Shape{1, T, 2 * (size_t)sp.n * esize + (esize == 32 ? (size_t)sp.twn * esize : 0)};
 }
 
 int check_desc(const kbsrc_gpu_desc* d) {
@@ -750,11 +789,7 @@ int upload_real(const double* hilo, long long n, bool dd_tables, DevBuf& out) {
 int create_impl(const kbsrc_gpu_desc* desc, kbsrc_gpu_engine** out) {
     int rc = check_desc(desc);
     if (rc) return rc;
-    int ndev = 0;
-    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) {
-        cudaGetLastError();
-        return fail(KBSRC_GPU_E_NODEVICE, "no CUDA device");
-    }
+    if ((rc = require_device()) != KBSRC_GPU_OK) return rc;
     if ((rc = allow_large_smem()) != KBSRC_GPU_OK) return rc;
     auto* e = new kbsrc_gpu_engine();
     struct Guard {
@@ -780,7 +815,7 @@ int create_impl(const kbsrc_gpu_desc* desc, kbsrc_gpu_engine** out) {
     if ((rc = upload_cx(split_roots(e->Mb), e->exact, e->w_iv)) != KBSRC_GPU_OK) return rc;
     if ((rc = upload_real(desc->H, desc->H_len, e->exact, e->H)) != KBSRC_GPU_OK) return rc;
     const size_t esize = e->exact ? 32 : 16;
-    const int fmax = env_int("KBSRC_GPU_FMAX", e->exact ? 4 : 8);
+    const int fmax = env_int("KBSRC_GPU_FMAX", e->exact ? 8 : 16);
     const HostCfft &f = e->fw.host, &v = e->iv.host;
     if (f.four) {
         e->col_fw = pick_shape(f.s1, f.N2, esize, fmax);
@@ -932,12 +967,9 @@ int kbsrc_gpu_kernel_spectrum(const double* taps, int L, int n, double scale, do
     if (!taps || !H || L < 0 || n < 2 || n % 2 || 2LL * L >= n)
         return fail(KBSRC_GPU_E_ARG, "bad kernel spectrum arguments");
     try {
-        int ndev = 0;
-        if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) {
-            cudaGetLastError();
-            return fail(KBSRC_GPU_E_NODEVICE, "no CUDA device");
-        }
-        int rc = allow_large_smem();
+        int rc = require_device();
+        if (rc) return rc;
+        rc = allow_large_smem();
         if (rc) return rc;
         // the symmetric kernel placed circularly (design.cpp:42-43)
         std::vector<double> r((size_t)2 * n, 0.0);

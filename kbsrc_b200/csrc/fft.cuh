@@ -20,6 +20,7 @@ struct Stage {
 };
 struct SubPlan {
     int n, nst;
+    int tw0, twn;  // this plan's twiddles: entries [tw0, tw0 + twn) of the table
     Stage st[kMaxStages];
 };
 
@@ -43,12 +44,20 @@ __device__ __forceinline__ cx<dd> ld_tw<dd>(const cx<dd>* p) {
     return cx<dd>{dd{a.x, a.y}, dd{b.x, b.y}};
 }
 
+// Stage twiddles are read from shared memory (double-double: staged once per CTA) or straight from the global
+// table through the read-only path (f64: a CTA's work is too short to amortise the copy).
+template <class Ar>
+__device__ __forceinline__ CxW<Ar> tw_at(const CxW<Ar>* p) {
+    if constexpr (Ar::kDD) return *p;
+    else return ld_tw(p);
+}
+
 template <class Ar>
 __device__ __forceinline__ void bfly2(const CxR<Ar>* src, int sin, CxR<Ar>* dst, int sout, const CxW<Ar>* tw,
                                       bool p0) {
     const CxR<Ar> a0 = src[0], a1 = src[sin];
     dst[0] = c_add<Ar>(a0, a1);
-    dst[sout] = p0 ? c_sub<Ar>(a0, a1) : c_mulw<Ar>(c_sub<Ar>(a0, a1), ld_tw(tw));
+    dst[sout] = p0 ? c_sub<Ar>(a0, a1) : c_mulw<Ar>(c_sub<Ar>(a0, a1), tw_at<Ar>(tw));
 }
 
 template <class Ar>
@@ -64,9 +73,9 @@ __device__ __forceinline__ void bfly4(const CxR<Ar>* src, int sin, CxR<Ar>* dst,
         dst[2 * sout] = c_sub<Ar>(t0, t2);
         dst[3 * sout] = c_sub<Ar>(t1, t3);
     } else {
-        dst[sout] = c_mulw<Ar>(c_add<Ar>(t1, t3), ld_tw(tw));
-        dst[2 * sout] = c_mulw<Ar>(c_sub<Ar>(t0, t2), ld_tw(tw + 1));
-        dst[3 * sout] = c_mulw<Ar>(c_sub<Ar>(t1, t3), ld_tw(tw + 2));
+        dst[sout] = c_mulw<Ar>(c_add<Ar>(t1, t3), tw_at<Ar>(tw));
+        dst[2 * sout] = c_mulw<Ar>(c_sub<Ar>(t0, t2), tw_at<Ar>(tw + 1));
+        dst[3 * sout] = c_mulw<Ar>(c_sub<Ar>(t1, t3), tw_at<Ar>(tw + 2));
     }
 }
 
@@ -104,20 +113,38 @@ __device__ __forceinline__ void bfly_odd(const CxR<Ar>* src, int sin, CxR<Ar>* d
             dst[u * sout] = xu;
             dst[(R - u) * sout] = xr;
         } else {
-            dst[u * sout] = c_mulw<Ar>(xu, ld_tw(tw + u - 1));
-            dst[(R - u) * sout] = c_mulw<Ar>(xr, ld_tw(tw + R - u - 1));
+            dst[u * sout] = c_mulw<Ar>(xu, tw_at<Ar>(tw + u - 1));
+            dst[(R - u) * sout] = c_mulw<Ar>(xr, tw_at<Ar>(tw + R - u - 1));
         }
     }
 }
 
-// Runs every stage of `sp` on F sequences held in `a` (layout [j*F + f]); `b` is the other buffer.
-// Returns the buffer that holds the result. Ends with the CTA synchronised.
+// Twiddles a pass reads: for double-double, the plan's stage twiddles copied to shared memory (tws, sp.twn
+// entries; the caller synchronises before use); for f64, the global table itself.
 template <class Ar>
-__device__ CxR<Ar>* stockham(const SubPlan& sp, CxR<Ar>* a, CxR<Ar>* b, int F, const CxW<Ar>* __restrict__ tw,
-                             const OddRoots<typename Ar::W>& odd) {
+__device__ __forceinline__ const CxW<Ar>* stage_twiddles(const SubPlan& sp, const CxW<Ar>* __restrict__ tw,
+                                                         CxW<Ar>* tws) {
+    if constexpr (!Ar::kDD) {
+        return tw + sp.tw0;
+    } else {
+        for (int i = threadIdx.x; i < sp.twn; i += blockDim.x) tws[i] = ld_tw(tw + sp.tw0 + i);
+        return tws;
+    }
+}
+template <class Ar>
+constexpr size_t staged_twiddle_bytes(int twn) {
+    return Ar::kDD ? (size_t)twn * sizeof(CxW<Ar>) : 0;
+}
+
+// Runs every stage of `sp` on F sequences held in `a` (layout [j*F + f]); `b` is the other buffer; `tws` the
+// plan's twiddles from stage_twiddles (entry 0 = table entry sp.tw0). Returns the buffer that holds the result.
+// Ends with the CTA synchronised.
+template <class Ar>
+__device__ __forceinline__ CxR<Ar>* stockham(const SubPlan& sp, CxR<Ar>* a, CxR<Ar>* b, int F,
+                                             const CxW<Ar>* tws, const OddRoots<typename Ar::W>& odd) {
     for (int g = 0; g < sp.nst; g++) {
         const int r = sp.st[g].r, m = sp.st[g].m, s = sp.st[g].s;
-        const CxW<Ar>* twg = tw + sp.st[g].tw;
+        const CxW<Ar>* twg = tws + (sp.st[g].tw - sp.tw0);
         const int total = m * s * F, sin = s * m * F, sout = s * F;
         for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
             const int f = idx % F, bf = idx / F, q = bf % s, p = bf / s;
