@@ -89,6 +89,19 @@ void kbsrc_gpu_engine_destroy(kbsrc_gpu_engine* e);
  * taps: (L+1) (hi, lo) pairs; H: (n/2+1) (hi, lo) pairs out. n must be even. */
 int kbsrc_gpu_kernel_spectrum(const double* taps, int L, int n, double scale, double* H);
 
+/* The same kernel spectrum for callers that cannot allocate device memory (a fixed memory pool, a real-time
+ * thread that must not enter the allocator, a region being captured into a CUDA graph by a framework that
+ * forbids allocation). No counterpart in the reference: it exists for such callers only.
+ *   d_taps  (L+1) (hi, lo) pairs in device memory; d_H  (n/2+1) (hi, lo) pairs out, device memory
+ *   stream  cudaStream_t to run on (NULL: the CUDA default stream); the call returns once the work is queued
+ * It calls no cudaMalloc, cudaFree or other allocator: its scratch is one 24 MiB device array inside the library
+ * (present on every GPU that loads it, until exit), so n is limited to about 300,000 points (80 bytes per point);
+ * larger n returns KBSRC_GPU_E_ARG with the sizes in the message. The first call on each device looks up the
+ * array's device address (cudaGetSymbolAddress) and sets kernel attributes; make that first call before any
+ * stream capture. All calls share the one array and it keeps the previous call's contents (each call rewrites
+ * what it reads), so calls that can overlap on the GPU (other streams, other threads) race: serialise them. */
+int kbsrc_gpu_kernel_spectrum_static(const double* d_taps, int L, int n, double scale, double* d_H, void* stream);
+
 /* Text of the last error on this thread ("" if none). */
 const char* kbsrc_gpu_last_error(void);
 

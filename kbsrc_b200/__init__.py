@@ -64,6 +64,8 @@ GPU_SYMBOLS = {
     "kbsrc_gpu_engine_info": (ctypes.c_int, [ctypes.c_void_p, _lp, _lp, _lp]),
     "kbsrc_gpu_engine_destroy": (None, [ctypes.c_void_p]),
     "kbsrc_gpu_kernel_spectrum": (ctypes.c_int, [_dp, ctypes.c_int, ctypes.c_int, ctypes.c_double, _dp]),
+    "kbsrc_gpu_kernel_spectrum_static": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                                        ctypes.c_void_p, ctypes.c_void_p]),
     "kbsrc_gpu_last_error": (ctypes.c_char_p, []),
     "kbsrc_gpu_engine_name": (ctypes.c_char_p, []),
 }

@@ -19,6 +19,7 @@
 #include <algorithm>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -859,6 +860,39 @@ int run_device_impl(kbsrc_gpu_engine* e, const double* in, const double* head, c
 // ------------------------------------------------------------------------------------------------------
 // C ABI
 // ------------------------------------------------------------------------------------------------------
+// ---- kernel spectrum for callers that cannot allocate device memory ----------------------------------------
+//
+// Some callers own every device allocation themselves and may not call cudaMalloc from a library: a host that
+// runs on a fixed, pre-reserved memory pool, a real-time audio thread that must not block in the allocator, or
+// code being captured into a CUDA graph by a framework that forbids allocation inside the region. For them,
+// kbsrc_gpu_kernel_spectrum_static takes its inputs and outputs in device memory and keeps all of its scratch
+// (the placed taps, two FFT work buffers, the twiddle tables) in one file-scope device array below. The array
+// is part of the library image: every GPU that loads the library holds it until the process exits.
+
+// Capacity of the shared scratch: transforms up to about 300,000 points (80 bytes per point), which covers the
+// automatic plans of the common rates (for example 201,600 points for 96 kHz -> 44.1 kHz at --len 0.2).
+constexpr size_t kSpectrumScratchBytes = (size_t)24 << 20;
+static __device__ __align__(256) unsigned char g_spectrum_scratch[kSpectrumScratchBytes];
+
+namespace {
+
+std::mutex g_scratch_mu;
+void* g_scratch_ptr[64] = {};  // device address of g_spectrum_scratch, per device, looked up on first use
+
+// r[i] = h[i] for i <= L, h[n - i] for i >= n - L, else 0 (the circular placement of design.cpp:42-43);
+// every entry is written, so nothing left by an earlier call survives.
+__global__ void k_place_taps(const double* __restrict__ taps, int L, int n, double* __restrict__ r) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int m = i <= L ? i : (i >= n - L ? n - i : -1);
+        r[2 * i] = m >= 0 ? taps[2 * m] : 0.0;
+        r[2 * i + 1] = m >= 0 ? taps[2 * m + 1] : 0.0;
+    }
+}
+
+size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
+
+}  // namespace
+
 extern "C" {
 
 int kbsrc_gpu_engine_create(const kbsrc_gpu_desc* desc, kbsrc_gpu_engine** out) {
@@ -1024,6 +1058,93 @@ int kbsrc_gpu_kernel_spectrum(const double* taps, int L, int n, double scale, do
         KB_CUDA(cudaGetLastError());
         KB_CUDA(cudaMemcpyAsync(H, Hd.p, (size_t)(h + 1) * 16, cudaMemcpyDeviceToHost, st));
         KB_CUDA(cudaStreamSynchronize(st));
+        return KBSRC_GPU_OK;
+    } catch (const std::bad_alloc&) {
+        return fail(KBSRC_GPU_E_NOMEM, "host allocation failed");
+    } catch (const std::exception& x) {
+        return fail(KBSRC_GPU_E_CUDA, x.what());
+    }
+}
+
+int kbsrc_gpu_kernel_spectrum_static(const double* d_taps, int L, int n, double scale, double* d_H, void* stream) {
+    if (!d_taps || !d_H || L < 0 || n < 2 || n % 2 || 2LL * L >= n)
+        return fail(KBSRC_GPU_E_ARG, "bad kernel spectrum arguments");
+    try {
+        int rc = require_device();
+        if (rc) return rc;
+        rc = allow_large_smem();
+        if (rc) return rc;
+        int dev = 0;
+        KB_CUDA(cudaGetDevice(&dev));
+        if (dev < 0 || dev >= 64) return fail(KBSRC_GPU_E_ARG, "device index out of range");
+        unsigned char* base = nullptr;
+        {
+            std::lock_guard<std::mutex> lock(g_scratch_mu);
+            if (!g_scratch_ptr[dev]) {
+                void* p = nullptr;
+                const cudaError_t e = cudaGetSymbolAddress(&p, g_spectrum_scratch);
+                if (e != cudaSuccess || !p)
+                    return fail(KBSRC_GPU_E_CUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
+                g_scratch_ptr[dev] = p;
+            }
+            base = static_cast<unsigned char*>(g_scratch_ptr[dev]);
+        }
+        // plan and tables on the host (dd, exactly as the allocating entry builds them)
+        const int h = n / 2;
+        HostCfft c;
+        if ((rc = build_cfft(h, c)) != KBSRC_GPU_OK) return rc;
+        const std::vector<HostCx> w = split_roots(n);
+        const size_t esize = 32;
+        const size_t off_r = 0, off_A = align256(off_r + (size_t)n * 16), off_B = align256(off_A + (size_t)(h + 1) * esize),
+                     off_w = align256(off_B + (size_t)(h + 1) * esize), off_ts = align256(off_w + w.size() * esize),
+                     off_t4 = align256(off_ts + c.tw_stage.size() * esize),
+                     end = align256(off_t4 + c.tw4.size() * esize);
+        if (end > kSpectrumScratchBytes)
+            return fail(KBSRC_GPU_E_ARG, "kernel spectrum of " + std::to_string(n) + " points needs " +
+                                             std::to_string(end) + " bytes of scratch; the static scratch holds " +
+                                             std::to_string(kSpectrumScratchBytes) + " (about 300,000 points)");
+        cudaStream_t st = static_cast<cudaStream_t>(stream);
+        auto put = [&](size_t off, const std::vector<HostCx>& v) -> int {
+            if (v.empty()) return KBSRC_GPU_OK;
+            std::vector<double> flat(v.size() * 4);
+            for (size_t i = 0; i < v.size(); i++) {
+                flat[4 * i] = v[i].re.hi; flat[4 * i + 1] = v[i].re.lo;
+                flat[4 * i + 2] = v[i].im.hi; flat[4 * i + 3] = v[i].im.lo;
+            }
+            KB_CUDA(cudaMemcpyAsync(base + off, flat.data(), flat.size() * 8, cudaMemcpyHostToDevice, st));
+            return KBSRC_GPU_OK;
+        };
+        if ((rc = put(off_w, w)) || (rc = put(off_ts, c.tw_stage)) || (rc = put(off_t4, c.tw4))) return rc;
+        using C = CxR<ArDDAccurate>;
+        double* r = reinterpret_cast<double*>(base + off_r);
+        C* A = reinterpret_cast<C*>(base + off_A);
+        C* B = reinterpret_cast<C*>(base + off_B);
+        k_place_taps<<<grid_for(n, 256), 256, 0, st>>>(d_taps, L, n, r);
+        PassParams<ArDDAccurate> p{};
+        p.tw_stage = reinterpret_cast<const CxW<ArDDAccurate>*>(base + off_ts);
+        p.odd = odd_roots<dd>();
+        p.ddreal = r;
+        p.stride = 0;
+        if (c.four) {
+            const Shape sc = pick_shape(c.s1, c.N2, esize, 4), sr = pick_shape(c.s2, c.N1, esize, 4);
+            p.sp = c.s1; p.N1 = c.N1; p.N2 = c.N2; p.F = sc.F;
+            p.tw4 = reinterpret_cast<const CxW<ArDDAccurate>*>(base + off_t4);
+            p.src = A; p.dst = A;
+            k_column<ArDDAccurate, kSrcDDReal><<<dim3((c.N2 + sc.F - 1) / sc.F, 1), sc.T, sc.smem, st>>>(p);
+            p.sp = c.s2; p.F = sr.F; p.src = A; p.dst = B;
+            k_row<ArDDAccurate, kDstComplex><<<dim3((c.N1 + sr.F - 1) / sr.F, 1), sr.T, sr.smem, st>>>(p);
+        } else {
+            const Shape sd = direct_shape(c.sd, esize);
+            p.sp = c.sd; p.F = 1; p.dst = B;
+            k_direct<ArDDAccurate, kSrcDDReal, kDstComplex><<<dim3(1, 1), sd.T, sd.smem, st>>>(p);
+        }
+        SpecParams<ArDDAccurate> s{};
+        s.Z = B; s.X = A;
+        s.w_fw = reinterpret_cast<const CxW<ArDDAccurate>*>(base + off_w);
+        s.h = h; s.scale = scale; s.Hout = reinterpret_cast<dd*>(d_H);
+        k_split<ArDDAccurate><<<grid_for(h / 2 + 1, 256), 256, 0, st>>>(s);
+        k_design_out<<<grid_for(h + 1, 256), 256, 0, st>>>(s);
+        KB_CUDA(cudaGetLastError());
         return KBSRC_GPU_OK;
     } catch (const std::bad_alloc&) {
         return fail(KBSRC_GPU_E_NOMEM, "host allocation failed");
