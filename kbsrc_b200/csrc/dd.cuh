@@ -18,7 +18,7 @@
 
 namespace kbsrc::dev {
 
-struct dd {
+struct alignas(16) dd {
     double hi, lo;
 };
 

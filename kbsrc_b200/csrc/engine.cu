@@ -73,7 +73,13 @@ __device__ __forceinline__ double signal_at(const Signal& s, int c, long long g)
 struct Output {
     double* out;
     long long nout, o, hopP, margP, nblk;
+    int ch;
 };
+
+// Tasks are numbered block-major, task = b * channels + c, so the channels of one block run side by side and
+// share the sectors of the interleaved input. The order of tasks does not affect any value.
+__device__ __forceinline__ int task_channel(long long task, int ch) { return (int)(task % ch); }
+__device__ __forceinline__ long long task_block(long long task, int ch) { return task / ch; }
 
 __device__ __forceinline__ void emit(const Output& o, int c, long long b, long long e, double v) {
     const long long k = e - o.margP;
@@ -101,17 +107,41 @@ struct PassParams {
     Output out;                   // kDstOutput
 };
 
-template <class Ar>
-__device__ __forceinline__ CxR<Ar> load_input(const PassParams<Ar>& P, int src_kind, const CxR<Ar>* src, long long i,
-                                              long long task) {
+// Where a task's first pass reads: the staged signal of one channel, a complex buffer, or dd reals.
+struct TaskSource {
+    int c;
+    long long g0;   // staged index of the block's first sample minus lead: signal frame of real sample 0
+    bool interior;  // every sample of the block lies inside the input (no edge or padding tests needed)
+};
+
+__device__ __forceinline__ TaskSource task_source(const Signal& s, long long task, long long nreal) {
+    TaskSource t;
+    t.c = task_channel(task, s.ch);
+    t.g0 = task_block(task, s.ch) * s.hopQ - s.lead;
+    t.interior = t.g0 >= 0 && t.g0 + nreal <= s.frames;
+    return t;
+}
+
+// Complex input value i of a task: (x[2i], x[2i+1]) of the staged signal (fft.hpp:363), a buffer value, or a
+// dd real pair (kernel design).
+template <class Ar, int SRC>
+__device__ __forceinline__ CxR<Ar> load_input(const PassParams<Ar>& P, const TaskSource& ts, const CxR<Ar>* src,
+                                              long long i) {
     using R = typename Ar::R;
-    if (src_kind == kSrcSignal) {
-        const int c = (int)(task / P.sig.nblk);
-        const long long b = task % P.sig.nblk, g = b * P.sig.hopQ + 2 * i;
-        return CxR<Ar>{Ar::from_f64(signal_at(P.sig, c, g)), Ar::from_f64(signal_at(P.sig, c, g + 1))};
-    }
-    if (src_kind == kSrcComplex) return src[i];
-    if constexpr (Ar::kDD) {
+    if constexpr (SRC == kSrcSignal) {
+        const long long t = ts.g0 + 2 * i;
+        double x0, x1;
+        if (ts.interior) {
+            x0 = __ldg(P.sig.in + t * P.sig.ch + ts.c);
+            x1 = __ldg(P.sig.in + (t + 1) * P.sig.ch + ts.c);
+        } else {
+            x0 = signal_at(P.sig, ts.c, t + P.sig.lead);
+            x1 = signal_at(P.sig, ts.c, t + 1 + P.sig.lead);
+        }
+        return CxR<Ar>{Ar::from_f64(x0), Ar::from_f64(x1)};
+    } else if constexpr (SRC == kSrcComplex) {
+        return src[i];
+    } else if constexpr (Ar::kDD) {
         const double2 a = __ldg(reinterpret_cast<const double2*>(P.ddreal) + 2 * i);
         const double2 b = __ldg(reinterpret_cast<const double2*>(P.ddreal) + 2 * i + 1);
         return CxR<Ar>{R{a.x, a.y}, R{b.x, b.y}};
@@ -125,10 +155,13 @@ __device__ __forceinline__ CxR<Ar> czero() {
     return CxR<Ar>{Ar::zero(), Ar::zero()};
 }
 
-// Shared memory of a pass: two sequence buffers of n*F values, then the sub-FFT's stage twiddles.
+// Loads per thread issued together before their shared-memory stores (memory-level parallelism)
+constexpr int kLoadBatch = 4;
+
+// Shared memory of a pass: two plane pairs of n*F values, then (double-double) the sub-FFT's stage twiddles.
 template <class Ar>
-__device__ __forceinline__ CxW<Ar>* twiddle_smem(unsigned char* smem, int n, int F) {
-    return reinterpret_cast<CxW<Ar>*>(smem + 2 * (size_t)n * F * sizeof(CxR<Ar>));
+__device__ __forceinline__ CxW<Ar>* twiddle_smem(unsigned char* after_planes) {
+    return reinterpret_cast<CxW<Ar>*>(after_planes);
 }
 
 // Column pass: sequences n2 in [c0, c0+F) of length N1 (stride N2), twiddle, store in place
@@ -137,34 +170,41 @@ template <class Ar, int SRC>
 __global__ void __launch_bounds__(256, Ar::kMinBlocks) k_column(const __grid_constant__ PassParams<Ar> P) {
     extern __shared__ __align__(16) unsigned char smem[];
     using C = CxR<Ar>;
-    const int F = P.F, N1 = P.N1, N2 = P.N2;
-    C* A = reinterpret_cast<C*>(smem);
-    C* B = A + N1 * F;
+    const int F = P.F, N1 = P.N1, N2 = P.N2, total = N1 * F;
+    Planes<Ar> A, B;
+    unsigned char* rest = carve<Ar>(smem, total, A, B);
     const long long task = P.task0 + blockIdx.y;
     const int c0 = blockIdx.x * F;
     const C* src = P.src + blockIdx.y * P.stride;
     C* dst = P.dst + blockIdx.y * P.stride;
-    const CxW<Ar>* tws = stage_twiddles<Ar>(P.sp, P.tw_stage, twiddle_smem<Ar>(smem, N1, F));
-    for (int e = threadIdx.x; e < N1 * F; e += blockDim.x) {
-        const int r = e / F, f = e - r * F, n2 = c0 + f;
-        A[r * F + f] = n2 < N2 ? load_input<Ar>(P, SRC, src, (long long)r * N2 + n2, task) : czero<Ar>();
-    }
-    __syncthreads();
-    const C* res = stockham<Ar>(P.sp, A, B, F, tws, P.odd);
-    // four-step twiddle and store; the table loads of a chunk are issued before any of its products
-    constexpr int kChunk = 4;
-    for (int e0 = threadIdx.x; e0 < N1 * F; e0 += kChunk * blockDim.x) {
-        CxW<Ar> w[kChunk];
+    const TaskSource ts = SRC == kSrcSignal ? task_source(P.sig, task, 2LL * N1 * N2) : TaskSource{0, 0, false};
+    const CxW<Ar>* tws = stage_twiddles<Ar>(P.sp, P.tw_stage, twiddle_smem<Ar>(rest));
+    for (int e0 = threadIdx.x; e0 < total; e0 += kLoadBatch * blockDim.x) {
+        C v[kLoadBatch];
 #pragma unroll
-        for (int j = 0; j < kChunk; j++) {
-            const int e = e0 + j * blockDim.x, k1 = e / F, n2 = c0 + (e - k1 * F);
-            if (e < N1 * F && n2 < N2 && k1 && (Ar::kLanes || n2)) w[j] = ld_tw(P.tw4 + (long long)k1 * N2 + n2);
+        for (int j = 0; j < kLoadBatch; j++) {
+            const int e = e0 + j * blockDim.x, r = e / F, n2 = c0 + (e - r * F);
+            if (e < total) v[j] = n2 < N2 ? load_input<Ar, SRC>(P, ts, src, (long long)r * N2 + n2) : czero<Ar>();
         }
 #pragma unroll
-        for (int j = 0; j < kChunk; j++) {
-            const int e = e0 + j * blockDim.x, k1 = e / F, f = e - k1 * F, n2 = c0 + f;
-            if (e >= N1 * F || n2 >= N2) continue;
-            C v = res[k1 * F + f];
+        for (int j = 0; j < kLoadBatch; j++)
+            if (e0 + j * blockDim.x < total) A.st(e0 + j * blockDim.x, v[j]);
+    }
+    __syncthreads();
+    const Planes<Ar> res = stockham<Ar>(P.sp, A, B, F, tws, P.odd);
+    // four-step twiddle and store; the table loads of a batch are issued before any of its products
+    for (int e0 = threadIdx.x; e0 < total; e0 += kLoadBatch * blockDim.x) {
+        CxW<Ar> w[kLoadBatch];
+#pragma unroll
+        for (int j = 0; j < kLoadBatch; j++) {
+            const int e = e0 + j * blockDim.x, k1 = e / F, n2 = c0 + (e - k1 * F);
+            if (e < total && n2 < N2 && k1 && (Ar::kLanes || n2)) w[j] = ld_tw(P.tw4 + (long long)k1 * N2 + n2);
+        }
+#pragma unroll
+        for (int j = 0; j < kLoadBatch; j++) {
+            const int e = e0 + j * blockDim.x, k1 = e / F, n2 = c0 + (e - k1 * F);
+            if (e >= total || n2 >= N2) continue;
+            C v = res.ld(e);
             if (k1 && (Ar::kLanes || n2)) v = c_mulw<Ar>(v, w[j]);
             if (Ar::kLaneRenorm) v = c_renorm<Ar>(v);
             dst[(long long)k1 * N2 + n2] = v;
@@ -178,26 +218,35 @@ template <class Ar, int DST>
 __global__ void __launch_bounds__(256, Ar::kMinBlocks) k_row(const __grid_constant__ PassParams<Ar> P) {
     extern __shared__ __align__(16) unsigned char smem[];
     using C = CxR<Ar>;
-    const int F = P.F, N1 = P.N1, N2 = P.N2;
-    C* A = reinterpret_cast<C*>(smem);
-    C* B = A + N2 * F;
+    const int F = P.F, N1 = P.N1, N2 = P.N2, total = N2 * F;
+    Planes<Ar> A, B;
+    unsigned char* rest = carve<Ar>(smem, total, A, B);
     const long long task = P.task0 + blockIdx.y;
     const int r0 = blockIdx.x * F;
     const C* src = P.src + blockIdx.y * P.stride;
-    const CxW<Ar>* tws = stage_twiddles<Ar>(P.sp, P.tw_stage, twiddle_smem<Ar>(smem, N2, F));
-    for (int e = threadIdx.x; e < N2 * F; e += blockDim.x) {
-        const int f = e / N2, i = e - f * N2, row = r0 + f;
-        A[i * F + f] = row < N1 ? src[(long long)row * N2 + i] : czero<Ar>();
+    const CxW<Ar>* tws = stage_twiddles<Ar>(P.sp, P.tw_stage, twiddle_smem<Ar>(rest));
+    for (int e0 = threadIdx.x; e0 < total; e0 += kLoadBatch * blockDim.x) {
+        C v[kLoadBatch];
+#pragma unroll
+        for (int j = 0; j < kLoadBatch; j++) {
+            const int e = e0 + j * blockDim.x, f = e / N2, i = e - f * N2, row = r0 + f;
+            if (e < total) v[j] = row < N1 ? src[(long long)row * N2 + i] : czero<Ar>();
+        }
+#pragma unroll
+        for (int j = 0; j < kLoadBatch; j++) {
+            const int e = e0 + j * blockDim.x, f = e / N2, i = e - f * N2;
+            if (e < total) A.st(i * F + f, v[j]);
+        }
     }
     __syncthreads();
-    const C* res = stockham<Ar>(P.sp, A, B, F, tws, P.odd);
+    const Planes<Ar> res = stockham<Ar>(P.sp, A, B, F, tws, P.odd);
     C* dst = P.dst + blockIdx.y * P.stride;
-    const int c = DST == kDstOutput ? (int)(task / P.out.nblk) : 0;
-    const long long b = DST == kDstOutput ? task % P.out.nblk : 0;
-    for (int e = threadIdx.x; e < N2 * F; e += blockDim.x) {
+    const int c = DST == kDstOutput ? task_channel(task, P.out.ch) : 0;
+    const long long b = DST == kDstOutput ? task_block(task, P.out.ch) : 0;
+    for (int e = threadIdx.x; e < total; e += blockDim.x) {
         const int k2 = e / F, f = e - k2 * F, row = r0 + f;
         if (row >= N1) continue;
-        C v = res[k2 * F + f];
+        C v = res.ld(e);
         if (Ar::kLaneRenorm) v = c_renorm<Ar>(v);
         const long long iz = (long long)N1 * k2 + row;
         if (DST == kDstComplex) {
@@ -215,19 +264,20 @@ __global__ void __launch_bounds__(256, Ar::kMinBlocks) k_direct(const __grid_con
     extern __shared__ __align__(16) unsigned char smem[];
     using C = CxR<Ar>;
     const int n = P.sp.n;
-    C* A = reinterpret_cast<C*>(smem);
-    C* B = A + n;
+    Planes<Ar> A, B;
+    unsigned char* rest = carve<Ar>(smem, n, A, B);
     const long long task = P.task0 + blockIdx.y;
     const C* src = P.src + blockIdx.y * P.stride;
-    const CxW<Ar>* tws = stage_twiddles<Ar>(P.sp, P.tw_stage, twiddle_smem<Ar>(smem, n, 1));
-    for (int i = threadIdx.x; i < n; i += blockDim.x) A[i] = load_input<Ar>(P, SRC, src, i, task);
+    const TaskSource ts = SRC == kSrcSignal ? task_source(P.sig, task, 2LL * n) : TaskSource{0, 0, false};
+    const CxW<Ar>* tws = stage_twiddles<Ar>(P.sp, P.tw_stage, twiddle_smem<Ar>(rest));
+    for (int i = threadIdx.x; i < n; i += blockDim.x) A.st(i, load_input<Ar, SRC>(P, ts, src, i));
     __syncthreads();
-    const C* res = stockham<Ar>(P.sp, A, B, 1, tws, P.odd);
+    const Planes<Ar> res = stockham<Ar>(P.sp, A, B, 1, tws, P.odd);
     C* dst = P.dst + blockIdx.y * P.stride;
-    const int c = DST == kDstOutput ? (int)(task / P.out.nblk) : 0;
-    const long long b = DST == kDstOutput ? task % P.out.nblk : 0;
+    const int c = DST == kDstOutput ? task_channel(task, P.out.ch) : 0;
+    const long long b = DST == kDstOutput ? task_block(task, P.out.ch) : 0;
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        const C v = res[i];
+        const C v = res.ld(i);
         if (DST == kDstComplex) {
             dst[i] = v;
         } else {
@@ -677,7 +727,7 @@ int enqueue(kbsrc_gpu_engine* e, const double* in, const double* head, const dou
     using WS = typename ArS::W;
     const kbsrc_gpu_desc& d = e->d;
     const Signal sig{in, head, tail, d.frames, d.edge_len, d.lead, (long long)e->hop * d.Q, d.nblk, d.channels};
-    const Output o{out, d.nout, d.o, (long long)e->hop * d.P, (long long)d.marg * d.P, d.nblk};
+    const Output o{out, d.nout, d.o, (long long)e->hop * d.P, (long long)d.marg * d.P, d.nblk, d.channels};
     CL* AL = static_cast<CL*>(e->bufA.p);
     CL* BL = static_cast<CL*>(e->bufB.p);
     CS* AS = static_cast<CS*>(e->bufA.p);

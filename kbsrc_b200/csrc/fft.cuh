@@ -52,51 +52,76 @@ __device__ __forceinline__ CxW<Ar> tw_at(const CxW<Ar>* p) {
     else return ld_tw(p);
 }
 
+// Shared-memory view of F sequences in split planes: element i = j*F + f (sample j of sequence f) has its real
+// part at re[i] and its imaginary part at im[i], so consecutive threads (consecutive f) read consecutive
+// 16-byte (dd) or 8-byte (f64) words of each plane without bank conflicts.
 template <class Ar>
-__device__ __forceinline__ void bfly2(const CxR<Ar>* src, int sin, CxR<Ar>* dst, int sout, const CxW<Ar>* tw,
-                                      bool p0) {
-    const CxR<Ar> a0 = src[0], a1 = src[sin];
-    dst[0] = c_add<Ar>(a0, a1);
-    dst[sout] = p0 ? c_sub<Ar>(a0, a1) : c_mulw<Ar>(c_sub<Ar>(a0, a1), tw_at<Ar>(tw));
+struct Planes {
+    typename Ar::R* re;
+    typename Ar::R* im;
+    __device__ __forceinline__ CxR<Ar> ld(int i) const { return CxR<Ar>{re[i], im[i]}; }
+    __device__ __forceinline__ void st(int i, const CxR<Ar>& v) const {
+        re[i] = v.re;
+        im[i] = v.im;
+    }
+};
+
+// Carves two plane pairs of nF values each from the start of shared memory; returns the first byte after them.
+template <class Ar>
+__device__ __forceinline__ unsigned char* carve(unsigned char* smem, int nF, Planes<Ar>& A, Planes<Ar>& B) {
+    using R = typename Ar::R;
+    R* p = reinterpret_cast<R*>(smem);
+    A = Planes<Ar>{p, p + nF};
+    B = Planes<Ar>{p + 2 * nF, p + 3 * nF};
+    return reinterpret_cast<unsigned char*>(p + 4 * nF);
 }
 
 template <class Ar>
-__device__ __forceinline__ void bfly4(const CxR<Ar>* src, int sin, CxR<Ar>* dst, int sout, const CxW<Ar>* tw,
-                                      bool p0) {
+__device__ __forceinline__ void bfly2(const Planes<Ar>& a, int ia, int sin, const Planes<Ar>& b, int ib, int sout,
+                                      const CxW<Ar>* tw, bool p0) {
+    const CxR<Ar> a0 = a.ld(ia), a1 = a.ld(ia + sin);
+    b.st(ib, c_add<Ar>(a0, a1));
+    b.st(ib + sout, p0 ? c_sub<Ar>(a0, a1) : c_mulw<Ar>(c_sub<Ar>(a0, a1), tw_at<Ar>(tw)));
+}
+
+template <class Ar>
+__device__ __forceinline__ void bfly4(const Planes<Ar>& a, int ia, int sin, const Planes<Ar>& b, int ib, int sout,
+                                      const CxW<Ar>* tw, bool p0) {
     using C = CxR<Ar>;
-    const C a0 = src[0], a1 = src[sin], a2 = src[2 * sin], a3 = src[3 * sin];
+    const C a0 = a.ld(ia), a1 = a.ld(ia + sin), a2 = a.ld(ia + 2 * sin), a3 = a.ld(ia + 3 * sin);
     const C t0 = c_add<Ar>(a0, a2), t1 = c_sub<Ar>(a0, a2), t2 = c_add<Ar>(a1, a3);
     const C t3 = c_mul_mi<Ar>(c_sub<Ar>(a1, a3));
-    dst[0] = c_add<Ar>(t0, t2);
+    b.st(ib, c_add<Ar>(t0, t2));
     if (p0) {
-        dst[sout] = c_add<Ar>(t1, t3);
-        dst[2 * sout] = c_sub<Ar>(t0, t2);
-        dst[3 * sout] = c_sub<Ar>(t1, t3);
+        b.st(ib + sout, c_add<Ar>(t1, t3));
+        b.st(ib + 2 * sout, c_sub<Ar>(t0, t2));
+        b.st(ib + 3 * sout, c_sub<Ar>(t1, t3));
     } else {
-        dst[sout] = c_mulw<Ar>(c_add<Ar>(t1, t3), tw_at<Ar>(tw));
-        dst[2 * sout] = c_mulw<Ar>(c_sub<Ar>(t0, t2), tw_at<Ar>(tw + 1));
-        dst[3 * sout] = c_mulw<Ar>(c_sub<Ar>(t1, t3), tw_at<Ar>(tw + 2));
+        b.st(ib + sout, c_mulw<Ar>(c_add<Ar>(t1, t3), tw_at<Ar>(tw)));
+        b.st(ib + 2 * sout, c_mulw<Ar>(c_sub<Ar>(t0, t2), tw_at<Ar>(tw + 1)));
+        b.st(ib + 3 * sout, c_mulw<Ar>(c_sub<Ar>(t1, t3), tw_at<Ar>(tw + 2)));
     }
 }
 
 // Odd radix R: x_u = a0 + sum_t S_t cos(2pi tu/R) -/+ i sum_t D_t sin(2pi tu/R) (fft.hpp:62-84)
 template <class Ar, int R>
-__device__ __forceinline__ void bfly_odd(const CxR<Ar>* src, int sin, CxR<Ar>* dst, int sout, const CxW<Ar>* tw,
-                                         bool p0, const typename Ar::W* cr, const typename Ar::W* sr) {
+__device__ __forceinline__ void bfly_odd(const Planes<Ar>& a, int ia, int sin, const Planes<Ar>& b, int ib,
+                                         int sout, const CxW<Ar>* tw, bool p0, const typename Ar::W* cr,
+                                         const typename Ar::W* sr) {
     using C = CxR<Ar>;
     constexpr int H = (R - 1) / 2;
-    const C a0 = src[0];
+    const C a0 = a.ld(ia);
     C S[H], Df[H];
 #pragma unroll
     for (int t = 1; t <= H; t++) {
-        const C x = src[t * sin], y = src[(R - t) * sin];
+        const C x = a.ld(ia + t * sin), y = a.ld(ia + (R - t) * sin);
         S[t - 1] = c_add<Ar>(x, y);
         Df[t - 1] = c_sub<Ar>(x, y);
     }
     C sum = a0;
 #pragma unroll
     for (int t = 0; t < H; t++) sum = c_add<Ar>(sum, S[t]);
-    dst[0] = sum;
+    b.st(ib, sum);
 #pragma unroll
     for (int u = 1; u <= H; u++) {
         C A = a0, B = {Ar::zero(), Ar::zero()};
@@ -110,11 +135,11 @@ __device__ __forceinline__ void bfly_odd(const CxR<Ar>* src, int sin, CxR<Ar>* d
         const C xu = {Ar::add(A.re, B.im), Ar::sub(A.im, B.re)};
         const C xr = {Ar::sub(A.re, B.im), Ar::add(A.im, B.re)};
         if (p0) {
-            dst[u * sout] = xu;
-            dst[(R - u) * sout] = xr;
+            b.st(ib + u * sout, xu);
+            b.st(ib + (R - u) * sout, xr);
         } else {
-            dst[u * sout] = c_mulw<Ar>(xu, tw_at<Ar>(tw + u - 1));
-            dst[(R - u) * sout] = c_mulw<Ar>(xr, tw_at<Ar>(tw + R - u - 1));
+            b.st(ib + u * sout, c_mulw<Ar>(xu, tw_at<Ar>(tw + u - 1)));
+            b.st(ib + (R - u) * sout, c_mulw<Ar>(xr, tw_at<Ar>(tw + R - u - 1)));
         }
     }
 }
@@ -131,35 +156,30 @@ __device__ __forceinline__ const CxW<Ar>* stage_twiddles(const SubPlan& sp, cons
         return tws;
     }
 }
-template <class Ar>
-constexpr size_t staged_twiddle_bytes(int twn) {
-    return Ar::kDD ? (size_t)twn * sizeof(CxW<Ar>) : 0;
-}
 
-// Runs every stage of `sp` on F sequences held in `a` (layout [j*F + f]); `b` is the other buffer; `tws` the
-// plan's twiddles from stage_twiddles (entry 0 = table entry sp.tw0). Returns the buffer that holds the result.
-// Ends with the CTA synchronised.
+// Runs every stage of `sp` on F sequences held in `a` (element j of sequence f at j*F + f); `b` is the other
+// plane pair; `tws` the plan's twiddles from stage_twiddles (entry 0 = table entry sp.tw0). Returns the planes
+// that hold the result. Ends with the CTA synchronised.
 template <class Ar>
-__device__ __forceinline__ CxR<Ar>* stockham(const SubPlan& sp, CxR<Ar>* a, CxR<Ar>* b, int F,
-                                             const CxW<Ar>* tws, const OddRoots<typename Ar::W>& odd) {
+__device__ __forceinline__ Planes<Ar> stockham(const SubPlan& sp, Planes<Ar> a, Planes<Ar> b, int F,
+                                               const CxW<Ar>* tws, const OddRoots<typename Ar::W>& odd) {
     for (int g = 0; g < sp.nst; g++) {
         const int r = sp.st[g].r, m = sp.st[g].m, s = sp.st[g].s;
         const CxW<Ar>* twg = tws + (sp.st[g].tw - sp.tw0);
         const int total = m * s * F, sin = s * m * F, sout = s * F;
         for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
             const int f = idx % F, bf = idx / F, q = bf % s, p = bf / s;
-            const CxR<Ar>* src = a + (s * p + q) * F + f;
-            CxR<Ar>* dst = b + (s * r * p + q) * F + f;
+            const int ia = (s * p + q) * F + f, ib = (s * r * p + q) * F + f;
             const CxW<Ar>* t = twg + p * (r - 1);
             const bool p0 = p == 0;
-            if (r == 4) bfly4<Ar>(src, sin, dst, sout, t, p0);
-            else if (r == 2) bfly2<Ar>(src, sin, dst, sout, t, p0);
-            else if (r == 3) bfly_odd<Ar, 3>(src, sin, dst, sout, t, p0, odd.c[0], odd.s[0]);
-            else if (r == 5) bfly_odd<Ar, 5>(src, sin, dst, sout, t, p0, odd.c[1], odd.s[1]);
-            else bfly_odd<Ar, 7>(src, sin, dst, sout, t, p0, odd.c[2], odd.s[2]);
+            if (r == 4) bfly4<Ar>(a, ia, sin, b, ib, sout, t, p0);
+            else if (r == 2) bfly2<Ar>(a, ia, sin, b, ib, sout, t, p0);
+            else if (r == 3) bfly_odd<Ar, 3>(a, ia, sin, b, ib, sout, t, p0, odd.c[0], odd.s[0]);
+            else if (r == 5) bfly_odd<Ar, 5>(a, ia, sin, b, ib, sout, t, p0, odd.c[1], odd.s[1]);
+            else bfly_odd<Ar, 7>(a, ia, sin, b, ib, sout, t, p0, odd.c[2], odd.s[2]);
         }
         __syncthreads();
-        CxR<Ar>* t = a;
+        const Planes<Ar> t = a;
         a = b;
         b = t;
     }
