@@ -96,7 +96,8 @@ int kbsrc_gpu_kernel_spectrum(const double* taps, int L, int n, double scale, do
  *   stream  cudaStream_t to run on (NULL: the CUDA default stream); the call returns once the work is queued
  * It calls no cudaMalloc, cudaFree or other allocator: its scratch is one 24 MiB device array inside the library
  * (present on every GPU that loads it, until exit), so n is limited to about 300,000 points (80 bytes per point);
- * larger n returns KBSRC_GPU_E_ARG with the sizes in the message. The first call on each device looks up the
+ * larger n returns KBSRC_GPU_E_ARG with the sizes in the message, and n/2 must be 7-smooth (otherwise
+ * KBSRC_GPU_E_UNSUPPORTED: the Bluestein tables would need more scratch). The first call on each device looks up the
  * array's device address (cudaGetSymbolAddress) and sets kernel attributes; make that first call before any
  * stream capture. All calls share the one array and it keeps the previous call's contents (each call rewrites
  * what it reads), so calls that can overlap on the GPU (other streams, other threads) race: serialise them. */

@@ -19,6 +19,7 @@
 #include <algorithm>
 #include <cstdlib>
 #include <cstring>
+#include <memory>
 #include <mutex>
 #include <new>
 #include <string>
@@ -105,6 +106,9 @@ struct PassParams {
     Signal sig;                   // kSrcSignal
     const double* ddreal;         // kSrcDDReal: (hi, lo) pairs
     Output out;                   // kDstOutput
+    const CxW<Ar>* bc;            // Bluestein chirp (bn entries) and kernel spectrum (bm entries)
+    const CxW<Ar>* vf;
+    int bn, bm;
 };
 
 // Where a task's first pass reads: the staged signal of one channel, a complex buffer, or dd reals.
@@ -287,6 +291,54 @@ __global__ void __launch_bounds__(256, Ar::kMinBlocks) k_direct(const __grid_con
     }
 }
 
+// Bluestein (chirp-z) steps for lengths that are not 7-smooth (fft.hpp:268-277), n points through an m-point
+// smooth transform: u = x conj(b) zero-padded to m; U = FFT(u); A = conj(U Vf); C = FFT(A); y = conj(C) conj(b).
+// Scalar arithmetic (accurate dd in exact).
+template <class Ar, int SRC>
+__global__ void k_blue_pre(const __grid_constant__ PassParams<Ar> P) {
+    using C = CxR<Ar>;
+    const long long task = P.task0 + blockIdx.y;
+    const C* src = P.src + blockIdx.y * P.stride;
+    C* dst = P.dst + blockIdx.y * P.stride;
+    const TaskSource ts = SRC == kSrcSignal ? task_source(P.sig, task, 2LL * P.bn) : TaskSource{0, 0, false};
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < P.bm; j += gridDim.x * blockDim.x) {
+        if (j < P.bn) {
+            const CxW<Ar> b = ld_tw(P.bc + j);
+            dst[j] = c_mulw<Ar>(load_input<Ar, SRC>(P, ts, src, j), CxW<Ar>{b.re, w_neg(b.im)});
+        } else {
+            dst[j] = czero<Ar>();
+        }
+    }
+}
+
+template <class Ar>
+__global__ void k_blue_mid(const __grid_constant__ PassParams<Ar> P) {
+    const CxR<Ar>* src = P.src + blockIdx.y * P.stride;
+    CxR<Ar>* dst = P.dst + blockIdx.y * P.stride;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < P.bm; k += gridDim.x * blockDim.x)
+        dst[k] = c_conj<Ar>(c_mulw<Ar>(src[k], ld_tw(P.vf + k)));
+}
+
+template <class Ar, int DST>
+__global__ void k_blue_post(const __grid_constant__ PassParams<Ar> P) {
+    using C = CxR<Ar>;
+    const long long task = P.task0 + blockIdx.y;
+    const C* src = P.src + blockIdx.y * P.stride;
+    C* dst = P.dst + blockIdx.y * P.stride;
+    const int c = DST == kDstOutput ? task_channel(task, P.out.ch) : 0;
+    const long long b = DST == kDstOutput ? task_block(task, P.out.ch) : 0;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < P.bn; k += gridDim.x * blockDim.x) {
+        const CxW<Ar> w = ld_tw(P.bc + k);
+        const C y = c_mulw<Ar>(c_conj<Ar>(src[k]), CxW<Ar>{w.re, w_neg(w.im)});
+        if (DST == kDstComplex) {
+            dst[k] = y;
+        } else {
+            emit(P.out, c, b, 2LL * k, Ar::to_f64(y.re));
+            emit(P.out, c, b, 2LL * k + 1, Ar::to_f64(Ar::neg(y.im)));
+        }
+    }
+}
+
 // ------------------------------------------------------------------------------------------------------
 // real-FFT split, spectrum, real-FFT merge
 // ------------------------------------------------------------------------------------------------------
@@ -301,6 +353,7 @@ struct SpecParams {
     const typename Ar::W* H;
     int h, hi;           // Nb/2 and Mb/2
     int Nb, Mb, up;
+    int Jg;              // general-fold bin limit, 0 otherwise
     double scale;        // kernel design: H = X.re / scale
     typename Ar::W* Hout;
 };
@@ -349,6 +402,27 @@ template <class Ar>
 __device__ __forceinline__ CxR<Ar> spectrum_bin(const SpecParams<Ar>& P, const CxR<Ar>* X, int k) {
     using C = CxR<Ar>;
     const int Nb = P.Nb, Mb = P.Mb;
+    if (P.Jg) {
+        // General fold (resampler.cpp:53-63): bin j <= Jg of the true kernel response lands on j mod Mb, on
+        // Mb - (j mod Mb) conjugated when above Mb/2, and bins 0 and Mb/2 take twice the real part (bin j = 0
+        // whole). Bin k collects j = k, Mb-k, Mb+k, 2Mb-k, ... in that (increasing) order, as the loop over j did.
+        const bool edge = k == 0 || 2 * k == Mb;
+        C y = czero<Ar>();
+        auto take = [&](long long j, bool mirrored) {
+            const int jj = (int)(j % Nb);
+            const C x = jj <= Nb / 2 ? X[jj] : c_conj<Ar>(X[Nb - jj]);
+            const C v = c_scale<Ar>(x, Ar::from_w(ld_w(P.H + j)));
+            if (j == 0) y = c_add<Ar>(y, v);
+            else if (edge) y.re = Ar::add(y.re, Ar::mul(Ar::from_f64(2.0), v.re));
+            else y = c_add<Ar>(y, mirrored ? c_conj<Ar>(v) : v);
+        };
+        for (long long base = 0; base + k <= P.Jg; base += Mb) {
+            take(base + k, false);
+            if (!edge && base + Mb - k <= P.Jg) take(base + Mb - k, true);
+        }
+        if (edge) y.im = Ar::zero();
+        return y;
+    }
     if (P.up) {
         const int kk = k % Nb;
         const C v = kk <= Nb / 2 ? X[kk] : c_conj<Ar>(X[Nb - kk]);
@@ -559,22 +633,6 @@ OddRoots<W> odd_roots() {
     return o;
 }
 
-// A complex FFT resident on the device
-struct DevCfft {
-    HostCfft host;  // shapes and sub-plans (tables released after upload)
-    DevBuf tw_stage, tw4;
-};
-
-int make_dev_cfft(int n, bool dd_tables, DevCfft& d) {
-    int rc = build_cfft(n, d.host);
-    if (rc) return rc;
-    if ((rc = upload_cx(d.host.tw_stage, dd_tables, d.tw_stage)) != KBSRC_GPU_OK) return rc;
-    if (d.host.four && (rc = upload_cx(d.host.tw4, dd_tables, d.tw4)) != KBSRC_GPU_OK) return rc;
-    std::vector<HostCx>().swap(d.host.tw_stage);
-    std::vector<HostCx>().swap(d.host.tw4);
-    return KBSRC_GPU_OK;
-}
-
 // Launch shape of a shared-memory pass over sequences of length n: F sequences per CTA, T threads.
 struct Shape {
     int F, T;
@@ -590,10 +648,10 @@ int max_bfly(const SubPlan& sp) {
 int env_int(const char* name, int dflt);
 
 // F sequences per CTA (a divisor of `count` when one fits) and T threads, within a shared-memory budget; the
-// block also holds the sub-FFT's twiddles.
+// block also holds the sub-FFT's twiddles in double-double.
 Shape pick_shape(const SubPlan& sp, int count, size_t esize, int fmax) {
     const size_t budget = (size_t)env_int("KBSRC_GPU_SMEM_KB", 100) * 1024;
-    const size_t tw = esize == 32 ? (size_t)sp.twn * esize : 0;  // double-double stages its twiddles
+    const size_t tw = esize == 32 ? (size_t)sp.twn * esize : 0;
     int F = 1;
     for (int f = fmax; f >= 1; f--) {
         if (2 * (size_t)sp.n * f * esize + tw > budget) continue;
@@ -603,6 +661,64 @@ Shape pick_shape(const SubPlan& sp, int count, size_t esize, int fmax) {
     int T = ((max_bfly(sp) * F + 31) / 32) * 32;
     T = std::max(64, std::min(env_int("KBSRC_GPU_THREADS", 256), T));
     return Shape{F, T, 2 * (size_t)sp.n * F * esize + tw};
+}
+
+Shape direct_shape(const SubPlan& sp, size_t esize) {
+    int T = ((max_bfly(sp) + 31) / 32) * 32;
+    T = std::max(64, std::min(256, T));
+    return Shape{1, T, 2 * (size_t)sp.n * esize + (esize == 32 ? (size_t)sp.twn * esize : 0)};
+}
+
+long long next_smooth7(long long n) {
+    while (!hd::smooth7(n)) n++;
+    return n;
+}
+
+// A complex FFT resident on the device: a smooth plan (direct or four-step) with its twiddle tables and launch
+// shapes, or Bluestein's chirp-z for a length that is not 7-smooth (fft.hpp:228-240): n points through the
+// m-point smooth transform `inner`, with the chirp bc[t] = e^{+i pi t^2/n} and Vf = FFT(v)/m, v the chirp
+// placed at t and m - t (computed once on the GPU with the scalar double-double FFT, as the reference does with
+// CFFT<dd,dd,dd>).
+struct DevCfft {
+    HostCfft host;  // shapes and sub-plans (tables released after upload)
+    DevBuf tw_stage, tw4;
+    Shape col{}, row{}, dir{};
+    int n = 0, m = 0;
+    std::unique_ptr<DevCfft> inner;
+    DevBuf bc, vf;
+    long long slot() const { return m ? m : n; }  // complex values one task slot must hold
+};
+
+int bluestein_kernel(DevCfft& d, bool dd_tables, cudaStream_t st);  // Vf, defined with the launchers
+
+int make_dev_cfft(int n, bool dd_tables, int fmax, DevCfft& d, cudaStream_t st) {
+    d.n = n;
+    int rc;
+    const size_t esize = dd_tables ? 32 : 16;
+    if (!hd::smooth7(n)) {
+        d.m = (int)next_smooth7(2LL * n - 1);
+        d.inner = std::make_unique<DevCfft>();
+        if ((rc = make_dev_cfft(d.m, dd_tables, fmax, *d.inner, st)) != KBSRC_GPU_OK) return rc;
+        std::vector<HostCx> bc((size_t)n);
+        for (long long t = 0; t < n; t++) {
+            const long long e = (long long)((__int128)t * t % (2LL * n));
+            hd::unit_root(e, 2LL * n, bc[t].re, bc[t].im);
+        }
+        if ((rc = upload_cx(bc, dd_tables, d.bc)) != KBSRC_GPU_OK) return rc;
+        return bluestein_kernel(d, dd_tables, st);
+    }
+    if ((rc = build_cfft(n, d.host)) != KBSRC_GPU_OK) return rc;
+    if ((rc = upload_cx(d.host.tw_stage, dd_tables, d.tw_stage)) != KBSRC_GPU_OK) return rc;
+    if (d.host.four && (rc = upload_cx(d.host.tw4, dd_tables, d.tw4)) != KBSRC_GPU_OK) return rc;
+    std::vector<HostCx>().swap(d.host.tw_stage);
+    std::vector<HostCx>().swap(d.host.tw4);
+    if (d.host.four) {
+        d.col = pick_shape(d.host.s1, d.host.N2, esize, fmax);
+        d.row = pick_shape(d.host.s2, d.host.N1, esize, fmax);
+    } else {
+        d.dir = direct_shape(d.host.sd, esize);
+    }
+    return KBSRC_GPU_OK;
 }
 
 int env_int(const char* name, int dflt) {
@@ -626,9 +742,6 @@ struct kbsrc_gpu_engine {
     DevBuf w_fw, w_iv, H;
     DevBuf bufA, bufB;
     DevBuf d_in, d_head, d_tail, d_out;
-    Shape col_fw{}, row_fw{}, col_iv{}, row_iv{}, dir_fw{}, dir_iv{};
-    OddRoots<dd> odd_dd{};
-    OddRoots<double> odd_f64{};
     std::vector<cudaEvent_t> events;  // per-pass timing trail, created on first use
     ~kbsrc_gpu_engine() {
         for (cudaEvent_t x : events) cudaEventDestroy(x);
@@ -638,16 +751,18 @@ struct kbsrc_gpu_engine {
 
 namespace {
 
+// Radix 3/5/7 constants, computed once per process
 template <class W>
-const OddRoots<W>& odd_of(const kbsrc_gpu_engine* e);
-template <>
-const OddRoots<dd>& odd_of<dd>(const kbsrc_gpu_engine* e) { return e->odd_dd; }
-template <>
-const OddRoots<double>& odd_of<double>(const kbsrc_gpu_engine* e) { return e->odd_f64; }
+const OddRoots<W>& odd_table() {
+    static const OddRoots<W> t = odd_roots<W>();
+    return t;
+}
 
 // Lets every pass kernel use up to the device's shared memory per block (once per device).
 int allow_large_smem() {
     static bool done[64] = {};
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lock(mu);
     int dev = 0;
     KB_CUDA(cudaGetDevice(&dev));
     if (dev < 64 && done[dev]) return KBSRC_GPU_OK;
@@ -659,14 +774,17 @@ int allow_large_smem() {
     KB_SMEM((k_column<ArDDShort, kSrcSignal>));
     KB_SMEM((k_column<ArDDShort, kSrcComplex>));
     KB_SMEM((k_column<ArDDAccurate, kSrcDDReal>));
+    KB_SMEM((k_column<ArDDAccurate, kSrcComplex>));
     KB_SMEM((k_row<ArF64, kDstComplex>));
     KB_SMEM((k_row<ArF64, kDstOutput>));
     KB_SMEM((k_row<ArDDShort, kDstComplex>));
     KB_SMEM((k_row<ArDDShort, kDstOutput>));
     KB_SMEM((k_row<ArDDAccurate, kDstComplex>));
     KB_SMEM((k_direct<ArF64, kSrcSignal, kDstComplex>));
+    KB_SMEM((k_direct<ArF64, kSrcComplex, kDstComplex>));
     KB_SMEM((k_direct<ArF64, kSrcComplex, kDstOutput>));
     KB_SMEM((k_direct<ArDDAccurate, kSrcSignal, kDstComplex>));
+    KB_SMEM((k_direct<ArDDAccurate, kSrcComplex, kDstComplex>));
     KB_SMEM((k_direct<ArDDAccurate, kSrcComplex, kDstOutput>));
     KB_SMEM((k_direct<ArDDAccurate, kSrcDDReal, kDstComplex>));
 #undef KB_SMEM
@@ -691,16 +809,17 @@ unsigned grid_for(long long n, int threads) {
     return (unsigned)std::max(1LL, std::min(b, 65535LL));
 }
 
-// Enqueues all passes for every wave of tasks. ArL: four-step sub-FFT arithmetic, ArS: everything else.
 // Pass kinds for per-pass timing (kbsrc_gpu_engine_run_device_timed)
 enum PassKind { kFwdA = 0, kFwdB, kSplit, kMerge, kInvA, kInvB, kPassKinds };
 
-// Optional per-launch event trail: marks[0] before the first launch, then one event after each launch.
+// Optional per-launch event trail: an event before the first launch, then one after each launch.
 struct Trail {
     std::vector<cudaEvent_t>* ev = nullptr;
     std::vector<int>* kind = nullptr;
     size_t n = 0;
+    long long launches = 0;
     int mark(cudaStream_t st, int k) {
+        if (k >= 0) launches++;
         if (!ev) return KBSRC_GPU_OK;
         if (n >= ev->size()) {
             cudaEvent_t x;
@@ -714,100 +833,188 @@ struct Trail {
     }
 };
 
+// What every pass of one launch group shares: task slots, the signal view, the output.
+struct Slots {
+    long long stride, task0;
+    unsigned nt;
+    Signal sig;
+    const double* ddreal;
+    Output out;
+};
+
+template <class Ar>
+PassParams<Ar> pass_params(const Slots& sl, const DevCfft& c, void* src, void* dst) {
+    PassParams<Ar> p{};
+    p.tw_stage = static_cast<const CxW<Ar>*>(c.tw_stage.p);
+    p.tw4 = static_cast<const CxW<Ar>*>(c.tw4.p);
+    p.odd = odd_table<typename Ar::W>();
+    p.src = static_cast<CxR<Ar>*>(src);
+    p.dst = static_cast<CxR<Ar>*>(dst);
+    p.stride = sl.stride;
+    p.task0 = sl.task0;
+    p.sig = sl.sig;
+    p.ddreal = sl.ddreal;
+    p.out = sl.out;
+    return p;
+}
+
+// The smooth complex FFT `c` of every slot: input from SRC (x when complex; the four-step column pass works in
+// place on x), result to y in natural order, or to the output epilogue (DST). ArL: four-step sub-FFT
+// arithmetic; ArS: the direct transform's.
+template <class ArL, class ArS, int SRC, int DST>
+int launch_smooth(const DevCfft& c, const Slots& sl, void* x, void* y, cudaStream_t st, Trail& tr, int kA, int kB) {
+    const HostCfft& h = c.host;
+    int rc;
+    if (h.four) {
+        PassParams<ArL> p = pass_params<ArL>(sl, c, x, x);
+        p.sp = h.s1; p.N1 = h.N1; p.N2 = h.N2; p.F = c.col.F;
+        k_column<ArL, SRC><<<dim3((h.N2 + p.F - 1) / p.F, sl.nt), c.col.T, c.col.smem, st>>>(p);
+        if ((rc = tr.mark(st, kA)) != KBSRC_GPU_OK) return rc;
+        p.sp = h.s2; p.F = c.row.F; p.src = static_cast<CxR<ArL>*>(x); p.dst = static_cast<CxR<ArL>*>(y);
+        k_row<ArL, DST><<<dim3((h.N1 + p.F - 1) / p.F, sl.nt), c.row.T, c.row.smem, st>>>(p);
+        return tr.mark(st, kB);
+    }
+    PassParams<ArS> p = pass_params<ArS>(sl, c, x, y);
+    p.sp = h.sd; p.F = 1;
+    k_direct<ArS, SRC, DST><<<dim3(1, sl.nt), c.dir.T, c.dir.smem, st>>>(p);
+    return tr.mark(st, kA);
+}
+
+// Any complex FFT: smooth, or Bluestein (pre -> inner -> kernel -> inner -> post) through the work buffers
+// a and b (m values per slot each). x: complex input when SRC says so (read before a and b are written, so it
+// may alias b); y: the result (may alias a), unless DST writes the output.
+template <class ArL, class ArS, int SRC, int DST>
+int launch_cfft(const DevCfft& c, const Slots& sl, void* x, void* a, void* b, void* y, cudaStream_t st, Trail& tr,
+                int kA, int kB) {
+    if (!c.m) return launch_smooth<ArL, ArS, SRC, DST>(c, sl, x, y, st, tr, kA, kB);
+    int rc;
+    PassParams<ArS> p = pass_params<ArS>(sl, c, x, a);
+    p.bc = static_cast<const CxW<ArS>*>(c.bc.p);
+    p.vf = static_cast<const CxW<ArS>*>(c.vf.p);
+    p.bn = c.n;
+    p.bm = c.m;
+    const dim3 gm(grid_for(c.m, 256), sl.nt), gn(grid_for(c.n, 256), sl.nt);
+    k_blue_pre<ArS, SRC><<<gm, 256, 0, st>>>(p);
+    if ((rc = tr.mark(st, kA)) != KBSRC_GPU_OK) return rc;
+    if ((rc = launch_smooth<ArL, ArS, kSrcComplex, kDstComplex>(*c.inner, sl, a, b, st, tr, kA, kB)) != KBSRC_GPU_OK)
+        return rc;
+    p.src = static_cast<CxR<ArS>*>(b);
+    p.dst = static_cast<CxR<ArS>*>(a);
+    k_blue_mid<ArS><<<gm, 256, 0, st>>>(p);
+    if ((rc = tr.mark(st, kA)) != KBSRC_GPU_OK) return rc;
+    if ((rc = launch_smooth<ArL, ArS, kSrcComplex, kDstComplex>(*c.inner, sl, a, b, st, tr, kA, kB)) != KBSRC_GPU_OK)
+        return rc;
+    p.src = static_cast<CxR<ArS>*>(b);
+    p.dst = static_cast<CxR<ArS>*>(y);
+    k_blue_post<ArS, DST><<<gn, 256, 0, st>>>(p);
+    return tr.mark(st, kA);
+}
+
+// Vf = FFT(v)/m for Bluestein, v[t] = v[m-t] = e^{+i pi t^2/n} (fft.hpp:230-238): the m-point transform in
+// scalar double-double (the reference's CFFT<dd,dd,dd>), divided by m in dd, stored in the engine's precision.
+__global__ void k_vf_scale(const cx<dd>* __restrict__ V, int m, double* __restrict__ out, int dd_out) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x) {
+        const dd re = div_dd_f64(V[k].re, (double)m), im = div_dd_f64(V[k].im, (double)m);
+        if (dd_out) {
+            out[4 * k] = re.hi; out[4 * k + 1] = re.lo; out[4 * k + 2] = im.hi; out[4 * k + 3] = im.lo;
+        } else {
+            out[2 * k] = re.hi; out[2 * k + 1] = im.hi;
+        }
+    }
+}
+
+int bluestein_kernel(DevCfft& d, bool dd_tables, cudaStream_t st) {
+    const int n = d.n, m = d.m;
+    std::vector<HostCx> v((size_t)m);
+    for (long long t = 0; t < n; t++) {
+        const long long e = (long long)((__int128)t * t % (2LL * n));
+        hd::unit_root(e, 2LL * n, v[t].re, v[t].im);
+        if (t) v[m - t] = v[t];
+    }
+    DevCfft des;  // the same m-point plan with double-double tables, run in scalar dd
+    int rc;
+    if ((rc = make_dev_cfft(m, true, 4, des, st)) != KBSRC_GPU_OK) return rc;
+    DevBuf vin, vout;
+    if ((rc = upload_cx(v, true, vin)) != KBSRC_GPU_OK) return rc;
+    if ((rc = vout.alloc((size_t)m * 32)) != KBSRC_GPU_OK) return rc;
+    if ((rc = d.vf.alloc((size_t)m * (dd_tables ? 32 : 16))) != KBSRC_GPU_OK) return rc;
+    Slots sl{};
+    sl.nt = 1;
+    Trail tr;
+    if ((rc = launch_smooth<ArDDAccurate, ArDDAccurate, kSrcComplex, kDstComplex>(des, sl, vin.p, vout.p, st, tr, -1,
+                                                                                  -1)) != KBSRC_GPU_OK)
+        return rc;
+    k_vf_scale<<<grid_for(m, 256), 256, 0, st>>>(static_cast<const cx<dd>*>(vout.p), m, static_cast<double*>(d.vf.p),
+                                                  dd_tables ? 1 : 0);
+    KB_CUDA(cudaGetLastError());
+    KB_CUDA(cudaStreamSynchronize(st));  // the temporaries are freed on return
+    return KBSRC_GPU_OK;
+}
+
+// Enqueues the block loop for every wave of tasks. ArL: four-step sub-FFT arithmetic, ArS: everything else.
 template <class ArL, class ArS>
 int enqueue(kbsrc_gpu_engine* e, const double* in, const double* head, const double* tail, double* out,
             cudaStream_t st, Trail* trail) {
+    static_assert(sizeof(CxR<ArL>) == sizeof(CxR<ArS>), "one element size per mode");
+    using CS = CxR<ArS>;
+    using WS = typename ArS::W;
     Trail none;
     Trail& tr = trail ? *trail : none;
-    int rc;
-    using CL = CxR<ArL>;
-    using CS = CxR<ArS>;
-    static_assert(sizeof(CL) == sizeof(CS), "one element size per mode");
-    using WL = typename ArL::W;
-    using WS = typename ArS::W;
     const kbsrc_gpu_desc& d = e->d;
-    const Signal sig{in, head, tail, d.frames, d.edge_len, d.lead, (long long)e->hop * d.Q, d.nblk, d.channels};
-    const Output o{out, d.nout, d.o, (long long)e->hop * d.P, (long long)d.marg * d.P, d.nblk, d.channels};
-    CL* AL = static_cast<CL*>(e->bufA.p);
-    CL* BL = static_cast<CL*>(e->bufB.p);
-    CS* AS = static_cast<CS*>(e->bufA.p);
-    CS* BS = static_cast<CS*>(e->bufB.p);
-    long long launches = 0;
+    Slots sl{};
+    sl.stride = e->stride;
+    sl.sig = Signal{in, head, tail, d.frames, d.edge_len, d.lead, (long long)e->hop * d.Q, d.nblk, d.channels};
+    sl.out = Output{out, d.nout, d.o, (long long)e->hop * d.P, (long long)d.marg * d.P, d.nblk, d.channels};
+    void* buf[2] = {e->bufA.p, e->bufB.p};
+    int rc;
     if ((rc = tr.mark(st, -1)) != KBSRC_GPU_OK) return rc;
     for (long long t0 = 0; t0 < e->tasks; t0 += e->wave) {
-        const unsigned nt = (unsigned)std::min(e->wave, e->tasks - t0);
-        // forward real FFT: gather + complex FFT into B (natural order)
-        if (e->fw.host.four) {
-            const HostCfft& c = e->fw.host;
-            PassParams<ArL> p{};
-            p.sp = c.s1; p.N1 = c.N1; p.N2 = c.N2; p.F = e->col_fw.F;
-            p.tw_stage = static_cast<const CxW<ArL>*>(e->fw.tw_stage.p);
-            p.tw4 = static_cast<const CxW<ArL>*>(e->fw.tw4.p);
-            p.odd = odd_of<WL>(e);
-            p.src = AL; p.dst = AL; p.stride = e->stride; p.task0 = t0; p.sig = sig;
-            k_column<ArL, kSrcSignal><<<dim3((c.N2 + p.F - 1) / p.F, nt), e->col_fw.T, e->col_fw.smem, st>>>(p);
-            if ((rc = tr.mark(st, kFwdA)) != KBSRC_GPU_OK) return rc;
-            p.sp = c.s2; p.F = e->row_fw.F; p.src = AL; p.dst = BL;
-            k_row<ArL, kDstComplex><<<dim3((c.N1 + p.F - 1) / p.F, nt), e->row_fw.T, e->row_fw.smem, st>>>(p);
-            if ((rc = tr.mark(st, kFwdB)) != KBSRC_GPU_OK) return rc;
-            launches += 2;
+        sl.task0 = t0;
+        sl.nt = (unsigned)std::min(e->wave, e->tasks - t0);
+        // forward real FFT: gather + complex FFT; the spectrum Z lands in buf[z]
+        int z;
+        if (e->fw.m) {
+            z = 0;
+            rc = launch_cfft<ArL, ArS, kSrcSignal, kDstComplex>(e->fw, sl, nullptr, buf[0], buf[1], buf[0], st, tr,
+                                                                 kFwdA, kFwdB);
         } else {
-            PassParams<ArS> p{};
-            p.sp = e->fw.host.sd; p.F = 1;
-            p.tw_stage = static_cast<const CxW<ArS>*>(e->fw.tw_stage.p);
-            p.odd = odd_of<WS>(e);
-            p.src = AS; p.dst = BS; p.stride = e->stride; p.task0 = t0; p.sig = sig;
-            k_direct<ArS, kSrcSignal, kDstComplex><<<dim3(1, nt), e->dir_fw.T, e->dir_fw.smem, st>>>(p);
-            if ((rc = tr.mark(st, kFwdA)) != KBSRC_GPU_OK) return rc;
-            launches += 1;
+            z = 1;
+            rc = launch_cfft<ArL, ArS, kSrcSignal, kDstComplex>(e->fw, sl, buf[0], nullptr, nullptr, buf[1], st, tr,
+                                                                 kFwdA, kFwdB);
         }
-        // split into the real spectrum (B -> A), multiply/fold and merge (A -> B)
+        if (rc) return rc;
+        // split into the real spectrum (buf[z] -> buf[1-z]), multiply/fold and merge (buf[1-z] -> buf[z])
         SpecParams<ArS> s{};
-        s.Z = BS; s.X = AS; s.Zi = BS; s.stride = e->stride;
+        s.Z = static_cast<CS*>(buf[z]);
+        s.X = static_cast<CS*>(buf[1 - z]);
+        s.Zi = static_cast<CS*>(buf[z]);
+        s.stride = e->stride;
         s.w_fw = static_cast<const CxW<ArS>*>(e->w_fw.p);
         s.w_iv = static_cast<const CxW<ArS>*>(e->w_iv.p);
         s.H = static_cast<const WS*>(e->H.p);
-        s.h = e->hf; s.hi = e->hi; s.Nb = e->Nb; s.Mb = e->Mb; s.up = d.up;
-        k_split<ArS><<<dim3(grid_for(e->hf / 2 + 1 + (ArS::kDD ? 0 : e->hf / 2), 256), nt), 256, 0, st>>>(s);
+        s.h = e->hf; s.hi = e->hi; s.Nb = e->Nb; s.Mb = e->Mb; s.up = d.up; s.Jg = d.Jg;
+        k_split<ArS><<<dim3(grid_for(e->hf / 2 + 1 + (ArS::kDD ? 0 : e->hf / 2), 256), sl.nt), 256, 0, st>>>(s);
         if ((rc = tr.mark(st, kSplit)) != KBSRC_GPU_OK) return rc;
-        k_merge<ArS><<<dim3(grid_for(e->hi / 2 + 1 + (ArS::kDD ? 0 : e->hi / 2), 256), nt), 256, 0, st>>>(s);
+        k_merge<ArS><<<dim3(grid_for(e->hi / 2 + 1 + (ArS::kDD ? 0 : e->hi / 2), 256), sl.nt), 256, 0, st>>>(s);
         if ((rc = tr.mark(st, kMerge)) != KBSRC_GPU_OK) return rc;
-        launches += 2;
-        // inverse complex FFT of B and the output epilogue
-        if (e->iv.host.four) {
-            const HostCfft& c = e->iv.host;
-            PassParams<ArL> p{};
-            p.sp = c.s1; p.N1 = c.N1; p.N2 = c.N2; p.F = e->col_iv.F;
-            p.tw_stage = static_cast<const CxW<ArL>*>(e->iv.tw_stage.p);
-            p.tw4 = static_cast<const CxW<ArL>*>(e->iv.tw4.p);
-            p.odd = odd_of<WL>(e);
-            p.src = BL; p.dst = BL; p.stride = e->stride; p.task0 = t0; p.out = o;
-            k_column<ArL, kSrcComplex><<<dim3((c.N2 + p.F - 1) / p.F, nt), e->col_iv.T, e->col_iv.smem, st>>>(p);
-            if ((rc = tr.mark(st, kInvA)) != KBSRC_GPU_OK) return rc;
-            p.sp = c.s2; p.F = e->row_iv.F;
-            k_row<ArL, kDstOutput><<<dim3((c.N1 + p.F - 1) / p.F, nt), e->row_iv.T, e->row_iv.smem, st>>>(p);
-            if ((rc = tr.mark(st, kInvB)) != KBSRC_GPU_OK) return rc;
-            launches += 2;
-        } else {
-            PassParams<ArS> p{};
-            p.sp = e->iv.host.sd; p.F = 1;
-            p.tw_stage = static_cast<const CxW<ArS>*>(e->iv.tw_stage.p);
-            p.odd = odd_of<WS>(e);
-            p.src = BS; p.dst = BS; p.stride = e->stride; p.task0 = t0; p.out = o;
-            k_direct<ArS, kSrcComplex, kDstOutput><<<dim3(1, nt), e->dir_iv.T, e->dir_iv.smem, st>>>(p);
-            if ((rc = tr.mark(st, kInvA)) != KBSRC_GPU_OK) return rc;
-            launches += 1;
-        }
+        // inverse complex FFT of buf[z] and the output epilogue
+        rc = launch_cfft<ArL, ArS, kSrcComplex, kDstOutput>(e->iv, sl, buf[z], buf[1 - z], buf[z], nullptr, st, tr,
+                                                             kInvA, kInvB);
+        if (rc) return rc;
     }
-    e->launches = launches;
+    e->launches = tr.launches;
     KB_CUDA(cudaGetLastError());
     return KBSRC_GPU_OK;
 }
 
-Shape direct_shape(const SubPlan& sp, size_t esize) {
-    int T = ((max_bfly(sp) + 31) / 32) * 32;
-    T = std::max(64, std::min(256, T));
-    return Shape{1, T, 2 * (size_t)sp.n * esize + (esize == 32 ? (size_t)sp.twn * esize : 0)};
+long long cfft_launches(const DevCfft& c) {
+    if (c.m) return 3 + 2 * cfft_launches(*c.inner);
+    return c.host.four ? 2 : 1;
+}
+
+size_t cfft_bytes(const DevCfft& c) {
+    size_t b = c.tw_stage.bytes + c.tw4.bytes + c.bc.bytes + c.vf.bytes;
+    return c.m ? b + cfft_bytes(*c.inner) : b;
 }
 
 int check_desc(const kbsrc_gpu_desc* d) {
@@ -815,12 +1022,11 @@ int check_desc(const kbsrc_gpu_desc* d) {
     if (d->precision != KBSRC_GPU_FAST && d->precision != KBSRC_GPU_EXACT) return fail(KBSRC_GPU_E_ARG, "precision");
     if (d->channels < 1 || d->P < 1 || d->Q < 1 || d->nb < 2 || d->nb % 2 || d->marg < 0 || d->nb <= 2 * d->marg)
         return fail(KBSRC_GPU_E_ARG, "bad plan shape");
-    if (d->frames < 0 || d->nout < 0 || d->nblk < 0 || d->edge_len < 0 || d->lead < 0)
+    if (d->frames < 0 || d->nout < 0 || d->nblk < 0 || d->edge_len < 0 || d->lead < 0 || d->Jg < 0)
         return fail(KBSRC_GPU_E_ARG, "bad plan sizes");
     if ((long long)d->nb * std::max(d->P, d->Q) > (1LL << 30)) return fail(KBSRC_GPU_E_ARG, "transform too large");
     const long long need = d->Jg ? (long long)d->Jg + 1 : (d->up ? d->nb * d->P / 2 + 1 : d->nb * d->Q / 2 + 1);
     if (!d->H || d->H_len < need) return fail(KBSRC_GPU_E_ARG, "kernel spectrum too short");
-    if (d->Jg) return fail(KBSRC_GPU_E_UNSUPPORTED, "general fold (near-unity ratio) is not on the GPU yet");
     return KBSRC_GPU_OK;
 }
 
@@ -857,31 +1063,17 @@ int create_impl(const kbsrc_gpu_desc* desc, kbsrc_gpu_engine** out) {
     e->hi = e->Mb / 2;
     e->hop = desc->nb - 2 * desc->marg;
     e->tasks = (long long)desc->channels * desc->nblk;
-    e->odd_dd = odd_roots<dd>();
-    e->odd_f64 = odd_roots<double>();
     KB_CUDA(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
-    if ((rc = make_dev_cfft(e->hf, e->exact, e->fw)) != KBSRC_GPU_OK) return rc;
-    if ((rc = make_dev_cfft(e->hi, e->exact, e->iv)) != KBSRC_GPU_OK) return rc;
+    const int fmax = env_int("KBSRC_GPU_FMAX", e->exact ? 8 : 16);
+    if ((rc = make_dev_cfft(e->hf, e->exact, fmax, e->fw, e->stream)) != KBSRC_GPU_OK) return rc;
+    if ((rc = make_dev_cfft(e->hi, e->exact, fmax, e->iv, e->stream)) != KBSRC_GPU_OK) return rc;
     if ((rc = upload_cx(split_roots(e->Nb), e->exact, e->w_fw)) != KBSRC_GPU_OK) return rc;
     if ((rc = upload_cx(split_roots(e->Mb), e->exact, e->w_iv)) != KBSRC_GPU_OK) return rc;
     if ((rc = upload_real(desc->H, desc->H_len, e->exact, e->H)) != KBSRC_GPU_OK) return rc;
     const size_t esize = e->exact ? 32 : 16;
-    const int fmax = env_int("KBSRC_GPU_FMAX", e->exact ? 8 : 16);
-    const HostCfft &f = e->fw.host, &v = e->iv.host;
-    if (f.four) {
-        e->col_fw = pick_shape(f.s1, f.N2, esize, fmax);
-        e->row_fw = pick_shape(f.s2, f.N1, esize, fmax);
-    } else {
-        e->dir_fw = direct_shape(f.sd, esize);
-    }
-    if (v.four) {
-        e->col_iv = pick_shape(v.s1, v.N2, esize, fmax);
-        e->row_iv = pick_shape(v.s2, v.N1, esize, fmax);
-    } else {
-        e->dir_iv = direct_shape(v.sd, esize);
-    }
-    // task slots: each holds max(h+1, h'+1) complex values, rounded to 8
-    e->stride = ((std::max(e->hf, e->hi) + 1 + 7) / 8) * 8;
+    // task slots: each holds the largest of h+1, h'+1 and the Bluestein lengths, rounded to 8
+    const long long need = std::max({(long long)e->hf + 1, (long long)e->hi + 1, e->fw.slot(), e->iv.slot()});
+    e->stride = (need + 7) / 8 * 8;
     const long long budget = (long long)env_int("KBSRC_GPU_WAVE_MB", 4096) << 20;
     const long long per_task = 2 * e->stride * (long long)esize;
     e->wave = std::max(1LL, std::min({e->tasks, budget / per_task, 65535LL}));
@@ -1034,13 +1226,13 @@ int kbsrc_gpu_engine_info(const kbsrc_gpu_engine* e, long long* tasks, long long
     if (!e) return fail(KBSRC_GPU_E_ARG, "null engine");
     if (tasks) *tasks = e->tasks;
     if (launches) {
-        long long per_wave = (e->fw.host.four ? 2 : 1) + 2 + (e->iv.host.four ? 2 : 1);
+        const long long per_wave = cfft_launches(e->fw) + 2 + cfft_launches(e->iv);
         *launches = e->tasks ? per_wave * ((e->tasks + e->wave - 1) / e->wave) : 0;
     }
     if (device_bytes) {
-        *device_bytes = (long long)(e->fw.tw_stage.bytes + e->fw.tw4.bytes + e->iv.tw_stage.bytes + e->iv.tw4.bytes +
-                                    e->w_fw.bytes + e->w_iv.bytes + e->H.bytes + e->bufA.bytes + e->bufB.bytes +
-                                    e->d_in.bytes + e->d_head.bytes + e->d_tail.bytes + e->d_out.bytes);
+        *device_bytes = (long long)(cfft_bytes(e->fw) + cfft_bytes(e->iv) + e->w_fw.bytes + e->w_iv.bytes +
+                                    e->H.bytes + e->bufA.bytes + e->bufB.bytes + e->d_in.bytes + e->d_head.bytes +
+                                    e->d_tail.bytes + e->d_out.bytes);
     }
     return KBSRC_GPU_OK;
 }
@@ -1053,8 +1245,13 @@ int kbsrc_gpu_kernel_spectrum(const double* taps, int L, int n, double scale, do
     try {
         int rc = require_device();
         if (rc) return rc;
-        rc = allow_large_smem();
-        if (rc) return rc;
+        if ((rc = allow_large_smem()) != KBSRC_GPU_OK) return rc;
+        cudaStream_t st = nullptr;
+        KB_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        struct StreamGuard {
+            cudaStream_t s;
+            ~StreamGuard() { cudaStreamDestroy(s); }
+        } sg{st};
         // the symmetric kernel placed circularly (design.cpp:42-43)
         std::vector<double> r((size_t)2 * n, 0.0);
         r[0] = taps[0];
@@ -1064,43 +1261,37 @@ int kbsrc_gpu_kernel_spectrum(const double* taps, int L, int n, double scale, do
             r[2 * (size_t)(n - m)] = taps[2 * m]; r[2 * (size_t)(n - m) + 1] = taps[2 * m + 1];
         }
         const int h = n / 2;
-        DevCfft c;
-        if ((rc = make_dev_cfft(h, true, c)) != KBSRC_GPU_OK) return rc;
+        DevCfft c;  // scalar double-double transform (RFFT<dd,dd,dd>), Bluestein when h is not 7-smooth
+        if ((rc = make_dev_cfft(h, true, 4, c, st)) != KBSRC_GPU_OK) return rc;
         DevBuf w, rin, A, B, Hd;
         if ((rc = upload_cx(split_roots(n), true, w)) != KBSRC_GPU_OK) return rc;
         if ((rc = rin.alloc(r.size() * 8)) != KBSRC_GPU_OK) return rc;
-        const size_t esize = 32;
-        if ((rc = A.alloc((size_t)(h + 1) * esize)) || (rc = B.alloc((size_t)(h + 1) * esize)) != KBSRC_GPU_OK) return rc;
+        const size_t slot = (size_t)std::max<long long>(h + 1, c.slot()) * 32;
+        if ((rc = A.alloc(slot)) != KBSRC_GPU_OK) return rc;
+        if ((rc = B.alloc(slot)) != KBSRC_GPU_OK) return rc;
         if ((rc = Hd.alloc((size_t)(h + 1) * 16)) != KBSRC_GPU_OK) return rc;
-        cudaStream_t st = nullptr;
-        KB_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-        struct StreamGuard {
-            cudaStream_t s;
-            ~StreamGuard() { cudaStreamDestroy(s); }
-        } sg{st};
         KB_CUDA(cudaMemcpyAsync(rin.p, r.data(), r.size() * 8, cudaMemcpyHostToDevice, st));
         using C = CxR<ArDDAccurate>;
-        const OddRoots<dd> odd = odd_roots<dd>();
-        PassParams<ArDDAccurate> p{};
-        p.tw_stage = static_cast<const CxW<ArDDAccurate>*>(c.tw_stage.p);
-        p.odd = odd;
-        p.ddreal = static_cast<const double*>(rin.p);
-        p.stride = 0;
-        if (c.host.four) {
-            const Shape sc = pick_shape(c.host.s1, c.host.N2, esize, 4), sr = pick_shape(c.host.s2, c.host.N1, esize, 4);
-            p.sp = c.host.s1; p.N1 = c.host.N1; p.N2 = c.host.N2; p.F = sc.F;
-            p.tw4 = static_cast<const CxW<ArDDAccurate>*>(c.tw4.p);
-            p.src = static_cast<C*>(A.p); p.dst = static_cast<C*>(A.p);
-            k_column<ArDDAccurate, kSrcDDReal><<<dim3((c.host.N2 + sc.F - 1) / sc.F, 1), sc.T, sc.smem, st>>>(p);
-            p.sp = c.host.s2; p.F = sr.F; p.src = static_cast<C*>(A.p); p.dst = static_cast<C*>(B.p);
-            k_row<ArDDAccurate, kDstComplex><<<dim3((c.host.N1 + sr.F - 1) / sr.F, 1), sr.T, sr.smem, st>>>(p);
+        Slots sl{};
+        sl.nt = 1;
+        sl.ddreal = static_cast<const double*>(rin.p);
+        Trail tr;
+        void *zbuf, *xbuf;
+        if (c.m) {
+            zbuf = A.p;
+            xbuf = B.p;
+            rc = launch_cfft<ArDDAccurate, ArDDAccurate, kSrcDDReal, kDstComplex>(c, sl, nullptr, A.p, B.p, A.p, st, tr,
+                                                                               -1, -1);
         } else {
-            const Shape sd = direct_shape(c.host.sd, esize);
-            p.sp = c.host.sd; p.F = 1; p.dst = static_cast<C*>(B.p);
-            k_direct<ArDDAccurate, kSrcDDReal, kDstComplex><<<dim3(1, 1), sd.T, sd.smem, st>>>(p);
+            zbuf = B.p;
+            xbuf = A.p;
+            rc = launch_cfft<ArDDAccurate, ArDDAccurate, kSrcDDReal, kDstComplex>(c, sl, A.p, nullptr, nullptr, B.p,
+                                                                               st, tr, -1, -1);
         }
+        if (rc) return rc;
         SpecParams<ArDDAccurate> s{};
-        s.Z = static_cast<C*>(B.p); s.X = static_cast<C*>(A.p);
+        s.Z = static_cast<C*>(zbuf);
+        s.X = static_cast<C*>(xbuf);
         s.w_fw = static_cast<const CxW<ArDDAccurate>*>(w.p);
         s.h = h; s.scale = scale; s.Hout = static_cast<dd*>(Hd.p);
         k_split<ArDDAccurate><<<grid_for(h / 2 + 1, 256), 256, 0, st>>>(s);

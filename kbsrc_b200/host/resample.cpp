@@ -282,7 +282,6 @@ std::unique_ptr<Conversion> prepare(const double* in, long long frames, int ch, 
     if (pl.copy) return cv;
     if (opt.precision == Precision::LongDouble)
         throw std::runtime_error("mode ld (x87 long double) is not available on the GPU engine");
-    if (pl.general) throw std::runtime_error("near-unity ratios (general fold) are not available on the GPU engine");
     const double t0 = now();
     const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
     const int threads = opt.threads ? opt.threads : std::min(hw, 8);
@@ -314,12 +313,30 @@ std::unique_ptr<Conversion> prepare(const double* in, long long frames, int ch, 
         });
     }
     // kernel: taps on the host, spectrum on the GPU (design.cpp:40-49)
-    const long long gc = std::gcd(pl.c2, pl.fk);
-    const std::vector<dd> taps = kaiser_taps((int)pl.Lk, pl.c2 / gc, pl.fk / gc, opt.beta, threads);
-    const int nspec = (int)(pl.up ? Mb : Nb);
+    std::vector<dd> taps;
+    int nspec, Jg = 0;
+    if (pl.general) {
+        // Near-unity ratios: the kernel sampled on a finer grid of Nk points (rate Nk*fi/Nb) so its spectrum is
+        // the true continuous response, folded modulo Mb by the engine (resampler.cpp:187-202).
+        long long Nk = std::max(Nb, Mb) * 5LL / 4;
+        Nk += Nk & 1;
+        while (!host::smooth7(Nk / 2)) Nk += 2;
+        const __int128 A = (__int128)pl.c2 * Nb, B = (__int128)Nk * pl.fi;
+        const long long g2 = (long long)std::gcd((unsigned long long)pl.c2 * (unsigned long long)Nb,
+                                                 (unsigned long long)Nk * (unsigned long long)pl.fi);
+        const double fk2 = (double)Nk * pl.fi / Nb;
+        taps = kaiser_taps((int)std::floor(opt.length * fk2), (long long)(A / g2), (long long)(B / g2), opt.beta,
+                           threads);
+        nspec = (int)Nk;
+        Jg = (int)std::min<long long>(Nk / 2, (long long)std::ceil((pl.mn / 2.0 + 4 * pl.fml) * Nb / pl.fi));
+    } else {
+        const long long gc = std::gcd(pl.c2, pl.fk);
+        taps = kaiser_taps((int)pl.Lk, pl.c2 / gc, pl.fk / gc, opt.beta, threads);
+        nspec = (int)(pl.up ? Mb : Nb);
+    }
     std::vector<double> H((size_t)(nspec / 2 + 1) * 2);
-    gpu_check(kbsrc_gpu_kernel_spectrum(reinterpret_cast<const double*>(taps.data()), (int)pl.Lk, nspec, (double)Nb,
-                                        H.data()),
+    gpu_check(kbsrc_gpu_kernel_spectrum(reinterpret_cast<const double*>(taps.data()), (int)taps.size() - 1, nspec,
+                                        (double)Nb, H.data()),
               "kernel spectrum");
     kbsrc_gpu_desc d{};
     d.precision = opt.precision == Precision::Fast ? KBSRC_GPU_FAST : KBSRC_GPU_EXACT;
@@ -334,7 +351,7 @@ std::unique_ptr<Conversion> prepare(const double* in, long long frames, int ch, 
     d.frames = frames;
     d.nout = pl.nout;
     d.up = pl.up;
-    d.Jg = 0;
+    d.Jg = Jg;
     d.edge_len = ext;
     d.H = H.data();
     d.H_len = (long long)H.size() / 2;
@@ -357,7 +374,7 @@ void fill_stats(const Conversion& cv, Stats* stats, double process_seconds) {
     stats->taps = 2 * pl.Lk + 1;
     stats->block = pl.nb;
     stats->threads = 1;
-    stats->general_fold = false;
+    stats->general_fold = pl.general;
     stats->design_seconds = cv.design_seconds;
     stats->process_seconds = process_seconds;
     stats->passband = (double)pl.c2 / 2 - pl.fml;

@@ -54,6 +54,15 @@ CASES = {
     "s_48k_44k1_exact_10frames": (("frames", 26, 10, 1), 48000, 44100, {"mode": "exact"}),
     "s_48k_44k1_exact_empty": (("frames", 27, 0, 1), 48000, 44100, {"mode": "exact"}),
     "s_22k05_48k_fast_len002": (("frames", 28, 3000, 1), 22050, 48000, {"mode": "fast", "length": 0.02}),
+    # near-unity ratios (general fold) and transform lengths that are not 7-smooth (Bluestein)
+    "s_44k1_44k101_exact": (("frames", 29, 3000, 1), 44100, 44101, {"mode": "exact"}),
+    "s_44k101_44k1_fast": (("frames", 30, 3000, 2), 44101, 44100, {"mode": "fast"}),
+    "s_1001_1000_exact": (("frames", 31, 2500, 1), 1001, 1000, {"mode": "exact"}),
+    "s_1000_1001_fast": (("frames", 32, 2500, 1), 1000, 1001, {"mode": "fast"}),
+    "s_48k_48k001_exact": (("frames", 33, 3000, 1), 48000, 48001, {"mode": "exact"}),
+    "s_96k_32k001_exact": (("frames", 34, 4000, 1), 96000, 32001, {"mode": "exact"}),
+    "s_96k_32k001_fast": (("frames", 35, 4000, 2), 96000, 32001, {"mode": "fast"}),
+    "s_22k05_48k001_exact": (("frames", 36, 3000, 1), 22050, 48001, {"mode": "exact"}),
 }
 
 
