@@ -142,3 +142,22 @@ def test_cli_equal_rates_copy_without_gpu(tmp_path, src):
     data = out.read_bytes()
     x = np.frombuffer(src.read_bytes()[-1024:], "<f8")
     assert np.frombuffer(data[-1024:], "<f8").tobytes() == x.tobytes()
+
+
+@pytest.mark.skipif(not os.path.exists(oracle.REF_CLI), reason="reference CLI not built (oracle/_ref)")
+@pytest.mark.parametrize("fmt", ["s16", "s24", "s32", "f32", "f64"])
+@pytest.mark.parametrize("dither", [False, True])
+def test_wav_writer_bytes_equal_reference_cli(tmp_path, fmt, dither):
+    """Equal rates take the host copy path, so the writer (scaling, TPDF dither from mt19937_64(12345), rounding,
+    clipping, header) is compared with the reference CLI without a GPU."""
+    x = np.random.default_rng(3).uniform(-1.2, 1.2, (5000, 3))
+    src = tmp_path / "in.wav"
+    src.write_bytes(wav(3, 3, 48000, 64, 24, x.astype("<f8").tobytes()))
+    extra = ["--dither"] if dither else []
+    a, b = tmp_path / "a.wav", tmp_path / "b.wav"
+    ra = cli(src, a, "--rate", 48000, "--format", fmt, *extra)
+    rb = subprocess.run([oracle.REF_CLI, str(src), str(b), "--rate", "48000", "--format", fmt, *extra],
+                        capture_output=True, text=True)
+    assert ra.returncode == rb.returncode == 0, (ra.stderr, rb.stderr)
+    assert ra.stderr == rb.stderr  # the clipped-samples warning
+    assert a.read_bytes() == b.read_bytes()
