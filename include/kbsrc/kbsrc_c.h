@@ -51,6 +51,25 @@ int kbsrc_conversion_info_c(const kbsrc_conversion* cv, long long* nout, long lo
                             const double** tail, struct kbsrc_gpu_engine** engine, kbsrc_stats_c* stats);
 void kbsrc_conversion_free_c(kbsrc_conversion* cv);
 
+/* Batches: many conversions (files) of any lengths, channel counts and rate pairs, planned together and run
+ * on the GPU as one recorded launch sequence (kbsrc_gpu_batch in include/kbsrc_gpu.h); conversions with equal
+ * plans share their kernel design and launches. Each output equals that of kbsrc_resample_c for the item. */
+typedef struct {
+    const double* in; /* interleaved frames x channels (used for the LPC edges at prepare) */
+    long long frames;
+    int channels, rate_in, rate_out;
+} kbsrc_batch_item_c;
+typedef struct kbsrc_batch kbsrc_batch;
+int kbsrc_batch_prepare_c(const kbsrc_batch_item_c* items, int count, const kbsrc_options_c* opt,
+                          kbsrc_batch** out, char* err, int err_len);
+/* in[i]: interleaved input of item i; out[i]: planar output, channels * nout doubles. */
+int kbsrc_batch_run_c(kbsrc_batch* b, const double* const* in, double* const* out, char* err, int err_len);
+/* Item i: output frames, LPC edges (channels * edge_len each) and its index in the GPU batch (-1: equal rates). */
+int kbsrc_batch_info_c(const kbsrc_batch* b, int i, long long* nout, long long* edge_len, const double** head,
+                       const double** tail, int* gpu_index);
+struct kbsrc_gpu_batch* kbsrc_batch_gpu_c(kbsrc_batch* b);
+void kbsrc_batch_free_c(kbsrc_batch* b);
+
 /* Diagnostics: the host-side steps on their own (no GPU needed).
  * kbsrc_plan_c: the block plan of src/resampler.cpp:98-167, info[16] = P Q taps nb marg hop nblk Nb Mb pre o E
  *   lead general up nout; returns 0, 1 (equal rates: copy) or -1 (invalid argument).

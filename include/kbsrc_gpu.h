@@ -84,6 +84,23 @@ int kbsrc_gpu_engine_info(const kbsrc_gpu_engine* e, long long* tasks, long long
 
 void kbsrc_gpu_engine_destroy(kbsrc_gpu_engine* e);
 
+/* Batches: many conversions at once (the uneven multi-file queue). Conversions whose plans are equal (precision,
+ * P/Q, block, margin, fold, kernel spectrum) form one group and share FFT tables and launches; groups run one after
+ * another. The first run records the whole launch sequence in a CUDA graph and later runs replay it: every buffer
+ * pointer is read from a small per-run table, so new buffers need no new recording. Replaces running run_engine
+ * once per file (src/resampler.cpp:34-88). descs[i] as for kbsrc_gpu_engine_create (H copied at create). */
+typedef struct kbsrc_gpu_batch kbsrc_gpu_batch;
+int kbsrc_gpu_batch_create(const kbsrc_gpu_desc* descs, int count, kbsrc_gpu_batch** out);
+/* Device buffers per conversion (arrays of count pointers; head/tail may be NULL when no conversion has edges).
+ * Asynchronous on `stream` (NULL: the batch's own stream); a run waits for the previous one to have started. */
+int kbsrc_gpu_batch_run_device(kbsrc_gpu_batch* b, const double* const* d_in, const double* const* d_head,
+                               const double* const* d_tail, double* const* d_out, void* stream);
+/* Host buffers per conversion, synchronous (device buffers allocated on the first call). */
+int kbsrc_gpu_batch_run_host(kbsrc_gpu_batch* b, const double* const* in, const double* const* head,
+                             const double* const* tail, double* const* out);
+int kbsrc_gpu_batch_info(const kbsrc_gpu_batch* b, long long* groups, long long* tasks, long long* launches);
+void kbsrc_gpu_batch_destroy(kbsrc_gpu_batch* b);
+
 /* Real spectrum of the symmetric kernel h[0..L] placed circularly in n points, divided by scale, computed on
  * the GPU with the reference's scalar double-double real FFT (src/design.cpp:40-49, RFFT<dd,dd,dd>).
  * taps: (L+1) (hi, lo) pairs; H: (n/2+1) (hi, lo) pairs out. n must be even. */

@@ -43,6 +43,12 @@ class Stats(ctypes.Structure):
         return d
 
 
+class BatchItem(ctypes.Structure):
+    """kbsrc_batch_item_c (include/kbsrc/kbsrc_c.h)."""
+    _fields_ = [("in_", _dp), ("frames", ctypes.c_longlong), ("channels", ctypes.c_int), ("rate_in", ctypes.c_int),
+                ("rate_out", ctypes.c_int)]
+
+
 class GpuDesc(ctypes.Structure):
     """kbsrc_gpu_desc (include/kbsrc_gpu.h)."""
     _fields_ = [("precision", ctypes.c_int), ("channels", ctypes.c_int), ("P", ctypes.c_longlong),
@@ -66,6 +72,13 @@ GPU_SYMBOLS = {
     "kbsrc_gpu_kernel_spectrum": (ctypes.c_int, [_dp, ctypes.c_int, ctypes.c_int, ctypes.c_double, _dp]),
     "kbsrc_gpu_kernel_spectrum_static": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                                         ctypes.c_void_p, ctypes.c_void_p]),
+    "kbsrc_gpu_batch_create": (ctypes.c_int, [_P(GpuDesc), ctypes.c_int, _P(ctypes.c_void_p)]),
+    "kbsrc_gpu_batch_run_device": (ctypes.c_int, [ctypes.c_void_p, _P(ctypes.c_void_p), _P(ctypes.c_void_p),
+                                                  _P(ctypes.c_void_p), _P(ctypes.c_void_p), ctypes.c_void_p]),
+    "kbsrc_gpu_batch_run_host": (ctypes.c_int, [ctypes.c_void_p, _P(ctypes.c_void_p), _P(ctypes.c_void_p),
+                                                _P(ctypes.c_void_p), _P(ctypes.c_void_p)]),
+    "kbsrc_gpu_batch_info": (ctypes.c_int, [ctypes.c_void_p, _lp, _lp, _lp]),
+    "kbsrc_gpu_batch_destroy": (None, [ctypes.c_void_p]),
     "kbsrc_gpu_last_error": (ctypes.c_char_p, []),
     "kbsrc_gpu_engine_name": (ctypes.c_char_p, []),
 }
@@ -81,6 +94,14 @@ HOST_SYMBOLS = {
     "kbsrc_conversion_info_c": (ctypes.c_int, [ctypes.c_void_p, _lp, _lp, _P(_dp), _P(_dp),
                                                _P(ctypes.c_void_p), _P(Stats)]),
     "kbsrc_conversion_free_c": (None, [ctypes.c_void_p]),
+    "kbsrc_batch_prepare_c": (ctypes.c_int, [_P(BatchItem), ctypes.c_int, _P(Options), _P(ctypes.c_void_p),
+                                             ctypes.c_char_p, ctypes.c_int]),
+    "kbsrc_batch_run_c": (ctypes.c_int, [ctypes.c_void_p, _P(ctypes.c_void_p), _P(ctypes.c_void_p), ctypes.c_char_p,
+                                         ctypes.c_int]),
+    "kbsrc_batch_info_c": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _lp, _lp, _P(_dp), _P(_dp),
+                                          _P(ctypes.c_int)]),
+    "kbsrc_batch_gpu_c": (ctypes.c_void_p, [ctypes.c_void_p]),
+    "kbsrc_batch_free_c": (None, [ctypes.c_void_p]),
     "kbsrc_plan_c": (ctypes.c_int, [ctypes.c_longlong, ctypes.c_int, ctypes.c_int, ctypes.c_int, _P(Options), _lp,
                                     ctypes.c_char_p, ctypes.c_int]),
     "kbsrc_kernel_taps_c": (ctypes.c_int, [ctypes.c_int, ctypes.c_longlong, ctypes.c_longlong, ctypes.c_double,
@@ -239,6 +260,75 @@ class Conversion:
     def close(self):
         if self._h:
             host_lib().kbsrc_conversion_free_c(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Many conversions at once (kbsrc_batch_prepare_c): items are (x, rate_in, rate_out) with x (frames, channels)
+    float64. Conversions with equal plans share kernel design and GPU launches; the GPU run is one recorded launch
+    sequence (CUDA graph) replayed on every run."""
+
+    def __init__(self, items, mode="exact", length=0.2, beta=40.0, block=0, lpc=True, threads=0):
+        self.xs = [np.ascontiguousarray(x if np.ndim(x) == 2 else np.asarray(x)[:, None], dtype=np.float64)
+                   for x, _, _ in items]
+        arr = (BatchItem * len(items))()
+        for i, ((_, fi, fo), x) in enumerate(zip(items, self.xs)):
+            arr[i] = BatchItem(_ptr(x), x.shape[0], x.shape[1], fi, fo)
+        self._h = ctypes.c_void_p()
+        err = ctypes.create_string_buffer(512)
+        opt = _options(mode, length, beta, block, lpc, threads)
+        r = host_lib().kbsrc_batch_prepare_c(arr, len(items), ctypes.byref(opt), ctypes.byref(self._h), err, 512)
+        if r == -1:
+            raise ValueError(err.value.decode())
+        if r < 0:
+            raise RuntimeError(err.value.decode())
+        self.nout, self.edge_len, self.gpu_index, self.head, self.tail = [], [], [], [], []
+        for i, x in enumerate(self.xs):
+            n, e, gi = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_int()
+            hp, tp = _dp(), _dp()
+            host_lib().kbsrc_batch_info_c(self._h, i, ctypes.byref(n), ctypes.byref(e), ctypes.byref(hp),
+                                          ctypes.byref(tp), ctypes.byref(gi))
+            self.nout.append(n.value)
+            self.edge_len.append(e.value)
+            self.gpu_index.append(gi.value)
+            m = e.value * x.shape[1]
+            self.head.append(np.ctypeslib.as_array(hp, (m,)).copy() if m else np.zeros(1))
+            self.tail.append(np.ctypeslib.as_array(tp, (m,)).copy() if m else np.zeros(1))
+        self.gpu = host_lib().kbsrc_batch_gpu_c(self._h)
+
+    def run(self, xs=None):
+        """Host buffers in and out; returns a list of planar (channels, nout) arrays."""
+        xs = self.xs if xs is None else [np.ascontiguousarray(x, dtype=np.float64) for x in xs]
+        outs = [np.zeros((x.shape[1], max(n, 1))) for x, n in zip(xs, self.nout)]
+        pin = (ctypes.c_void_p * len(xs))(*[x.ctypes.data for x in xs])
+        pout = (ctypes.c_void_p * len(xs))(*[o.ctypes.data for o in outs])
+        err = ctypes.create_string_buffer(512)
+        if host_lib().kbsrc_batch_run_c(self._h, pin, pout, err, 512):
+            raise RuntimeError(err.value.decode())
+        return [o[:, :n] for o, n in zip(outs, self.nout)]
+
+    def gpu_info(self):
+        g, t, l = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_longlong()
+        gpu_lib().kbsrc_gpu_batch_info(self.gpu, ctypes.byref(g), ctypes.byref(t), ctypes.byref(l))
+        return {"groups": g.value, "tasks": t.value, "launches": l.value}
+
+    def run_device(self, d_in, d_head, d_tail, d_out, stream=0):
+        """GPU items only (gpu_index order): lists of device pointers; asynchronous on `stream`."""
+        n = len(d_in)
+        arrs = [(ctypes.c_void_p * n)(*v) for v in (d_in, d_head, d_tail, d_out)]
+        rc = gpu_lib().kbsrc_gpu_batch_run_device(self.gpu, *arrs, stream or None)
+        if rc:
+            raise RuntimeError(f"kbsrc_gpu_batch_run_device: {rc} {gpu_error()}")
+
+    def close(self):
+        if self._h:
+            host_lib().kbsrc_batch_free_c(self._h)
             self._h = ctypes.c_void_p()
 
     def __del__(self):

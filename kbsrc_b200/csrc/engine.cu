@@ -52,18 +52,41 @@ int fail(int code, const std::string& msg) {
 // kernel parameter blocks
 // ------------------------------------------------------------------------------------------------------
 
-// The staged channel of the reference (resampler.cpp:168-186) without materialising it: zeros, the LPC head,
-// the interleaved input, the LPC tail, zeros.
-struct Signal {
-    const double* in;
-    const double* head;
-    const double* tail;
-    long long frames, edge, lead, hopQ, nblk;
+// One conversion's buffers and placement; a single engine runs one, a batch many.
+// The staged channel of the reference (resampler.cpp:168-186) is read without being materialised: zeros, the
+// LPC head, the interleaved input, the LPC tail, zeros; frame t of the signal is staged sample t + lead.
+struct Item {
+    const double* in;    // interleaved input, frames x ch
+    const double* head;  // ch x edge: head[c*edge + i] is frame -1-i
+    const double* tail;  // ch x edge: tail[c*edge + i] is frame frames+i
+    double* out;         // planar output, ch x nout
+    long long frames, edge, lead, nout, o;
     int ch;
 };
 
-__device__ __forceinline__ double signal_at(const Signal& s, int c, long long g) {
-    const long long t = g - s.lead;
+// Which conversion, channel and block a task is.
+struct TaskRef {
+    int item, c;
+    long long b;
+};
+
+// The tasks of one launch group: a single conversion (refs == nullptr; task = b * ch + c, so the channels of
+// one block run side by side and share the sectors of the interleaved input) or a batch (device tables). The
+// order of tasks does not affect any value.
+struct Work {
+    Item item0;
+    const Item* items;
+    const TaskRef* refs;
+    long long hopQ, hopP, margP;  // block hop in staged samples and output samples, output margin
+};
+
+__device__ __forceinline__ TaskRef task_ref(const Work& w, long long task) {
+    if (w.refs) return w.refs[task];
+    return TaskRef{0, (int)(task % w.item0.ch), task / w.item0.ch};
+}
+__device__ __forceinline__ Item item_of(const Work& w, const TaskRef& r) { return w.refs ? w.items[r.item] : w.item0; }
+
+__device__ __forceinline__ double signal_at(const Item& s, int c, long long t) {
     if (t >= 0 && t < s.frames) return __ldg(s.in + t * s.ch + c);
     if (t < 0 && t >= -s.edge) return __ldg(s.head + c * s.edge + (-1 - t));
     if (t >= s.frames && t < s.frames + s.edge) return __ldg(s.tail + c * s.edge + (t - s.frames));
@@ -71,22 +94,11 @@ __device__ __forceinline__ double signal_at(const Signal& s, int c, long long g)
 }
 
 // Discard and copy (resampler.cpp:80-84): sample e of block b's inverse FFT lands at b*hopP + e - margP - o
-struct Output {
-    double* out;
-    long long nout, o, hopP, margP, nblk;
-    int ch;
-};
-
-// Tasks are numbered block-major, task = b * channels + c, so the channels of one block run side by side and
-// share the sectors of the interleaved input. The order of tasks does not affect any value.
-__device__ __forceinline__ int task_channel(long long task, int ch) { return (int)(task % ch); }
-__device__ __forceinline__ long long task_block(long long task, int ch) { return task / ch; }
-
-__device__ __forceinline__ void emit(const Output& o, int c, long long b, long long e, double v) {
-    const long long k = e - o.margP;
-    if (k < 0 || k >= o.hopP) return;
-    const long long d = b * o.hopP + k - o.o;
-    if (d >= 0 && d < o.nout) o.out[c * o.nout + d] = v;
+__device__ __forceinline__ void emit(const Work& w, const Item& it, int c, long long b, long long e, double v) {
+    const long long k = e - w.margP;
+    if (k < 0 || k >= w.hopP) return;
+    const long long d = b * w.hopP + k - it.o;
+    if (d >= 0 && d < it.nout) it.out[c * it.nout + d] = v;
 }
 
 enum Src { kSrcSignal = 0, kSrcComplex = 1, kSrcDDReal = 2 };
@@ -103,26 +115,29 @@ struct PassParams {
     CxR<Ar>* dst;
     long long stride;             // complex elements between task slots
     long long task0;              // first task of this launch (blockIdx.y adds)
-    Signal sig;                   // kSrcSignal
+    Work work;                    // kSrcSignal / kDstOutput: the conversions and their buffers
     const double* ddreal;         // kSrcDDReal: (hi, lo) pairs
-    Output out;                   // kDstOutput
     const CxW<Ar>* bc;            // Bluestein chirp (bn entries) and kernel spectrum (bm entries)
     const CxW<Ar>* vf;
     int bn, bm;
 };
 
-// Where a task's first pass reads: the staged signal of one channel, a complex buffer, or dd reals.
+// Where a task's first pass reads the staged signal: its conversion, channel and the signal frame of real
+// sample 0 of the block; interior when no sample of the block needs the edge or padding tests.
 struct TaskSource {
+    Item it;
     int c;
-    long long g0;   // staged index of the block's first sample minus lead: signal frame of real sample 0
-    bool interior;  // every sample of the block lies inside the input (no edge or padding tests needed)
+    long long g0;
+    bool interior;
 };
 
-__device__ __forceinline__ TaskSource task_source(const Signal& s, long long task, long long nreal) {
+__device__ __forceinline__ TaskSource task_source(const Work& w, long long task, long long nreal) {
+    const TaskRef r = task_ref(w, task);
     TaskSource t;
-    t.c = task_channel(task, s.ch);
-    t.g0 = task_block(task, s.ch) * s.hopQ - s.lead;
-    t.interior = t.g0 >= 0 && t.g0 + nreal <= s.frames;
+    t.it = item_of(w, r);
+    t.c = r.c;
+    t.g0 = r.b * w.hopQ - t.it.lead;
+    t.interior = t.g0 >= 0 && t.g0 + nreal <= t.it.frames;
     return t;
 }
 
@@ -136,11 +151,11 @@ __device__ __forceinline__ CxR<Ar> load_input(const PassParams<Ar>& P, const Tas
         const long long t = ts.g0 + 2 * i;
         double x0, x1;
         if (ts.interior) {
-            x0 = __ldg(P.sig.in + t * P.sig.ch + ts.c);
-            x1 = __ldg(P.sig.in + (t + 1) * P.sig.ch + ts.c);
+            x0 = __ldg(ts.it.in + t * ts.it.ch + ts.c);
+            x1 = __ldg(ts.it.in + (t + 1) * ts.it.ch + ts.c);
         } else {
-            x0 = signal_at(P.sig, ts.c, t + P.sig.lead);
-            x1 = signal_at(P.sig, ts.c, t + 1 + P.sig.lead);
+            x0 = signal_at(ts.it, ts.c, t);
+            x1 = signal_at(ts.it, ts.c, t + 1);
         }
         return CxR<Ar>{Ar::from_f64(x0), Ar::from_f64(x1)};
     } else if constexpr (SRC == kSrcComplex) {
@@ -181,7 +196,7 @@ __global__ void __launch_bounds__(256, Ar::kMinBlocks) k_column(const __grid_con
     const int c0 = blockIdx.x * F;
     const C* src = P.src + blockIdx.y * P.stride;
     C* dst = P.dst + blockIdx.y * P.stride;
-    const TaskSource ts = SRC == kSrcSignal ? task_source(P.sig, task, 2LL * N1 * N2) : TaskSource{0, 0, false};
+    const TaskSource ts = SRC == kSrcSignal ? task_source(P.work, task, 2LL * N1 * N2) : TaskSource{};
     const CxW<Ar>* tws = stage_twiddles<Ar>(P.sp, P.tw_stage, twiddle_smem<Ar>(rest));
     for (int e0 = threadIdx.x; e0 < total; e0 += kLoadBatch * blockDim.x) {
         C v[kLoadBatch];
@@ -245,8 +260,8 @@ __global__ void __launch_bounds__(256, Ar::kMinBlocks) k_row(const __grid_consta
     __syncthreads();
     const Planes<Ar> res = stockham<Ar>(P.sp, A, B, F, tws, P.odd);
     C* dst = P.dst + blockIdx.y * P.stride;
-    const int c = DST == kDstOutput ? task_channel(task, P.out.ch) : 0;
-    const long long b = DST == kDstOutput ? task_block(task, P.out.ch) : 0;
+    const TaskRef tr = DST == kDstOutput ? task_ref(P.work, task) : TaskRef{0, 0, 0};
+    const Item it = DST == kDstOutput ? item_of(P.work, tr) : Item{};
     for (int e = threadIdx.x; e < total; e += blockDim.x) {
         const int k2 = e / F, f = e - k2 * F, row = r0 + f;
         if (row >= N1) continue;
@@ -256,8 +271,8 @@ __global__ void __launch_bounds__(256, Ar::kMinBlocks) k_row(const __grid_consta
         if (DST == kDstComplex) {
             dst[iz] = v;
         } else {
-            emit(P.out, c, b, 2 * iz, Ar::to_f64(v.re));
-            emit(P.out, c, b, 2 * iz + 1, Ar::to_f64(Ar::neg(v.im)));
+            emit(P.work, it, tr.c, tr.b, 2 * iz, Ar::to_f64(v.re));
+            emit(P.work, it, tr.c, tr.b, 2 * iz + 1, Ar::to_f64(Ar::neg(v.im)));
         }
     }
 }
@@ -272,21 +287,21 @@ __global__ void __launch_bounds__(256, Ar::kMinBlocks) k_direct(const __grid_con
     unsigned char* rest = carve<Ar>(smem, n, A, B);
     const long long task = P.task0 + blockIdx.y;
     const C* src = P.src + blockIdx.y * P.stride;
-    const TaskSource ts = SRC == kSrcSignal ? task_source(P.sig, task, 2LL * n) : TaskSource{0, 0, false};
+    const TaskSource ts = SRC == kSrcSignal ? task_source(P.work, task, 2LL * n) : TaskSource{};
     const CxW<Ar>* tws = stage_twiddles<Ar>(P.sp, P.tw_stage, twiddle_smem<Ar>(rest));
     for (int i = threadIdx.x; i < n; i += blockDim.x) A.st(i, load_input<Ar, SRC>(P, ts, src, i));
     __syncthreads();
     const Planes<Ar> res = stockham<Ar>(P.sp, A, B, 1, tws, P.odd);
     C* dst = P.dst + blockIdx.y * P.stride;
-    const int c = DST == kDstOutput ? task_channel(task, P.out.ch) : 0;
-    const long long b = DST == kDstOutput ? task_block(task, P.out.ch) : 0;
+    const TaskRef tr = DST == kDstOutput ? task_ref(P.work, task) : TaskRef{0, 0, 0};
+    const Item it = DST == kDstOutput ? item_of(P.work, tr) : Item{};
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
         const C v = res.ld(i);
         if (DST == kDstComplex) {
             dst[i] = v;
         } else {
-            emit(P.out, c, b, 2LL * i, Ar::to_f64(v.re));
-            emit(P.out, c, b, 2LL * i + 1, Ar::to_f64(Ar::neg(v.im)));
+            emit(P.work, it, tr.c, tr.b, 2LL * i, Ar::to_f64(v.re));
+            emit(P.work, it, tr.c, tr.b, 2LL * i + 1, Ar::to_f64(Ar::neg(v.im)));
         }
     }
 }
@@ -300,7 +315,7 @@ __global__ void k_blue_pre(const __grid_constant__ PassParams<Ar> P) {
     const long long task = P.task0 + blockIdx.y;
     const C* src = P.src + blockIdx.y * P.stride;
     C* dst = P.dst + blockIdx.y * P.stride;
-    const TaskSource ts = SRC == kSrcSignal ? task_source(P.sig, task, 2LL * P.bn) : TaskSource{0, 0, false};
+    const TaskSource ts = SRC == kSrcSignal ? task_source(P.work, task, 2LL * P.bn) : TaskSource{};
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < P.bm; j += gridDim.x * blockDim.x) {
         if (j < P.bn) {
             const CxW<Ar> b = ld_tw(P.bc + j);
@@ -325,16 +340,16 @@ __global__ void k_blue_post(const __grid_constant__ PassParams<Ar> P) {
     const long long task = P.task0 + blockIdx.y;
     const C* src = P.src + blockIdx.y * P.stride;
     C* dst = P.dst + blockIdx.y * P.stride;
-    const int c = DST == kDstOutput ? task_channel(task, P.out.ch) : 0;
-    const long long b = DST == kDstOutput ? task_block(task, P.out.ch) : 0;
+    const TaskRef tr = DST == kDstOutput ? task_ref(P.work, task) : TaskRef{0, 0, 0};
+    const Item it = DST == kDstOutput ? item_of(P.work, tr) : Item{};
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < P.bn; k += gridDim.x * blockDim.x) {
         const CxW<Ar> w = ld_tw(P.bc + k);
         const C y = c_mulw<Ar>(c_conj<Ar>(src[k]), CxW<Ar>{w.re, w_neg(w.im)});
         if (DST == kDstComplex) {
             dst[k] = y;
         } else {
-            emit(P.out, c, b, 2LL * k, Ar::to_f64(y.re));
-            emit(P.out, c, b, 2LL * k + 1, Ar::to_f64(Ar::neg(y.im)));
+            emit(P.work, it, tr.c, tr.b, 2LL * k, Ar::to_f64(y.re));
+            emit(P.work, it, tr.c, tr.b, 2LL * k + 1, Ar::to_f64(Ar::neg(y.im)));
         }
     }
 }
@@ -731,15 +746,54 @@ int env_int(const char* name, int dflt) {
 // ------------------------------------------------------------------------------------------------------
 // the engine
 // ------------------------------------------------------------------------------------------------------
-struct kbsrc_gpu_engine {
-    kbsrc_gpu_desc d{};
+// The transform plan of one conversion shape: its FFTs, split/merge roots and kernel spectrum. Conversions that
+// share it (a batch group) run in the same launches.
+struct PlanCore {
+    kbsrc_gpu_desc d{};  // the shape (H is not kept)
     bool exact = false;
-    int device = 0;
     int Nb = 0, Mb = 0, hf = 0, hi = 0, hop = 0;
-    long long tasks = 0, wave = 0, stride = 0, launches = 0;
-    cudaStream_t stream = nullptr;
     DevCfft fw, iv;
     DevBuf w_fw, w_iv, H;
+    // complex values one task slot must hold: h+1, h'+1 and the Bluestein lengths
+    long long slot() const {
+        const long long n = std::max({(long long)hf + 1, (long long)hi + 1, fw.slot(), iv.slot()});
+        return (n + 7) / 8 * 8;
+    }
+    size_t esize() const { return exact ? 32 : 16; }
+};
+
+// A batch group: conversions with one plan, their tasks listed block-major per conversion.
+struct BatchGroup : PlanCore {
+    std::vector<int> members;
+    long long tasks = 0, stride = 0, wave = 0;
+    DevBuf refs;  // TaskRef[tasks]
+};
+
+struct kbsrc_gpu_batch {
+    std::vector<kbsrc_gpu_desc> descs;  // per conversion (H not kept)
+    std::vector<std::unique_ptr<BatchGroup>> groups;
+    std::vector<int> group_of;          // conversion -> group, -1 when it has no tasks
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    DevBuf items;                       // Item[count], rewritten from items_host by every run
+    Item* items_host = nullptr;         // pinned
+    DevBuf bufA, bufB;
+    cudaGraphExec_t graph = nullptr;    // the whole run, recorded on first use
+    cudaEvent_t done = nullptr;         // end of the last run (guards items_host)
+    long long launches = 0;
+    std::vector<DevBuf> d_in, d_head, d_tail, d_out;  // run_host buffers, allocated on first use
+    ~kbsrc_gpu_batch() {
+        if (graph) cudaGraphExecDestroy(graph);
+        if (done) cudaEventDestroy(done);
+        if (items_host) cudaFreeHost(items_host);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+struct kbsrc_gpu_engine : PlanCore {
+    int device = 0;
+    long long tasks = 0, wave = 0, stride = 0, launches = 0;
+    cudaStream_t stream = nullptr;
     DevBuf bufA, bufB;
     DevBuf d_in, d_head, d_tail, d_out;
     std::vector<cudaEvent_t> events;  // per-pass timing trail, created on first use
@@ -837,9 +891,8 @@ struct Trail {
 struct Slots {
     long long stride, task0;
     unsigned nt;
-    Signal sig;
+    Work work;
     const double* ddreal;
-    Output out;
 };
 
 template <class Ar>
@@ -852,9 +905,8 @@ PassParams<Ar> pass_params(const Slots& sl, const DevCfft& c, void* src, void* d
     p.dst = static_cast<CxR<Ar>*>(dst);
     p.stride = sl.stride;
     p.task0 = sl.task0;
-    p.sig = sl.sig;
+    p.work = sl.work;
     p.ddreal = sl.ddreal;
-    p.out = sl.out;
     return p;
 }
 
@@ -951,35 +1003,32 @@ int bluestein_kernel(DevCfft& d, bool dd_tables, cudaStream_t st) {
     return KBSRC_GPU_OK;
 }
 
-// Enqueues the block loop for every wave of tasks. ArL: four-step sub-FFT arithmetic, ArS: everything else.
+// Enqueues the block loop of `tasks` tasks of one plan, wave by wave through the slot buffers a, b.
+// ArL: four-step sub-FFT arithmetic, ArS: everything else.
 template <class ArL, class ArS>
-int enqueue(kbsrc_gpu_engine* e, const double* in, const double* head, const double* tail, double* out,
-            cudaStream_t st, Trail* trail) {
+int enqueue_plan(const PlanCore& pc, const Work& work, long long tasks, void* a, void* b, long long stride,
+                 long long wave, cudaStream_t st, Trail& tr) {
     static_assert(sizeof(CxR<ArL>) == sizeof(CxR<ArS>), "one element size per mode");
     using CS = CxR<ArS>;
     using WS = typename ArS::W;
-    Trail none;
-    Trail& tr = trail ? *trail : none;
-    const kbsrc_gpu_desc& d = e->d;
+    const kbsrc_gpu_desc& d = pc.d;
     Slots sl{};
-    sl.stride = e->stride;
-    sl.sig = Signal{in, head, tail, d.frames, d.edge_len, d.lead, (long long)e->hop * d.Q, d.nblk, d.channels};
-    sl.out = Output{out, d.nout, d.o, (long long)e->hop * d.P, (long long)d.marg * d.P, d.nblk, d.channels};
-    void* buf[2] = {e->bufA.p, e->bufB.p};
+    sl.stride = stride;
+    sl.work = work;
+    void* buf[2] = {a, b};
     int rc;
-    if ((rc = tr.mark(st, -1)) != KBSRC_GPU_OK) return rc;
-    for (long long t0 = 0; t0 < e->tasks; t0 += e->wave) {
+    for (long long t0 = 0; t0 < tasks; t0 += wave) {
         sl.task0 = t0;
-        sl.nt = (unsigned)std::min(e->wave, e->tasks - t0);
+        sl.nt = (unsigned)std::min(wave, tasks - t0);
         // forward real FFT: gather + complex FFT; the spectrum Z lands in buf[z]
         int z;
-        if (e->fw.m) {
+        if (pc.fw.m) {
             z = 0;
-            rc = launch_cfft<ArL, ArS, kSrcSignal, kDstComplex>(e->fw, sl, nullptr, buf[0], buf[1], buf[0], st, tr,
+            rc = launch_cfft<ArL, ArS, kSrcSignal, kDstComplex>(pc.fw, sl, nullptr, buf[0], buf[1], buf[0], st, tr,
                                                                  kFwdA, kFwdB);
         } else {
             z = 1;
-            rc = launch_cfft<ArL, ArS, kSrcSignal, kDstComplex>(e->fw, sl, buf[0], nullptr, nullptr, buf[1], st, tr,
+            rc = launch_cfft<ArL, ArS, kSrcSignal, kDstComplex>(pc.fw, sl, buf[0], nullptr, nullptr, buf[1], st, tr,
                                                                  kFwdA, kFwdB);
         }
         if (rc) return rc;
@@ -988,23 +1037,37 @@ int enqueue(kbsrc_gpu_engine* e, const double* in, const double* head, const dou
         s.Z = static_cast<CS*>(buf[z]);
         s.X = static_cast<CS*>(buf[1 - z]);
         s.Zi = static_cast<CS*>(buf[z]);
-        s.stride = e->stride;
-        s.w_fw = static_cast<const CxW<ArS>*>(e->w_fw.p);
-        s.w_iv = static_cast<const CxW<ArS>*>(e->w_iv.p);
-        s.H = static_cast<const WS*>(e->H.p);
-        s.h = e->hf; s.hi = e->hi; s.Nb = e->Nb; s.Mb = e->Mb; s.up = d.up; s.Jg = d.Jg;
-        k_split<ArS><<<dim3(grid_for(e->hf / 2 + 1 + (ArS::kDD ? 0 : e->hf / 2), 256), sl.nt), 256, 0, st>>>(s);
+        s.stride = stride;
+        s.w_fw = static_cast<const CxW<ArS>*>(pc.w_fw.p);
+        s.w_iv = static_cast<const CxW<ArS>*>(pc.w_iv.p);
+        s.H = static_cast<const WS*>(pc.H.p);
+        s.h = pc.hf; s.hi = pc.hi; s.Nb = pc.Nb; s.Mb = pc.Mb; s.up = d.up; s.Jg = d.Jg;
+        k_split<ArS><<<dim3(grid_for(pc.hf / 2 + 1 + (ArS::kDD ? 0 : pc.hf / 2), 256), sl.nt), 256, 0, st>>>(s);
         if ((rc = tr.mark(st, kSplit)) != KBSRC_GPU_OK) return rc;
-        k_merge<ArS><<<dim3(grid_for(e->hi / 2 + 1 + (ArS::kDD ? 0 : e->hi / 2), 256), sl.nt), 256, 0, st>>>(s);
+        k_merge<ArS><<<dim3(grid_for(pc.hi / 2 + 1 + (ArS::kDD ? 0 : pc.hi / 2), 256), sl.nt), 256, 0, st>>>(s);
         if ((rc = tr.mark(st, kMerge)) != KBSRC_GPU_OK) return rc;
         // inverse complex FFT of buf[z] and the output epilogue
-        rc = launch_cfft<ArL, ArS, kSrcComplex, kDstOutput>(e->iv, sl, buf[z], buf[1 - z], buf[z], nullptr, st, tr,
+        rc = launch_cfft<ArL, ArS, kSrcComplex, kDstOutput>(pc.iv, sl, buf[z], buf[1 - z], buf[z], nullptr, st, tr,
                                                              kInvA, kInvB);
         if (rc) return rc;
     }
-    e->launches = tr.launches;
-    KB_CUDA(cudaGetLastError());
     return KBSRC_GPU_OK;
+}
+
+int enqueue_any(const PlanCore& pc, const Work& work, long long tasks, void* a, void* b, long long stride,
+                long long wave, cudaStream_t st, Trail& tr) {
+    if (pc.exact) return enqueue_plan<ArDDShort, ArDDAccurate>(pc, work, tasks, a, b, stride, wave, st, tr);
+    return enqueue_plan<ArF64, ArF64>(pc, work, tasks, a, b, stride, wave, st, tr);
+}
+
+Work single_work(const PlanCore& pc, const double* in, const double* head, const double* tail, double* out) {
+    const kbsrc_gpu_desc& d = pc.d;
+    Work w{};
+    w.item0 = Item{in, head, tail, out, d.frames, d.edge_len, d.lead, d.nout, d.o, d.channels};
+    w.hopQ = (long long)pc.hop * d.Q;
+    w.hopP = (long long)pc.hop * d.P;
+    w.margP = (long long)d.marg * d.P;
+    return w;
 }
 
 long long cfft_launches(const DevCfft& c) {
@@ -1043,6 +1106,25 @@ int upload_real(const double* hilo, long long n, bool dd_tables, DevBuf& out) {
     return KBSRC_GPU_OK;
 }
 
+// Builds the plan of a descriptor (check_desc first): FFT tables, split/merge roots, kernel spectrum.
+int make_core(const kbsrc_gpu_desc* desc, PlanCore& pc, cudaStream_t st) {
+    int rc;
+    pc.d = *desc;
+    pc.d.H = nullptr;
+    pc.exact = desc->precision == KBSRC_GPU_EXACT;
+    pc.Nb = (int)(desc->nb * desc->Q);
+    pc.Mb = (int)(desc->nb * desc->P);
+    pc.hf = pc.Nb / 2;
+    pc.hi = pc.Mb / 2;
+    pc.hop = desc->nb - 2 * desc->marg;
+    const int fmax = env_int("KBSRC_GPU_FMAX", pc.exact ? 8 : 16);
+    if ((rc = make_dev_cfft(pc.hf, pc.exact, fmax, pc.fw, st)) != KBSRC_GPU_OK) return rc;
+    if ((rc = make_dev_cfft(pc.hi, pc.exact, fmax, pc.iv, st)) != KBSRC_GPU_OK) return rc;
+    if ((rc = upload_cx(split_roots(pc.Nb), pc.exact, pc.w_fw)) != KBSRC_GPU_OK) return rc;
+    if ((rc = upload_cx(split_roots(pc.Mb), pc.exact, pc.w_iv)) != KBSRC_GPU_OK) return rc;
+    return upload_real(desc->H, desc->H_len, pc.exact, pc.H);
+}
+
 int create_impl(const kbsrc_gpu_desc* desc, kbsrc_gpu_engine** out) {
     int rc = check_desc(desc);
     if (rc) return rc;
@@ -1053,33 +1135,17 @@ int create_impl(const kbsrc_gpu_desc* desc, kbsrc_gpu_engine** out) {
         kbsrc_gpu_engine* p;
         ~Guard() { delete p; }
     } guard{e};
-    e->d = *desc;
-    e->d.H = nullptr;
-    e->exact = desc->precision == KBSRC_GPU_EXACT;
     KB_CUDA(cudaGetDevice(&e->device));
-    e->Nb = (int)(desc->nb * desc->Q);
-    e->Mb = (int)(desc->nb * desc->P);
-    e->hf = e->Nb / 2;
-    e->hi = e->Mb / 2;
-    e->hop = desc->nb - 2 * desc->marg;
-    e->tasks = (long long)desc->channels * desc->nblk;
     KB_CUDA(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
-    const int fmax = env_int("KBSRC_GPU_FMAX", e->exact ? 8 : 16);
-    if ((rc = make_dev_cfft(e->hf, e->exact, fmax, e->fw, e->stream)) != KBSRC_GPU_OK) return rc;
-    if ((rc = make_dev_cfft(e->hi, e->exact, fmax, e->iv, e->stream)) != KBSRC_GPU_OK) return rc;
-    if ((rc = upload_cx(split_roots(e->Nb), e->exact, e->w_fw)) != KBSRC_GPU_OK) return rc;
-    if ((rc = upload_cx(split_roots(e->Mb), e->exact, e->w_iv)) != KBSRC_GPU_OK) return rc;
-    if ((rc = upload_real(desc->H, desc->H_len, e->exact, e->H)) != KBSRC_GPU_OK) return rc;
-    const size_t esize = e->exact ? 32 : 16;
-    // task slots: each holds the largest of h+1, h'+1 and the Bluestein lengths, rounded to 8
-    const long long need = std::max({(long long)e->hf + 1, (long long)e->hi + 1, e->fw.slot(), e->iv.slot()});
-    e->stride = (need + 7) / 8 * 8;
+    if ((rc = make_core(desc, *e, e->stream)) != KBSRC_GPU_OK) return rc;
+    e->tasks = (long long)desc->channels * desc->nblk;
+    e->stride = e->slot();
     const long long budget = (long long)env_int("KBSRC_GPU_WAVE_MB", 4096) << 20;
-    const long long per_task = 2 * e->stride * (long long)esize;
+    const long long per_task = 2 * e->stride * (long long)e->esize();
     e->wave = std::max(1LL, std::min({e->tasks, budget / per_task, 65535LL}));
     if (e->tasks > 0) {
-        if ((rc = e->bufA.alloc((size_t)(e->wave * e->stride * esize))) != KBSRC_GPU_OK) return rc;
-        if ((rc = e->bufB.alloc((size_t)(e->wave * e->stride * esize))) != KBSRC_GPU_OK) return rc;
+        if ((rc = e->bufA.alloc((size_t)(e->wave * e->stride * e->esize()))) != KBSRC_GPU_OK) return rc;
+        if ((rc = e->bufB.alloc((size_t)(e->wave * e->stride * e->esize()))) != KBSRC_GPU_OK) return rc;
     }
     guard.p = nullptr;
     *out = e;
@@ -1093,8 +1159,16 @@ int run_device_impl(kbsrc_gpu_engine* e, const double* in, const double* head, c
     if (e->tasks == 0 || d.nout == 0) return KBSRC_GPU_OK;
     if (d.frames > 0 && !in) return fail(KBSRC_GPU_E_ARG, "null input");
     if (d.edge_len > 0 && (!head || !tail)) return fail(KBSRC_GPU_E_ARG, "null edge buffers");
-    if (e->exact) return enqueue<ArDDShort, ArDDAccurate>(e, in, head, tail, out, st, trail);
-    return enqueue<ArF64, ArF64>(e, in, head, tail, out, st, trail);
+    Trail none;
+    Trail& tr = trail ? *trail : none;
+    int rc;
+    if ((rc = tr.mark(st, -1)) != KBSRC_GPU_OK) return rc;
+    rc = enqueue_any(*e, single_work(*e, in, head, tail, out), e->tasks, e->bufA.p, e->bufB.p, e->stride, e->wave,
+                     st, tr);
+    if (rc) return rc;
+    e->launches = tr.launches;
+    KB_CUDA(cudaGetLastError());
+    return KBSRC_GPU_OK;
 }
 
 }  // namespace
@@ -1102,6 +1176,148 @@ int run_device_impl(kbsrc_gpu_engine* e, const double* in, const double* head, c
 // ------------------------------------------------------------------------------------------------------
 // C ABI
 // ------------------------------------------------------------------------------------------------------
+// ---- batches: many conversions, grouped by plan -------------------------------------------------------------
+namespace {
+
+// Zeroes every conversion's output (the reference's value-initialised output), reading the pointers from the
+// item table so that the recorded run stays valid for new buffers.
+__global__ void k_zero_items(const Item* __restrict__ items, int count) {
+    const Item it = items[blockIdx.y];
+    const long long n = it.nout * it.ch;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        it.out[i] = 0.0;
+}
+
+bool same_plan(const kbsrc_gpu_desc& a, const kbsrc_gpu_desc& b) {
+    if (a.precision != b.precision || a.P != b.P || a.Q != b.Q || a.nb != b.nb || a.marg != b.marg || a.up != b.up ||
+        a.Jg != b.Jg || a.H_len != b.H_len)
+        return false;
+    return a.H == b.H || std::memcmp(a.H, b.H, (size_t)a.H_len * 16) == 0;
+}
+
+int batch_create_impl(const kbsrc_gpu_desc* descs, int count, kbsrc_gpu_batch** out) {
+    if (!descs || count < 1) return fail(KBSRC_GPU_E_ARG, "empty batch");
+    int rc;
+    for (int i = 0; i < count; i++)
+        if ((rc = check_desc(descs + i)) != KBSRC_GPU_OK) return fail(rc, "conversion " + std::to_string(i) + ": " + g_error);
+    if ((rc = require_device()) != KBSRC_GPU_OK) return rc;
+    if ((rc = allow_large_smem()) != KBSRC_GPU_OK) return rc;
+    auto bp = std::make_unique<kbsrc_gpu_batch>();
+    kbsrc_gpu_batch& b = *bp;
+    KB_CUDA(cudaGetDevice(&b.device));
+    KB_CUDA(cudaStreamCreateWithFlags(&b.stream, cudaStreamNonBlocking));
+    KB_CUDA(cudaEventCreateWithFlags(&b.done, cudaEventDisableTiming));
+    b.descs.assign(descs, descs + count);
+    b.group_of.assign(count, -1);
+    std::vector<int> rep;  // representative conversion of each group
+    for (int i = 0; i < count; i++) {
+        if (descs[i].nblk == 0 || descs[i].nout == 0) continue;
+        int g = -1;
+        for (size_t k = 0; k < rep.size() && g < 0; k++)
+            if (same_plan(descs[rep[k]], descs[i])) g = (int)k;
+        if (g < 0) {
+            g = (int)rep.size();
+            rep.push_back(i);
+            b.groups.push_back(std::make_unique<BatchGroup>());
+            if ((rc = make_core(descs + i, *b.groups.back(), b.stream)) != KBSRC_GPU_OK) return rc;
+        }
+        b.group_of[i] = g;
+        b.groups[g]->members.push_back(i);
+    }
+    // task tables (block-major per conversion) and slot buffers shared by the groups
+    long long bytes = 0, need = 0;
+    const long long budget = (long long)env_int("KBSRC_GPU_WAVE_MB", 4096) << 20;
+    for (auto& gp : b.groups) {
+        BatchGroup& g = *gp;
+        std::vector<TaskRef> refs;
+        for (int i : g.members)
+            for (long long blk = 0; blk < descs[i].nblk; blk++)
+                for (int c = 0; c < descs[i].channels; c++) refs.push_back(TaskRef{i, c, blk});
+        g.tasks = (long long)refs.size();
+        if ((rc = g.refs.alloc(refs.size() * sizeof(TaskRef))) != KBSRC_GPU_OK) return rc;
+        KB_CUDA(cudaMemcpy(g.refs.p, refs.data(), refs.size() * sizeof(TaskRef), cudaMemcpyHostToDevice));
+        g.stride = g.slot();
+        const long long per = g.stride * (long long)g.esize();
+        need = std::max(need, per);
+        bytes = std::max(bytes, std::min(g.tasks * per, budget));
+    }
+    bytes = std::max(bytes, need);
+    for (auto& gp : b.groups)
+        gp->wave = std::max(1LL, std::min({gp->tasks, bytes / (gp->stride * (long long)gp->esize()), 65535LL}));
+    if (!b.groups.empty()) {
+        if ((rc = b.bufA.alloc((size_t)bytes)) != KBSRC_GPU_OK) return rc;
+        if ((rc = b.bufB.alloc((size_t)bytes)) != KBSRC_GPU_OK) return rc;
+    }
+    if ((rc = b.items.alloc((size_t)count * sizeof(Item))) != KBSRC_GPU_OK) return rc;
+    KB_CUDA(cudaMallocHost(&b.items_host, (size_t)count * sizeof(Item)));
+    *out = bp.release();
+    return KBSRC_GPU_OK;
+}
+
+// The whole batch on one stream: item table upload, output zeroing, every group's block loop.
+int batch_enqueue(kbsrc_gpu_batch& b, cudaStream_t st, Trail& tr) {
+    const int count = (int)b.descs.size();
+    KB_CUDA(cudaMemcpyAsync(b.items.p, b.items_host, (size_t)count * sizeof(Item), cudaMemcpyHostToDevice, st));
+    long long most = 1;
+    for (const auto& d : b.descs) most = std::max(most, d.nout * d.channels);
+    k_zero_items<<<dim3(grid_for(most, 256), count), 256, 0, st>>>(static_cast<const Item*>(b.items.p), count);
+    int rc;
+    if ((rc = tr.mark(st, -2)) != KBSRC_GPU_OK) return rc;
+    for (auto& gp : b.groups) {
+        const BatchGroup& g = *gp;
+        Work w{};
+        w.items = static_cast<const Item*>(b.items.p);
+        w.refs = static_cast<const TaskRef*>(g.refs.p);
+        w.hopQ = (long long)g.hop * g.d.Q;
+        w.hopP = (long long)g.hop * g.d.P;
+        w.margP = (long long)g.d.marg * g.d.P;
+        if ((rc = enqueue_any(g, w, g.tasks, b.bufA.p, b.bufB.p, g.stride, g.wave, st, tr)) != KBSRC_GPU_OK) return rc;
+    }
+    KB_CUDA(cudaGetLastError());
+    return KBSRC_GPU_OK;
+}
+
+int batch_run_device_impl(kbsrc_gpu_batch& b, const double* const* in, const double* const* head,
+                          const double* const* tail, double* const* out, cudaStream_t st) {
+    const int count = (int)b.descs.size();
+    for (int i = 0; i < count; i++) {
+        const kbsrc_gpu_desc& d = b.descs[i];
+        if ((d.frames > 0 && !in[i]) || (d.nout > 0 && !out[i]) || (d.edge_len > 0 && (!head[i] || !tail[i])))
+            return fail(KBSRC_GPU_E_ARG, "null buffer for conversion " + std::to_string(i));
+    }
+    KB_CUDA(cudaEventSynchronize(b.done));  // the previous run has read the item table
+    for (int i = 0; i < count; i++) {
+        const kbsrc_gpu_desc& d = b.descs[i];
+        b.items_host[i] = Item{in[i], head ? head[i] : nullptr, tail ? tail[i] : nullptr, out[i], d.frames,
+                               d.edge_len, d.lead, d.nout, d.o, d.channels};
+    }
+    if (!b.graph) {
+        // record the run once; it reads every pointer from the item table, so it replays for new buffers
+        cudaGraph_t g = nullptr;
+        KB_CUDA(cudaStreamBeginCapture(b.stream, cudaStreamCaptureModeThreadLocal));
+        Trail tr;
+        int rc = batch_enqueue(b, b.stream, tr);
+        const cudaError_t ce = cudaStreamEndCapture(b.stream, &g);
+        if (rc) {
+            if (g) cudaGraphDestroy(g);
+            return rc;
+        }
+        if (ce != cudaSuccess) return fail(KBSRC_GPU_E_CUDA, std::string("stream capture: ") + cudaGetErrorString(ce));
+        const cudaError_t ie = cudaGraphInstantiate(&b.graph, g, 0);
+        cudaGraphDestroy(g);
+        if (ie != cudaSuccess) {
+            b.graph = nullptr;
+            return fail(KBSRC_GPU_E_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ie));
+        }
+        b.launches = tr.launches;
+    }
+    KB_CUDA(cudaGraphLaunch(b.graph, st));
+    KB_CUDA(cudaEventRecord(b.done, st));
+    return KBSRC_GPU_OK;
+}
+
+}  // namespace
+
 // ---- kernel spectrum for callers that cannot allocate device memory ----------------------------------------
 //
 // Some callers own every device allocation themselves and may not call cudaMalloc from a library: a host that
@@ -1392,6 +1608,88 @@ int kbsrc_gpu_kernel_spectrum_static(const double* d_taps, int L, int n, double 
     } catch (const std::exception& x) {
         return fail(KBSRC_GPU_E_CUDA, x.what());
     }
+}
+
+int kbsrc_gpu_batch_create(const kbsrc_gpu_desc* descs, int count, kbsrc_gpu_batch** out) {
+    if (!out) return fail(KBSRC_GPU_E_ARG, "null output pointer");
+    *out = nullptr;
+    try {
+        return batch_create_impl(descs, count, out);
+    } catch (const std::bad_alloc&) {
+        return fail(KBSRC_GPU_E_NOMEM, "host allocation failed");
+    } catch (const std::exception& x) {
+        return fail(KBSRC_GPU_E_ARG, x.what());
+    }
+}
+
+int kbsrc_gpu_batch_run_device(kbsrc_gpu_batch* b, const double* const* d_in, const double* const* d_head,
+                               const double* const* d_tail, double* const* d_out, void* stream) {
+    if (!b || !d_in || !d_out) return fail(KBSRC_GPU_E_ARG, "null batch or buffer array");
+    try {
+        return batch_run_device_impl(*b, d_in, d_head, d_tail, d_out, stream ? (cudaStream_t)stream : b->stream);
+    } catch (const std::exception& x) {
+        return fail(KBSRC_GPU_E_CUDA, x.what());
+    }
+}
+
+int kbsrc_gpu_batch_run_host(kbsrc_gpu_batch* b, const double* const* in, const double* const* head,
+                             const double* const* tail, double* const* out) {
+    if (!b || !in || !out) return fail(KBSRC_GPU_E_ARG, "null batch or buffer array");
+    try {
+        const int count = (int)b->descs.size();
+        int rc;
+        if (b->d_in.empty()) {
+            b->d_in.resize(count); b->d_head.resize(count); b->d_tail.resize(count); b->d_out.resize(count);
+            for (int i = 0; i < count; i++) {
+                const kbsrc_gpu_desc& d = b->descs[i];
+                if ((rc = b->d_in[i].alloc((size_t)(d.frames * d.channels * 8))) != KBSRC_GPU_OK) return rc;
+                if ((rc = b->d_head[i].alloc((size_t)(d.edge_len * d.channels * 8))) != KBSRC_GPU_OK) return rc;
+                if ((rc = b->d_tail[i].alloc((size_t)(d.edge_len * d.channels * 8))) != KBSRC_GPU_OK) return rc;
+                if ((rc = b->d_out[i].alloc((size_t)(d.nout * d.channels * 8))) != KBSRC_GPU_OK) return rc;
+            }
+        }
+        std::vector<const double*> pi(count), ph(count), pt(count);
+        std::vector<double*> po(count);
+        cudaStream_t st = b->stream;
+        for (int i = 0; i < count; i++) {
+            const kbsrc_gpu_desc& d = b->descs[i];
+            const size_t ni = (size_t)(d.frames * d.channels * 8), ne = (size_t)(d.edge_len * d.channels * 8);
+            if (ni) KB_CUDA(cudaMemcpyAsync(b->d_in[i].p, in[i], ni, cudaMemcpyHostToDevice, st));
+            if (ne && head && tail) {
+                KB_CUDA(cudaMemcpyAsync(b->d_head[i].p, head[i], ne, cudaMemcpyHostToDevice, st));
+                KB_CUDA(cudaMemcpyAsync(b->d_tail[i].p, tail[i], ne, cudaMemcpyHostToDevice, st));
+            }
+            pi[i] = (const double*)b->d_in[i].p; ph[i] = (const double*)b->d_head[i].p;
+            pt[i] = (const double*)b->d_tail[i].p; po[i] = (double*)b->d_out[i].p;
+        }
+        if ((rc = batch_run_device_impl(*b, pi.data(), ph.data(), pt.data(), po.data(), st)) != KBSRC_GPU_OK) return rc;
+        for (int i = 0; i < count; i++) {
+            const kbsrc_gpu_desc& d = b->descs[i];
+            if (d.nout) KB_CUDA(cudaMemcpyAsync(out[i], po[i], (size_t)(d.nout * d.channels * 8), cudaMemcpyDeviceToHost, st));
+        }
+        KB_CUDA(cudaStreamSynchronize(st));
+        return KBSRC_GPU_OK;
+    } catch (const std::exception& x) {
+        return fail(KBSRC_GPU_E_CUDA, x.what());
+    }
+}
+
+int kbsrc_gpu_batch_info(const kbsrc_gpu_batch* b, long long* groups, long long* tasks, long long* launches) {
+    if (!b) return fail(KBSRC_GPU_E_ARG, "null batch");
+    long long t = 0, l = 0;
+    for (const auto& g : b->groups) {
+        t += g->tasks;
+        l += (cfft_launches(g->fw) + 2 + cfft_launches(g->iv)) * ((g->tasks + g->wave - 1) / g->wave);
+    }
+    if (groups) *groups = (long long)b->groups.size();
+    if (tasks) *tasks = t;
+    if (launches) *launches = l + 1;  // + the output zeroing
+    return KBSRC_GPU_OK;
+}
+
+void kbsrc_gpu_batch_destroy(kbsrc_gpu_batch* b) {
+    if (b && b->done) cudaEventSynchronize(b->done);
+    delete b;
 }
 
 const char* kbsrc_gpu_last_error(void) { return g_error.c_str(); }

@@ -12,7 +12,10 @@
 #include <climits>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <memory>
+#include <mutex>
+#include <tuple>
 #include <numeric>
 #include <stdexcept>
 #include <string>
@@ -267,12 +270,20 @@ struct Conversion {
     long long frames = 0;
     std::vector<double> head, tail;  // LPC edges, ch * ext each
     long long ext = 0;
+    std::vector<double> H;           // kernel spectrum (hi, lo) pairs
+    kbsrc_gpu_desc desc{};           // the engine's plan (desc.H points into H)
     EngineHandle eng;
     double design_seconds = 0;
 };
 
+// Kernel spectra shared by the conversions of a batch: the same taps and transform give the same spectrum.
+struct SpectrumCache {
+    std::map<std::tuple<int, long long, long long, double, int, long long>, std::vector<double>> m;
+    std::mutex mu;
+};
+
 std::unique_ptr<Conversion> prepare(const double* in, long long frames, int ch, int rate_in, int rate_out,
-                                    const Options& opt) {
+                                    const Options& opt, bool make_engine = true, SpectrumCache* cache = nullptr) {
     auto cv = std::make_unique<Conversion>();
     cv->pl = make_plan(in, frames, ch, rate_in, rate_out, opt);
     cv->opt = opt;
@@ -313,8 +324,8 @@ std::unique_ptr<Conversion> prepare(const double* in, long long frames, int ch, 
         });
     }
     // kernel: taps on the host, spectrum on the GPU (design.cpp:40-49)
-    std::vector<dd> taps;
-    int nspec, Jg = 0;
+    int L, nspec, Jg = 0;
+    long long ta, tb;
     if (pl.general) {
         // Near-unity ratios: the kernel sampled on a finer grid of Nk points (rate Nk*fi/Nb) so its spectrum is
         // the true continuous response, folded modulo Mb by the engine (resampler.cpp:187-202).
@@ -325,20 +336,40 @@ std::unique_ptr<Conversion> prepare(const double* in, long long frames, int ch, 
         const long long g2 = (long long)std::gcd((unsigned long long)pl.c2 * (unsigned long long)Nb,
                                                  (unsigned long long)Nk * (unsigned long long)pl.fi);
         const double fk2 = (double)Nk * pl.fi / Nb;
-        taps = kaiser_taps((int)std::floor(opt.length * fk2), (long long)(A / g2), (long long)(B / g2), opt.beta,
-                           threads);
+        L = (int)std::floor(opt.length * fk2);
+        ta = (long long)(A / g2);
+        tb = (long long)(B / g2);
         nspec = (int)Nk;
         Jg = (int)std::min<long long>(Nk / 2, (long long)std::ceil((pl.mn / 2.0 + 4 * pl.fml) * Nb / pl.fi));
     } else {
         const long long gc = std::gcd(pl.c2, pl.fk);
-        taps = kaiser_taps((int)pl.Lk, pl.c2 / gc, pl.fk / gc, opt.beta, threads);
+        L = (int)pl.Lk;
+        ta = pl.c2 / gc;
+        tb = pl.fk / gc;
         nspec = (int)(pl.up ? Mb : Nb);
     }
-    std::vector<double> H((size_t)(nspec / 2 + 1) * 2);
-    gpu_check(kbsrc_gpu_kernel_spectrum(reinterpret_cast<const double*>(taps.data()), (int)taps.size() - 1, nspec,
-                                        (double)Nb, H.data()),
-              "kernel spectrum");
-    kbsrc_gpu_desc d{};
+    const auto key = std::make_tuple(L, ta, tb, opt.beta, nspec, Nb);
+    bool cached = false;
+    if (cache) {
+        std::lock_guard<std::mutex> lock(cache->mu);
+        auto it = cache->m.find(key);
+        if (it != cache->m.end()) {
+            cv->H = it->second;
+            cached = true;
+        }
+    }
+    if (!cached) {
+        const std::vector<dd> taps = kaiser_taps(L, ta, tb, opt.beta, threads);
+        cv->H.assign((size_t)(nspec / 2 + 1) * 2, 0.0);
+        gpu_check(kbsrc_gpu_kernel_spectrum(reinterpret_cast<const double*>(taps.data()), L, nspec, (double)Nb,
+                                            cv->H.data()),
+                  "kernel spectrum");
+        if (cache) {
+            std::lock_guard<std::mutex> lock(cache->mu);
+            cache->m.emplace(key, cv->H);
+        }
+    }
+    kbsrc_gpu_desc& d = cv->desc;
     d.precision = opt.precision == Precision::Fast ? KBSRC_GPU_FAST : KBSRC_GPU_EXACT;
     d.channels = ch;
     d.P = P;
@@ -353,9 +384,9 @@ std::unique_ptr<Conversion> prepare(const double* in, long long frames, int ch, 
     d.up = pl.up;
     d.Jg = Jg;
     d.edge_len = ext;
-    d.H = H.data();
-    d.H_len = (long long)H.size() / 2;
-    gpu_check(kbsrc_gpu_engine_create(&d, &cv->eng.e), "GPU engine");
+    d.H = cv->H.data();
+    d.H_len = (long long)cv->H.size() / 2;
+    if (make_engine) gpu_check(kbsrc_gpu_engine_create(&d, &cv->eng.e), "GPU engine");
     cv->design_seconds = now() - t0;
     return cv;
 }
@@ -588,3 +619,120 @@ extern "C" int kbsrc_burg_c(const double* x, long long len, long long n, double*
         return -4;
     }
 }
+
+// ---- batches of conversions ------------------------------------------------------------------------------------
+namespace kbsrc {
+namespace {
+struct BatchRun {
+    std::vector<std::unique_ptr<Conversion>> convs;
+    std::vector<int> gpu_index;  // conversion -> position in the GPU batch, -1 for equal-rate copies
+    kbsrc_gpu_batch* gb = nullptr;
+    ~BatchRun() { kbsrc_gpu_batch_destroy(gb); }
+};
+}  // namespace
+}  // namespace kbsrc
+
+extern "C" int kbsrc_batch_prepare_c(const kbsrc_batch_item_c* items, int count, const kbsrc_options_c* copt,
+                                     kbsrc_batch** out, char* err, int err_len) {
+    if (!out || !items || count < 1) return (int)report("empty batch", -1, err, err_len);
+    *out = nullptr;
+    try {
+        const kbsrc::Options o = options_from_c(copt);
+        kbsrc::RoundToNearest rn(o.precision == kbsrc::Precision::Exact);
+        auto b = std::make_unique<kbsrc::BatchRun>();
+        b->convs.resize(count);
+        kbsrc::SpectrumCache cache;
+        std::vector<std::string> errors(count);
+        std::vector<int> kinds(count, 0);  // 1 invalid argument, 3 runtime, 4 memory
+        const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
+        kbsrc::Options inner = o;
+        inner.threads = 1;  // parallel over conversions instead
+        kbsrc::parallel_for(o.threads ? o.threads : hw, count, 1, [&](long long i) {
+            kbsrc::RoundToNearest rn_worker(o.precision == kbsrc::Precision::Exact);
+            try {
+                b->convs[i] = kbsrc::prepare(items[i].in, items[i].frames, items[i].channels, items[i].rate_in,
+                                             items[i].rate_out, inner, false, &cache);
+            } catch (const std::invalid_argument& x) {
+                errors[i] = x.what();
+                kinds[i] = 1;
+            } catch (const std::bad_alloc&) {
+                errors[i] = "out of memory";
+                kinds[i] = 4;
+            } catch (const std::exception& x) {
+                errors[i] = x.what();
+                kinds[i] = 3;
+            }
+        });
+        for (int i = 0; i < count; i++)
+            if (kinds[i])
+                return (int)report(("conversion " + std::to_string(i) + ": " + errors[i]).c_str(), -kinds[i], err,
+                                   err_len);
+        std::vector<kbsrc_gpu_desc> descs;
+        b->gpu_index.assign(count, -1);
+        for (int i = 0; i < count; i++)
+            if (!b->convs[i]->pl.copy) {
+                b->gpu_index[i] = (int)descs.size();
+                descs.push_back(b->convs[i]->desc);
+            }
+        if (!descs.empty())
+            kbsrc::gpu_check(kbsrc_gpu_batch_create(descs.data(), (int)descs.size(), &b->gb), "GPU batch");
+        *out = reinterpret_cast<kbsrc_batch*>(b.release());
+        return 0;
+    } catch (const std::invalid_argument& x) {
+        return (int)report(x.what(), -1, err, err_len);
+    } catch (const std::bad_alloc&) {
+        return (int)report("out of memory", -4, err, err_len);
+    } catch (const std::exception& x) {
+        return (int)report(x.what(), -3, err, err_len);
+    }
+}
+
+extern "C" int kbsrc_batch_run_c(kbsrc_batch* bp, const double* const* in, double* const* out, char* err,
+                                 int err_len) {
+    if (!bp || !in || !out) return (int)report("null batch or buffer array", -1, err, err_len);
+    try {
+        auto& b = *reinterpret_cast<kbsrc::BatchRun*>(bp);
+        const int count = (int)b.convs.size();
+        std::vector<const double*> gi, gh, gt;
+        std::vector<double*> go;
+        for (int i = 0; i < count; i++) {
+            const kbsrc::Conversion& cv = *b.convs[i];
+            if (b.gpu_index[i] < 0) {  // equal rates: the host copy
+                for (int c = 0; c < cv.ch; c++)
+                    for (long long f = 0; f < cv.frames; f++) out[i][c * cv.pl.nout + f] = in[i][f * cv.ch + c];
+                continue;
+            }
+            gi.push_back(in[i]);
+            gh.push_back(cv.head.data());
+            gt.push_back(cv.tail.data());
+            go.push_back(out[i]);
+        }
+        if (b.gb)
+            kbsrc::gpu_check(kbsrc_gpu_batch_run_host(b.gb, gi.data(), gh.data(), gt.data(), go.data()), "GPU batch");
+        return 0;
+    } catch (const std::bad_alloc&) {
+        return (int)report("out of memory", -4, err, err_len);
+    } catch (const std::exception& x) {
+        return (int)report(x.what(), -3, err, err_len);
+    }
+}
+
+extern "C" int kbsrc_batch_info_c(const kbsrc_batch* bp, int i, long long* nout, long long* edge_len,
+                                  const double** head, const double** tail, int* gpu_index) {
+    if (!bp) return -1;
+    const auto& b = *reinterpret_cast<const kbsrc::BatchRun*>(bp);
+    if (i < 0 || i >= (int)b.convs.size()) return -1;
+    const kbsrc::Conversion& cv = *b.convs[i];
+    if (nout) *nout = cv.pl.nout;
+    if (edge_len) *edge_len = cv.ext;
+    if (head) *head = cv.head.data();
+    if (tail) *tail = cv.tail.data();
+    if (gpu_index) *gpu_index = b.gpu_index[i];
+    return 0;
+}
+
+extern "C" kbsrc_gpu_batch* kbsrc_batch_gpu_c(kbsrc_batch* bp) {
+    return bp ? reinterpret_cast<kbsrc::BatchRun*>(bp)->gb : nullptr;
+}
+
+extern "C" void kbsrc_batch_free_c(kbsrc_batch* bp) { delete reinterpret_cast<kbsrc::BatchRun*>(bp); }

@@ -80,3 +80,32 @@ def make_input(recipe):
 
 def is_small(name):
     return name.startswith("s_")
+
+
+# The uneven multi-file queue: for file i of `count`, length uniform in [min_s, max_s] seconds (whole frames),
+# 1-8 channels, an input rate from C4_RATES_IN and an output rate from C4_RATES_OUT, all drawn from
+# default_rng(seed); samples normal(0, 0.2) from default_rng([seed, i]), clipped to +-1 and rounded to float32
+# (the files are 32-bit float WAVs).
+C4_RATES_IN = [44100, 48000, 88200, 96000, 192000]
+C4_RATES_OUT = [44100, 48000, 96000]
+
+
+def c4_specs(seed=3, count=256, min_s=1.0, max_s=60.0):
+    rng = np.random.default_rng(seed)
+    specs = []
+    for _ in range(count):
+        sec = rng.uniform(min_s, max_s)
+        ch = int(rng.integers(1, 9))
+        fi = int(rng.choice(C4_RATES_IN))
+        fo = int(rng.choice(C4_RATES_OUT))
+        specs.append((int(round(sec * fi)), ch, fi, fo))
+    return specs
+
+
+def c4_samples(seed, i, frames, ch):
+    x = np.random.default_rng([seed, i]).normal(0.0, 0.2, (frames, ch))
+    return np.clip(x, -1.0, 1.0).astype(np.float32).astype(np.float64)
+
+
+# the scaled-down queue of the parity tests: 48 files of 0.2-3 s
+C4_SMALL = dict(seed=3, count=48, min_s=0.2, max_s=3.0)

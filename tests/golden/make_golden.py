@@ -29,9 +29,18 @@ def main():
         out[name] = {"sha256": hashlib.sha256(y.tobytes()).hexdigest(), "shape": list(y.shape),
                      "input_sha256": hashlib.sha256(x.astype("<f8").tobytes()).hexdigest()}
         print(name, y.shape, out[name]["sha256"][:16], flush=True)
+    # the scaled-down uneven queue, exact mode, one reference conversion per file
+    from cases import C4_SMALL, c4_specs, c4_samples
+    c4 = []
+    for i, (frames, ch, fi, fo) in enumerate(c4_specs(**C4_SMALL)):
+        x = c4_samples(C4_SMALL["seed"], i, frames, ch)
+        y = oracle.ref_resample(x, fi, fo).astype("<f8", copy=False)
+        c4.append({"spec": [frames, ch, fi, fo], "sha256": hashlib.sha256(y.tobytes()).hexdigest(),
+                   "shape": list(y.shape)})
+    print("c4_small", len(c4), "files", flush=True)
     with open(os.path.join(HERE, "golden.json"), "w") as f:
         json.dump({"generator": "HongYue1/KBSRC 1.3.0 built from source (oracle/_ref), kbsrc::resample",
-                   "cases": out}, f, indent=1, sort_keys=True)
+                   "cases": out, "c4_small": c4}, f, indent=1, sort_keys=True)
 
 
 if __name__ == "__main__":
