@@ -35,6 +35,8 @@ WORKLOADS = {
     "c2_fast": dict(seed=2, seconds=180, rate_in=96000, rate_out=44100, channels=2, mode="fast"),
     "c1_exact": dict(seed=1, seconds=10, rate_in=96000, rate_out=44100, channels=2, mode="exact"),
     "c3_exact": dict(sweep=True, seconds=60, rate_in=44100, rate_out=48000, channels=2, mode="exact"),
+    # the uneven queue: 256 files, 1-60 s, 1-8 channels, mixed rate pairs, one GPU batch (exact)
+    "c4_exact": dict(batch=True, seed=3, files=256, mode="exact"),
 }
 METRIC = "out Msamples/s 96k->44.1k exact (180 s stereo f64, byte-identical to the reference)"
 
@@ -348,6 +350,130 @@ def product_arm(args, w, world, rank, local, pg):
         pg.destroy_process_group()
 
 
+def batch_arm(args, w, world, rank, local, pg):
+    """The uneven multi-file queue as one GPU batch (kbsrc_b200.Batch): value on device-resident buffers, e2e
+    through the C batch entry with host buffers registered as pinned memory."""
+    import ctypes
+    import hashlib
+    import torch
+    import kbsrc_b200
+    from kbsrc_b200 import roofline
+    from cases import c4_samples, c4_specs
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    specs = c4_specs(seed=w["seed"], count=w["files"])
+    xs = [c4_samples(w["seed"], i, n, ch) for i, (n, ch, _, _) in enumerate(specs)]
+    t = time.perf_counter()
+    b = kbsrc_b200.Batch([(x, fi, fo) for x, (_, _, fi, fo) in zip(xs, specs)], mode=w["mode"])
+    prepare_s = time.perf_counter() - t
+    info = b.gpu_info()
+    gpu_items = [i for i, g in enumerate(b.gpu_index) if g >= 0]
+    samples = sum(specs[i][1] * b.nout[i] for i in range(len(specs)))
+    gpu_samples = sum(specs[i][1] * b.nout[i] for i in gpu_items)
+    ops = 0
+    for i in gpu_items:
+        n, ch, fi, fo = specs[i]
+        p = kbsrc_b200.plan(n, ch, fi, fo, w["mode"])
+        ops += roofline.conversion_work(p, ch, w["mode"] == "exact")["ops_total"]
+    side = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(side)
+    d_in = [torch.from_numpy(xs[i]).to(dev) for i in gpu_items]
+    d_h = [torch.from_numpy(b.head[i]).to(dev) for i in gpu_items]
+    d_t = [torch.from_numpy(b.tail[i]).to(dev) for i in gpu_items]
+    d_o = [torch.empty(specs[i][1] * max(b.nout[i], 1), dtype=torch.float64, device=dev) for i in gpu_items]
+    ptrs = [[t.data_ptr() for t in v] for v in (d_in, d_h, d_t, d_o)]
+    for _ in range(args.warmup):
+        b.run_device(*ptrs, stream=side.cuda_stream)
+    torch.cuda.synchronize()
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",")
+    phys = vis[local] if local < len(vis) and vis[local].strip().isdigit() else str(local)
+    sampler = ClockSampler(int(phys))
+    with sampler:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            b.run_device(*ptrs, stream=side.cuda_stream)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+    # byte identity of the timed outputs against the reference, file by file
+    golden = None
+    try:
+        with open(os.path.join(ROOT, "tests", "golden", "golden_c4.json")) as f:
+            golden = json.load(f)["files"]
+    except Exception:
+        pass
+    mism = None
+    if golden and w["files"] == len(golden):
+        mism = 0
+        for k, i in enumerate(gpu_items):
+            y = d_o[k][:specs[i][1] * b.nout[i]].cpu().numpy()
+            if hashlib.sha256(y.astype("<f8").tobytes()).hexdigest() != golden[i]["sha256"]:
+                mism += 1
+    del d_in, d_h, d_t, d_o, ptrs
+    torch.cuda.empty_cache()
+    # e2e: host buffers (registered pinned) through the batch C entry, copies inside the timed region
+    outs = [np.zeros((x.shape[1], max(n, 1))) for x, n in zip(xs, b.nout)]
+    cudart = torch.cuda.cudart()
+    regs = []
+    for a in xs + outs:
+        if a.nbytes and int(cudart.cudaHostRegister(a.ctypes.data, a.nbytes, 0)) == 0:
+            regs.append(a)
+    pin = (ctypes.c_void_p * len(xs))(*[x.ctypes.data for x in xs])
+    pout = (ctypes.c_void_p * len(xs))(*[o.ctypes.data for o in outs])
+    err = ctypes.create_string_buffer(512)
+    kbsrc_b200.host_lib().kbsrc_batch_run_c(b._h, pin, pout, err, 512)  # first call allocates
+    e2e_steps = max(2, args.steps // 3)
+    t = time.perf_counter()
+    for _ in range(e2e_steps):
+        if kbsrc_b200.host_lib().kbsrc_batch_run_c(b._h, pin, pout, err, 512):
+            raise RuntimeError(err.value.decode())
+    e2e_s = time.perf_counter() - t
+    for a in regs:
+        cudart.cudaHostUnregister(a.ctypes.data)
+    value = samples * args.steps / (ms * 1e-3) / 1e6
+    peaks = fp64_peak()
+    peak = max(peaks.values()) if peaks else None
+    achieved = ops / (ms * 1e-3 / args.steps)
+    cpu = None
+    if not args.no_cpu:
+        from oracle import oracle
+        if oracle.ref_available():
+            n_out, secs = 0, 0.0
+            for i in range(8):  # bounded sample: the first 8 files, engine time, all host threads
+                st = {}
+                y = oracle.ref_resample(xs[i], specs[i][2], specs[i][3], threads=os.cpu_count() or 1, stats=st)
+                n_out += y.size
+                secs += st["process_seconds"]
+            cpu = {"value": round(n_out / secs / 1e6, 3), "unit": "Msamples/s", "cores": os.cpu_count(),
+                   "kind": "reference", "sample": "the first 8 files of the queue, each converted alone by the "
+                   "reference built from source, engine time (Stats::process_seconds), all host threads"}
+    line = {
+        "metric": "out Msamples/s, uneven 256-file queue, exact (byte-identical per file)", "value": round(value, 3),
+        "unit": "Msamples/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "dd (double-double f64 pairs)", "data": "synthetic",
+        "config": {"workload": args.workload, "files": w["files"], "gpu_files": len(gpu_items),
+                   "output_samples": samples, "gpu_output_samples": gpu_samples, "groups": info["groups"],
+                   "tasks": info["tasks"], "l2": "inputs larger than L2"},
+        "e2e": {"value": round(samples * e2e_steps / e2e_s / 1e6, 3), "unit": "Msamples/s",
+                "h2d_bytes_per_step": int(sum(8 * x.size for x in xs) + sum(8 * (h.size + t.size) for h, t in
+                                                                            zip(b.head, b.tail))),
+                "d2h_bytes_per_step": int(8 * samples), "path": "kbsrc_batch_run_c (C API), pinned"},
+        "gpu_launches": int(info["launches"] * args.steps),
+        "roofline": {"bound": "fp64", "achieved": round(achieved / 1e12, 3),
+                     "peak": round(peak / 1e12, 3) if peak else None, "unit": "TFLOP/s",
+                     "frac": round(achieved / peak, 4) if peak else None, "traffic": None, "kernel": "whole batch",
+                     "note": "FP64 instructions of all groups per step / step time; the batch runs as one graph"},
+        "prepare_seconds": round(prepare_s, 3),
+        "cpu_baseline": cpu, "clocks": sampler.summary(),
+        "files_differing_from_reference": mism,
+    }
+    print(json.dumps(line), flush=True)
+    b.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -361,6 +487,8 @@ def main():
     world, rank, local, pg = dist_setup(args)
     if args.impl == "reference":
         reference_arm(args, w, world, rank, pg)
+    elif w.get("batch"):
+        batch_arm(args, w, world, rank, local, pg)
     else:
         product_arm(args, w, world, rank, local, pg)
 

@@ -42,6 +42,15 @@ std::vector<std::vector<double>> resample(const double* interleaved, long long f
                                           int rate_in, int rate_out, const Options& options = {},
                                           Stats* stats = nullptr);
 
+// The same conversion followed by the output step of a WAV writer, on the GPU: returns the data section of a WAV
+// file in `format` ("f64", "f32", "s32", "s24" or "s16"), interleaved little-endian; integer formats are scaled,
+// TPDF-dithered when `dither` (std::mt19937_64 seeded 12345, two uniform(-0.5, 0.5) draws per sample), rounded and
+// clipped, with the clipped count in `clipped` - byte for byte what the reference's kbsrc tool writes. Equal rates
+// (no conversion) throw std::invalid_argument.
+std::vector<unsigned char> resample_wav_data(const double* interleaved, long long frames, int channels, int rate_in,
+                                             int rate_out, const char* format, bool dither, long long& clipped,
+                                             const Options& options = {}, Stats* stats = nullptr);
+
 const char* version();
 
 }  // namespace kbsrc

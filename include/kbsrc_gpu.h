@@ -78,6 +78,20 @@ int kbsrc_gpu_engine_run_device_timed(kbsrc_gpu_engine* e, const double* d_in, c
                                       const double* d_tail, double* d_out, void* stream, float* pass_ms,
                                       int* pass_launches);
 
+/* Output step on the GPU (src/io/wav.cpp:242-255,371-418): the interleaved little-endian data section of a WAV
+ * file in `format` (0 f64, 1 f32, 2 s32, 3 s24, 4 s16). Integer formats are scaled by 2^(8B-1), TPDF-dithered
+ * when `dither` (two uniform(-0.5, 0.5) draws per sample from std::mt19937_64 seeded 12345, frame-major order,
+ * generated on the GPU), rounded to nearest, clipped; *clipped receives the number of clipped samples.
+ * kbsrc_gpu_engine_run_host_packed: the block loop on host input followed by the packing; out_bytes is
+ *   host memory of channels * nout * bytes-per-sample.
+ * kbsrc_gpu_pack: packs planar device samples (ch x frames, row stride `stride`) into device memory d_out on
+ *   `stream`, synchronous. */
+int kbsrc_gpu_engine_run_host_packed(kbsrc_gpu_engine* e, const double* in, const double* head,
+                                     const double* tail, int format, int dither, unsigned char* out_bytes,
+                                     long long* clipped);
+int kbsrc_gpu_pack(const double* d_planar, int channels, long long frames, long long stride, int format, int dither,
+                   unsigned char* d_out, long long* clipped, void* stream);
+
 /* Number of (channel, block) tasks, kernel launches per run, and the engine's device bytes. */
 int kbsrc_gpu_engine_info(const kbsrc_gpu_engine* e, long long* tasks, long long* launches,
                           long long* device_bytes);

@@ -67,6 +67,10 @@ GPU_SYMBOLS = {
     "kbsrc_gpu_engine_run_device_timed": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                                          ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                                          _P(ctypes.c_float), _P(ctypes.c_int)]),
+    "kbsrc_gpu_engine_run_host_packed": (ctypes.c_int, [ctypes.c_void_p, _dp, _dp, _dp, ctypes.c_int, ctypes.c_int,
+                                                        ctypes.c_void_p, _lp]),
+    "kbsrc_gpu_pack": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_longlong, ctypes.c_longlong, ctypes.c_int,
+                                      ctypes.c_int, ctypes.c_void_p, _lp, ctypes.c_void_p]),
     "kbsrc_gpu_engine_info": (ctypes.c_int, [ctypes.c_void_p, _lp, _lp, _lp]),
     "kbsrc_gpu_engine_destroy": (None, [ctypes.c_void_p]),
     "kbsrc_gpu_kernel_spectrum": (ctypes.c_int, [_dp, ctypes.c_int, ctypes.c_int, ctypes.c_double, _dp]),
@@ -365,6 +369,26 @@ def burg(x, n):
     if host_lib().kbsrc_burg_c(_ptr(x), len(x), n, _ptr(out)):
         raise ValueError("bad arguments")
     return out
+
+
+FORMATS = {"f64": (0, 8), "f32": (1, 4), "s32": (2, 4), "s24": (3, 3), "s16": (4, 2)}
+
+
+def pack(planar, fmt, dither=False):
+    """The GPU output step (kbsrc_gpu_pack): planar (channels, frames) float64 -> (WAV data bytes, clipped)."""
+    import torch
+    code, bps = FORMATS[fmt]
+    planar = np.ascontiguousarray(planar, dtype=np.float64)
+    ch, n = planar.shape
+    d_y = torch.from_numpy(planar).cuda()
+    d_o = torch.empty(max(1, ch * n * bps), dtype=torch.uint8, device="cuda")
+    clipped = ctypes.c_longlong()
+    rc = gpu_lib().kbsrc_gpu_pack(d_y.data_ptr(), ch, n, n, code, int(dither), d_o.data_ptr(), ctypes.byref(clipped),
+                                  None)
+    if rc:
+        raise RuntimeError(f"kbsrc_gpu_pack: {rc} {gpu_error()}")
+    torch.cuda.synchronize()
+    return d_o[:ch * n * bps].cpu().numpy().tobytes(), clipped.value
 
 
 def kernel_spectrum(taps, n, scale):

@@ -1176,6 +1176,133 @@ int run_device_impl(kbsrc_gpu_engine* e, const double* in, const double* head, c
 // ------------------------------------------------------------------------------------------------------
 // C ABI
 // ------------------------------------------------------------------------------------------------------
+// ---- output conversion: WAV sample packing and TPDF dither on the GPU -------------------------------------------
+//
+// The reference's writer (src/io/wav.cpp:242-255,371-418) interleaves the planar output and, for integer
+// formats, scales by 2^(8B-1), adds two draws of uniform_real_distribution<double>(-0.5, 0.5) from
+// std::mt19937_64 seeded 12345 per sample (frame-major, channel-minor), rounds to nearest, clips and counts the
+// clipped samples. The packer reproduces it sample for sample; the dither stream is the same generator run on the
+// GPU (MT19937-64, Matsumoto and Nishimura 2000): one CTA updates the 312-word state in parallel in the order the
+// sequential twist would, then tempers 312 outputs, two per sample.
+namespace {
+
+constexpr int kMtN = 312, kMtM = 156;
+constexpr unsigned long long kMtA = 0xB5026F5AA96619E9ULL, kMtUpper = 0xFFFFFFFF80000000ULL,
+                             kMtLower = 0x7FFFFFFFULL;
+
+__device__ __forceinline__ unsigned long long mt_temper(unsigned long long y) {
+    y ^= (y >> 29) & 0x5555555555555555ULL;
+    y ^= (y << 17) & 0x71D67FFFEDA60000ULL;
+    y ^= (y << 37) & 0xFFF7EEE000000000ULL;
+    y ^= y >> 43;
+    return y;
+}
+
+// uniform_real_distribution<double>(-0.5, 0.5) of one 64-bit draw: u / 2^64 (kept below 1), times (b - a), plus a
+__device__ __forceinline__ double mt_uniform(unsigned long long u) {
+    double r = __ddiv_rn(__ull2double_rn(u), 18446744073709551616.0);
+    if (r >= 1.0) r = 0x1.fffffffffffffp-1;
+    return __dadd_rn(__dmul_rn(r, 1.0), -0.5);
+}
+
+// D[k] = U(draw 2k) + U(draw 2k+1) for k < n: the dither added to sample k (frame-major, channel-minor)
+__global__ void __launch_bounds__(320) k_dither(unsigned long long seed, long long n, double* __restrict__ D) {
+    __shared__ unsigned long long st[kMtN];
+    const int t = threadIdx.x;
+    if (t == 0) {  // seeding is a sequential recurrence
+        st[0] = seed;
+        for (int i = 1; i < kMtN; i++) st[i] = 6364136223846793005ULL * (st[i - 1] ^ (st[i - 1] >> 62)) + i;
+    }
+    __syncthreads();
+    for (long long base = 0; base < n; base += kMtN / 2) {
+        unsigned long long a = 0, b = 0;
+        if (t < kMtN) {
+            a = st[t];
+            if (t + 1 < kMtN) b = st[t + 1];
+        }
+        __syncthreads();
+        if (t < kMtN - kMtM) {  // words 0..155 read only words not yet updated
+            const unsigned long long x = (a & kMtUpper) | (b & kMtLower);
+            st[t] = st[t + kMtM] ^ (x >> 1) ^ ((x & 1) ? kMtA : 0ULL);
+        }
+        __syncthreads();
+        if (t >= kMtN - kMtM && t < kMtN) {  // words 156..311 read the updated words t-156 (and 0 for the last)
+            if (t == kMtN - 1) b = st[0];
+            const unsigned long long x = (a & kMtUpper) | (b & kMtLower);
+            st[t] = st[t - (kMtN - kMtM)] ^ (x >> 1) ^ ((x & 1) ? kMtA : 0ULL);
+        }
+        __syncthreads();
+        if (t < kMtN / 2 && base + t < n)
+            D[base + t] = __dadd_rn(mt_uniform(mt_temper(st[2 * t])), mt_uniform(mt_temper(st[2 * t + 1])));
+    }
+}
+
+// Interleaved little-endian WAV data of planar samples y (ch x frames, row stride `stride`)
+template <int FMT>  // 0 f64, 1 f32, 2 s32, 3 s24, 4 s16
+__global__ void k_pack(const double* __restrict__ y, int ch, long long frames, long long stride,
+                       const double* __restrict__ D, unsigned char* __restrict__ out,
+                       unsigned long long* __restrict__ clipped) {
+    constexpr int B = FMT == 0 ? 8 : FMT == 1 ? 4 : FMT == 2 ? 4 : FMT == 3 ? 3 : 2;
+    constexpr double sc = FMT == 4 ? 32768.0 : FMT == 3 ? 8388608.0 : 2147483648.0;
+    const long long n = frames * ch;
+    unsigned long long clip = 0;
+    for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < n; s += (long long)gridDim.x * blockDim.x) {
+        const long long i = s / ch;
+        const int c = (int)(s - i * ch);
+        const double x = y[c * stride + i];
+        unsigned char* p = out + s * B;
+        if constexpr (FMT == 0) {
+            const unsigned long long bits = __double_as_longlong(x);
+#pragma unroll
+            for (int k = 0; k < 8; k++) p[k] = (unsigned char)(bits >> (8 * k));
+        } else if constexpr (FMT == 1) {
+            const unsigned int bits = __float_as_uint(__double2float_rn(x));
+#pragma unroll
+            for (int k = 0; k < 4; k++) p[k] = (unsigned char)(bits >> (8 * k));
+        } else {
+            double v = __dmul_rn(x, sc);
+            if (D) v = __dadd_rn(v, D[s]);
+            v = rint(v);
+            if (v > sc - 1) {
+                v = sc - 1;
+                clip++;
+            } else if (v < -sc) {
+                v = -sc;
+                clip++;
+            }
+            const long long iv = isnan(v) ? 0 : (long long)v;  // NaN is written as zero
+#pragma unroll
+            for (int k = 0; k < B; k++) p[k] = (unsigned char)((iv >> (8 * k)) & 255);
+        }
+    }
+    if (FMT >= 2) {
+        for (int o = 16; o > 0; o >>= 1) clip += __shfl_down_sync(0xffffffffu, clip, o);
+        if ((threadIdx.x & 31) == 0 && clip) atomicAdd(clipped, clip);
+    }
+}
+
+int format_bytes(int format) { return format == 0 ? 8 : format == 1 ? 4 : format == 2 ? 4 : format == 3 ? 3 : 2; }
+
+// Packs planar device samples into device WAV data; D: device dither values (nullptr: none).
+int enqueue_pack(const double* y, int ch, long long frames, long long stride, int format, const double* D,
+                 unsigned char* out, unsigned long long* clipped, cudaStream_t st) {
+    const long long n = frames * ch;
+    if (n == 0) return KBSRC_GPU_OK;
+    const unsigned g = grid_for(n, 256);
+    switch (format) {
+        case 0: k_pack<0><<<g, 256, 0, st>>>(y, ch, frames, stride, nullptr, out, clipped); break;
+        case 1: k_pack<1><<<g, 256, 0, st>>>(y, ch, frames, stride, nullptr, out, clipped); break;
+        case 2: k_pack<2><<<g, 256, 0, st>>>(y, ch, frames, stride, D, out, clipped); break;
+        case 3: k_pack<3><<<g, 256, 0, st>>>(y, ch, frames, stride, D, out, clipped); break;
+        case 4: k_pack<4><<<g, 256, 0, st>>>(y, ch, frames, stride, D, out, clipped); break;
+        default: return fail(KBSRC_GPU_E_ARG, "unknown sample format");
+    }
+    KB_CUDA(cudaGetLastError());
+    return KBSRC_GPU_OK;
+}
+
+}  // namespace
+
 // ---- batches: many conversions, grouped by plan -------------------------------------------------------------
 namespace {
 
@@ -1432,6 +1559,81 @@ int kbsrc_gpu_engine_run_host(kbsrc_gpu_engine* e, const double* in, const doubl
         if (rc) return rc;
         if (no) KB_CUDA(cudaMemcpyAsync(out, e->d_out.p, no * 8, cudaMemcpyDeviceToHost, st));
         KB_CUDA(cudaStreamSynchronize(st));
+        return KBSRC_GPU_OK;
+    } catch (const std::exception& x) {
+        return fail(KBSRC_GPU_E_CUDA, x.what());
+    }
+}
+
+int kbsrc_gpu_engine_run_host_packed(kbsrc_gpu_engine* e, const double* in, const double* head,
+                                     const double* tail, int format, int dither, unsigned char* out_bytes,
+                                     long long* clipped) {
+    if (!e) return fail(KBSRC_GPU_E_ARG, "null engine");
+    const kbsrc_gpu_desc& d = e->d;
+    if (format < 0 || format > 4) return fail(KBSRC_GPU_E_ARG, "unknown sample format");
+    if ((d.frames > 0 && !in) || (d.nout > 0 && !out_bytes) || (d.edge_len > 0 && (!head || !tail)))
+        return fail(KBSRC_GPU_E_ARG, "null buffer");
+    try {
+        int rc;
+        const size_t nin = (size_t)d.frames * d.channels, ne = (size_t)d.edge_len * d.channels,
+                     no = (size_t)d.nout * d.channels, nb = no * format_bytes(format);
+        if (!e->d_in.p && (rc = e->d_in.alloc(nin * 8)) != KBSRC_GPU_OK) return rc;
+        if (!e->d_head.p && (rc = e->d_head.alloc(ne * 8)) != KBSRC_GPU_OK) return rc;
+        if (!e->d_tail.p && (rc = e->d_tail.alloc(ne * 8)) != KBSRC_GPU_OK) return rc;
+        if (!e->d_out.p && (rc = e->d_out.alloc(no * 8)) != KBSRC_GPU_OK) return rc;
+        DevBuf bytes, dith, cnt;
+        if ((rc = bytes.alloc(nb)) != KBSRC_GPU_OK || (rc = cnt.alloc(8)) != KBSRC_GPU_OK) return rc;
+        const bool use_dither = dither && format >= 2 && no > 0;
+        if (use_dither && (rc = dith.alloc(no * 8)) != KBSRC_GPU_OK) return rc;
+        cudaStream_t st = e->stream;
+        KB_CUDA(cudaMemsetAsync(cnt.p, 0, 8, st));
+        if (use_dither) k_dither<<<1, 320, 0, st>>>(12345ULL, (long long)no, static_cast<double*>(dith.p));
+        if (nin) KB_CUDA(cudaMemcpyAsync(e->d_in.p, in, nin * 8, cudaMemcpyHostToDevice, st));
+        if (ne) {
+            KB_CUDA(cudaMemcpyAsync(e->d_head.p, head, ne * 8, cudaMemcpyHostToDevice, st));
+            KB_CUDA(cudaMemcpyAsync(e->d_tail.p, tail, ne * 8, cudaMemcpyHostToDevice, st));
+        }
+        rc = run_device_impl(e, (const double*)e->d_in.p, (const double*)e->d_head.p, (const double*)e->d_tail.p,
+                             (double*)e->d_out.p, st);
+        if (rc) return rc;
+        if ((rc = enqueue_pack((const double*)e->d_out.p, d.channels, d.nout, d.nout, format,
+                               use_dither ? (const double*)dith.p : nullptr, (unsigned char*)bytes.p,
+                               (unsigned long long*)cnt.p, st)) != KBSRC_GPU_OK)
+            return rc;
+        unsigned long long c = 0;
+        if (nb) KB_CUDA(cudaMemcpyAsync(out_bytes, bytes.p, nb, cudaMemcpyDeviceToHost, st));
+        KB_CUDA(cudaMemcpyAsync(&c, cnt.p, 8, cudaMemcpyDeviceToHost, st));
+        KB_CUDA(cudaStreamSynchronize(st));
+        if (clipped) *clipped = (long long)c;
+        return KBSRC_GPU_OK;
+    } catch (const std::exception& x) {
+        return fail(KBSRC_GPU_E_CUDA, x.what());
+    }
+}
+
+int kbsrc_gpu_pack(const double* d_planar, int channels, long long frames, long long stride, int format, int dither,
+                   unsigned char* d_out, long long* clipped, void* stream) {
+    if ((!d_planar || !d_out) && frames > 0) return fail(KBSRC_GPU_E_ARG, "null buffer");
+    if (channels < 1 || frames < 0 || stride < frames || format < 0 || format > 4)
+        return fail(KBSRC_GPU_E_ARG, "bad pack arguments");
+    try {
+        const long long n = frames * channels;
+        cudaStream_t st = static_cast<cudaStream_t>(stream);
+        int rc;
+        DevBuf dith, cnt;
+        if ((rc = cnt.alloc(8)) != KBSRC_GPU_OK) return rc;
+        const bool use_dither = dither && format >= 2 && n > 0;
+        if (use_dither && (rc = dith.alloc((size_t)n * 8)) != KBSRC_GPU_OK) return rc;
+        KB_CUDA(cudaMemsetAsync(cnt.p, 0, 8, st));
+        if (use_dither) k_dither<<<1, 320, 0, st>>>(12345ULL, n, static_cast<double*>(dith.p));
+        if ((rc = enqueue_pack(d_planar, channels, frames, stride, format,
+                               use_dither ? (const double*)dith.p : nullptr, d_out, (unsigned long long*)cnt.p, st)) !=
+            KBSRC_GPU_OK)
+            return rc;
+        unsigned long long c = 0;
+        KB_CUDA(cudaMemcpyAsync(&c, cnt.p, 8, cudaMemcpyDeviceToHost, st));
+        KB_CUDA(cudaStreamSynchronize(st));  // the temporaries are freed on return
+        if (clipped) *clipped = (long long)c;
         return KBSRC_GPU_OK;
     } catch (const std::exception& x) {
         return fail(KBSRC_GPU_E_CUDA, x.what());

@@ -109,12 +109,22 @@ int run(int argc, char** argv) {
     kbsrc::io::check_wav_output(a.ch, rate, format);  // fail before converting
     const double t1 = now();
     kbsrc::Stats st;
-    auto y = kbsrc::resample(a.d.data(), a.frames, a.ch, a.rate, rate, opt, &st);
-    const double t2 = now();
-    const long long nout = y.empty() ? 0 : (long long)y[0].size();
-    long long clipped = 0;
-    kbsrc::io::write_wav(out_path.c_str(), y, a.ch, nout, rate, format, dither, clipped);
-    const double t3 = now();
+    long long clipped = 0, nout = 0;
+    double t2, t3;
+    if (a.rate == rate) {  // equal rates: the host copy and the host writer
+        auto y = kbsrc::resample(a.d.data(), a.frames, a.ch, a.rate, rate, opt, &st);
+        t2 = now();
+        nout = y.empty() ? 0 : (long long)y[0].size();
+        kbsrc::io::write_wav(out_path.c_str(), y, a.ch, nout, rate, format, dither, clipped);
+    } else {  // the conversion and the output step (interleave, scale, dither, round, clip) on the GPU
+        const auto data = kbsrc::resample_wav_data(a.d.data(), a.frames, a.ch, a.rate, rate, format.c_str(), dither,
+                                                   clipped, opt, &st);
+        t2 = now();
+        const long long bps = format == "f64" ? 8 : format == "s24" ? 3 : format == "s16" ? 2 : 4;
+        nout = (long long)data.size() / (a.ch * bps);
+        kbsrc::io::write_wav_data(out_path.c_str(), a.ch, nout, rate, format, data.data(), data.size());
+    }
+    t3 = now();
     if (clipped) std::fprintf(stderr, "kbsrc: warning: %lld samples clipped\n", clipped);
     if (verbose) {
         std::fprintf(stderr, "%d Hz -> %d Hz, %d ch, %lld -> %lld frames\n", a.rate, rate, a.ch, a.frames, nout);

@@ -444,6 +444,25 @@ std::vector<std::vector<double>> resample(const double* in, long long frames, in
     return resample_gpu(in, frames, channels, rate_in, rate_out, opt, stats);
 }
 
+std::vector<unsigned char> resample_wav_data(const double* in, long long frames, int channels, int rate_in,
+                                             int rate_out, const char* format, bool dither, long long& clipped,
+                                             const Options& opt, Stats* stats) {
+    const std::string f = format ? format : "";
+    const int fmt = f == "f64" ? 0 : f == "f32" ? 1 : f == "s32" ? 2 : f == "s24" ? 3 : f == "s16" ? 4 : -1;
+    if (fmt < 0) throw std::invalid_argument("format must be f64, f32, s32, s24 or s16");
+    RoundToNearest rn(opt.precision == Precision::Exact);
+    auto cv = prepare(in, frames, channels, rate_in, rate_out, opt);
+    if (cv->pl.copy) throw std::invalid_argument("equal rates: nothing to convert");
+    const double t1 = now();
+    const int bps = fmt == 0 ? 8 : fmt == 3 ? 3 : fmt == 4 ? 2 : 4;
+    std::vector<unsigned char> data((size_t)(cv->pl.nout * channels * bps));
+    gpu_check(kbsrc_gpu_engine_run_host_packed(cv->eng.e, in, cv->head.data(), cv->tail.data(), fmt, dither ? 1 : 0,
+                                               data.data(), &clipped),
+              "GPU engine");
+    fill_stats(*cv, stats, now() - t1);
+    return data;
+}
+
 const char* version() { return KBSRC_VERSION; }
 
 }  // namespace kbsrc

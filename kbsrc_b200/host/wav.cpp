@@ -127,14 +127,15 @@ void check_wav_output(int ch, int rate, const std::string& fmt) {
     if (rate < 1 || rate * frame > 0xFFFFFFFFLL) fail("sample rate too high for a WAV file with this many channels");
 }
 
-void write_wav(const char* path, const std::vector<std::vector<double>>& y, int ch, long long frames, int rate,
-               const std::string& fmt, bool dither, long long& clipped) {
+namespace {
+// The RIFF/WAVE header for `frames` frames of `ch` channels in `fmt` (reference wav.cpp:355-371)
+std::vector<uint8_t> wav_header(int ch, long long frames, int rate, const std::string& fmt, size_t& data_bytes) {
     check_wav_output(ch, rate, fmt);
     const bool is_float = fmt == "f64" || fmt == "f32";
     const int bits = fmt == "f64" ? 64 : fmt == "f32" ? 32 : fmt == "s32" ? 32 : fmt == "s24" ? 24 : 16;
     const int bps = bits / 8, align = ch * bps;
     if (frames < 0 || frames > (0xFFFFFFFFLL - 80) / align) fail("output too large for WAV (4 GB limit)");
-    const size_t data_bytes = (size_t)frames * align;
+    data_bytes = (size_t)frames * align;
     std::vector<uint8_t> hdr;
     auto put16 = [&](unsigned v) { hdr.push_back(v & 255); hdr.push_back(v >> 8 & 255); };
     auto put32 = [&](uint32_t v) { put16(v & 0xFFFF); put16(v >> 16); };
@@ -156,6 +157,16 @@ void write_wav(const char* path, const std::vector<std::vector<double>>& y, int 
     }
     if (is_float) { tag("fact"); put32(4); put32((uint32_t)frames); }
     tag("data"); put32((uint32_t)data_bytes);
+    return hdr;
+}
+}  // namespace
+
+void write_wav(const char* path, const std::vector<std::vector<double>>& y, int ch, long long frames, int rate,
+               const std::string& fmt, bool dither, long long& clipped) {
+    size_t data_bytes = 0;
+    const std::vector<uint8_t> hdr = wav_header(ch, frames, rate, fmt, data_bytes);
+    const int bps = fmt == "f64" ? 8 : fmt == "f32" ? 4 : fmt == "s32" ? 4 : fmt == "s24" ? 3 : 2;
+    const int align = ch * bps;
     FileCloser fc{std::fopen(path, "wb")};
     FILE* f = fc.f;
     if (!f) fail("cannot open output");
@@ -190,6 +201,21 @@ void write_wav(const char* path, const std::vector<std::vector<double>>& y, int 
         const size_t nb = (size_t)(p - buf.data());
         if (std::fwrite(buf.data(), 1, nb, f) != nb) fail("write error");
     }
+    if (data_bytes & 1) std::fputc(0, f);
+    fc.f = nullptr;
+    if (std::fclose(f)) fail("write error");
+}
+
+void write_wav_data(const char* path, int ch, long long frames, int rate, const std::string& fmt,
+                    const unsigned char* data, size_t bytes) {
+    size_t data_bytes = 0;
+    const std::vector<uint8_t> hdr = wav_header(ch, frames, rate, fmt, data_bytes);
+    if (bytes != data_bytes) fail("internal error: WAV data size");
+    FileCloser fc{std::fopen(path, "wb")};
+    FILE* f = fc.f;
+    if (!f) fail("cannot open output");
+    if (std::fwrite(hdr.data(), 1, hdr.size(), f) != hdr.size()) fail("write error");
+    if (bytes && std::fwrite(data, 1, bytes, f) != bytes) fail("write error");
     if (data_bytes & 1) std::fputc(0, f);
     fc.f = nullptr;
     if (std::fclose(f)) fail("write error");

@@ -24,4 +24,9 @@ void check_wav_output(int ch, int rate, const std::string& format);
 void write_wav(const char* path, const std::vector<std::vector<double>>& y, int ch, long long frames, int rate,
                const std::string& format, bool dither, long long& clipped);
 
+// Writes a WAV file of `frames` frames whose data section (interleaved samples in `format`) was produced
+// elsewhere (the GPU packer); the header is the one write_wav produces.
+void write_wav_data(const char* path, int ch, long long frames, int rate, const std::string& format,
+                    const unsigned char* data, size_t bytes);
+
 }  // namespace kbsrc::io

@@ -92,3 +92,25 @@ def test_cli_bytes_equal_reference_cli(tmp_path, args):
     rb = cli(*args, src, b, binary=oracle.REF_CLI)
     assert ra.returncode == rb.returncode == 0, (ra.stderr, rb.stderr)
     assert a.read_bytes() == b.read_bytes()
+
+
+@pytest.mark.skipif(not os.path.exists(oracle.REF_CLI), reason="reference CLI not built (oracle/_ref)")
+@pytest.mark.parametrize("fmt", ["s16", "s24", "s32", "f32", "f64"])
+@pytest.mark.parametrize("dither", [False, True])
+def test_gpu_pack_equals_reference_writer(tmp_path, fmt, dither):
+    """The GPU output step against the reference's writer: equal rates make the reference CLI write the input
+    samples themselves, so its data section is the packing of exactly these samples (values beyond +-1 clip)."""
+    x = np.random.default_rng(4).uniform(-1.2, 1.2, (7001, 3))
+    x[5, 1] = np.nan
+    src = tmp_path / "in.wav"
+    from test_host import wav
+    src.write_bytes(wav(3, 3, 48000, 64, 24, x.astype("<f8").tobytes()))
+    ref = tmp_path / "ref.wav"
+    r = subprocess.run([oracle.REF_CLI, str(src), str(ref), "--rate", "48000", "--format", fmt] +
+                       (["--dither"] if dither else []), capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    _, want = read_wav_samples(ref)
+    got, clipped = kbsrc_b200.pack(x.T, fmt, dither)
+    assert got == want
+    m = re.search(r"warning: (\d+) samples clipped", r.stderr)
+    assert clipped == (int(m.group(1)) if m else 0)
