@@ -794,11 +794,17 @@ struct kbsrc_gpu_engine : PlanCore {
     int device = 0;
     long long tasks = 0, wave = 0, stride = 0, launches = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t copy_in = nullptr, copy_out = nullptr;  // run_host's copy pipeline
+    cudaEvent_t ev_in[2] = {}, ev_done[2] = {};
     DevBuf bufA, bufB;
     DevBuf d_in, d_head, d_tail, d_out;
     std::vector<cudaEvent_t> events;  // per-pass timing trail, created on first use
     ~kbsrc_gpu_engine() {
         for (cudaEvent_t x : events) cudaEventDestroy(x);
+        for (cudaEvent_t x : {ev_in[0], ev_in[1], ev_done[0], ev_done[1]})
+            if (x) cudaEventDestroy(x);
+        if (copy_in) cudaStreamDestroy(copy_in);
+        if (copy_out) cudaStreamDestroy(copy_out);
         if (stream) cudaStreamDestroy(stream);
     }
 };
@@ -1003,11 +1009,11 @@ int bluestein_kernel(DevCfft& d, bool dd_tables, cudaStream_t st) {
     return KBSRC_GPU_OK;
 }
 
-// Enqueues the block loop of `tasks` tasks of one plan, wave by wave through the slot buffers a, b.
+// Enqueues the block loop of tasks [t_begin, t_end) of one plan, wave by wave through the slot buffers a, b.
 // ArL: four-step sub-FFT arithmetic, ArS: everything else.
 template <class ArL, class ArS>
-int enqueue_plan(const PlanCore& pc, const Work& work, long long tasks, void* a, void* b, long long stride,
-                 long long wave, cudaStream_t st, Trail& tr) {
+int enqueue_plan(const PlanCore& pc, const Work& work, long long t_begin, long long t_end, void* a, void* b,
+                 long long stride, long long wave, cudaStream_t st, Trail& tr) {
     static_assert(sizeof(CxR<ArL>) == sizeof(CxR<ArS>), "one element size per mode");
     using CS = CxR<ArS>;
     using WS = typename ArS::W;
@@ -1017,9 +1023,9 @@ int enqueue_plan(const PlanCore& pc, const Work& work, long long tasks, void* a,
     sl.work = work;
     void* buf[2] = {a, b};
     int rc;
-    for (long long t0 = 0; t0 < tasks; t0 += wave) {
+    for (long long t0 = t_begin; t0 < t_end; t0 += wave) {
         sl.task0 = t0;
-        sl.nt = (unsigned)std::min(wave, tasks - t0);
+        sl.nt = (unsigned)std::min(wave, t_end - t0);
         // forward real FFT: gather + complex FFT; the spectrum Z lands in buf[z]
         int z;
         if (pc.fw.m) {
@@ -1054,10 +1060,10 @@ int enqueue_plan(const PlanCore& pc, const Work& work, long long tasks, void* a,
     return KBSRC_GPU_OK;
 }
 
-int enqueue_any(const PlanCore& pc, const Work& work, long long tasks, void* a, void* b, long long stride,
-                long long wave, cudaStream_t st, Trail& tr) {
-    if (pc.exact) return enqueue_plan<ArDDShort, ArDDAccurate>(pc, work, tasks, a, b, stride, wave, st, tr);
-    return enqueue_plan<ArF64, ArF64>(pc, work, tasks, a, b, stride, wave, st, tr);
+int enqueue_any(const PlanCore& pc, const Work& work, long long t_begin, long long t_end, void* a, void* b,
+                long long stride, long long wave, cudaStream_t st, Trail& tr) {
+    if (pc.exact) return enqueue_plan<ArDDShort, ArDDAccurate>(pc, work, t_begin, t_end, a, b, stride, wave, st, tr);
+    return enqueue_plan<ArF64, ArF64>(pc, work, t_begin, t_end, a, b, stride, wave, st, tr);
 }
 
 Work single_work(const PlanCore& pc, const double* in, const double* head, const double* tail, double* out) {
@@ -1163,8 +1169,8 @@ int run_device_impl(kbsrc_gpu_engine* e, const double* in, const double* head, c
     Trail& tr = trail ? *trail : none;
     int rc;
     if ((rc = tr.mark(st, -1)) != KBSRC_GPU_OK) return rc;
-    rc = enqueue_any(*e, single_work(*e, in, head, tail, out), e->tasks, e->bufA.p, e->bufB.p, e->stride, e->wave,
-                     st, tr);
+    rc = enqueue_any(*e, single_work(*e, in, head, tail, out), 0, e->tasks, e->bufA.p, e->bufB.p, e->stride,
+                     e->wave, st, tr);
     if (rc) return rc;
     e->launches = tr.launches;
     KB_CUDA(cudaGetLastError());
@@ -1303,6 +1309,13 @@ int enqueue_pack(const double* y, int ch, long long frames, long long stride, in
 
 }  // namespace
 
+// Chunks of blocks for run_host's copy pipeline: about 16, none smaller than a wave's worth of full-GPU work
+// (KBSRC_GPU_CHUNKS overrides).
+long long nout_chunks(const kbsrc_gpu_engine* e, long long nblk) {
+    const long long want = env_int("KBSRC_GPU_CHUNKS", 16);
+    return std::max(1LL, std::min(want, nblk));
+}
+
 // ---- batches: many conversions, grouped by plan -------------------------------------------------------------
 namespace {
 
@@ -1398,7 +1411,8 @@ int batch_enqueue(kbsrc_gpu_batch& b, cudaStream_t st, Trail& tr) {
         w.hopQ = (long long)g.hop * g.d.Q;
         w.hopP = (long long)g.hop * g.d.P;
         w.margP = (long long)g.d.marg * g.d.P;
-        if ((rc = enqueue_any(g, w, g.tasks, b.bufA.p, b.bufB.p, g.stride, g.wave, st, tr)) != KBSRC_GPU_OK) return rc;
+        if ((rc = enqueue_any(g, w, 0, g.tasks, b.bufA.p, b.bufB.p, g.stride, g.wave, st, tr)) != KBSRC_GPU_OK)
+            return rc;
     }
     KB_CUDA(cudaGetLastError());
     return KBSRC_GPU_OK;
@@ -1548,17 +1562,61 @@ int kbsrc_gpu_engine_run_host(kbsrc_gpu_engine* e, const double* in, const doubl
         if (!e->d_head.p && (rc = e->d_head.alloc(ne * 8)) != KBSRC_GPU_OK) return rc;
         if (!e->d_tail.p && (rc = e->d_tail.alloc(ne * 8)) != KBSRC_GPU_OK) return rc;
         if (!e->d_out.p && (rc = e->d_out.alloc(no * 8)) != KBSRC_GPU_OK) return rc;
-        cudaStream_t st = e->stream;
-        if (nin) KB_CUDA(cudaMemcpyAsync(e->d_in.p, in, nin * 8, cudaMemcpyHostToDevice, st));
-        if (ne) {
-            KB_CUDA(cudaMemcpyAsync(e->d_head.p, head, ne * 8, cudaMemcpyHostToDevice, st));
-            KB_CUDA(cudaMemcpyAsync(e->d_tail.p, tail, ne * 8, cudaMemcpyHostToDevice, st));
+        if (!e->copy_in) {
+            KB_CUDA(cudaStreamCreateWithFlags(&e->copy_in, cudaStreamNonBlocking));
+            KB_CUDA(cudaStreamCreateWithFlags(&e->copy_out, cudaStreamNonBlocking));
+            for (int k = 0; k < 2; k++) {
+                KB_CUDA(cudaEventCreateWithFlags(&e->ev_in[k], cudaEventDisableTiming));
+                KB_CUDA(cudaEventCreateWithFlags(&e->ev_done[k], cudaEventDisableTiming));
+            }
         }
-        rc = run_device_impl(e, (const double*)e->d_in.p, (const double*)e->d_head.p, (const double*)e->d_tail.p,
-                             (double*)e->d_out.p, st);
-        if (rc) return rc;
-        if (no) KB_CUDA(cudaMemcpyAsync(out, e->d_out.p, no * 8, cudaMemcpyDeviceToHost, st));
-        KB_CUDA(cudaStreamSynchronize(st));
+        // Pipeline by chunks of blocks: the input frames a chunk reads go up while the previous chunk computes,
+        // and its output goes down while the next one computes. Tasks are block-major, so a chunk of blocks is a
+        // contiguous task range; every frame is copied once, in order.
+        if (e->tasks == 0 || d.nout == 0) return KBSRC_GPU_OK;
+        cudaStream_t cs = e->stream, hs = e->copy_in, ds = e->copy_out;
+        const double* dinp = (const double*)e->d_in.p;
+        double* dout = (double*)e->d_out.p;
+        KB_CUDA(cudaMemsetAsync(dout, 0, no * 8, cs));
+        if (ne) {
+            KB_CUDA(cudaMemcpyAsync(e->d_head.p, head, ne * 8, cudaMemcpyHostToDevice, hs));
+            KB_CUDA(cudaMemcpyAsync(e->d_tail.p, tail, ne * 8, cudaMemcpyHostToDevice, hs));
+        }
+        const long long nblk = d.nblk, ch = d.channels, hopQ = (long long)e->hop * d.Q, hopP = (long long)e->hop * d.P;
+        const long long chunks = nout_chunks(e, nblk);
+        const Work w = single_work(*e, dinp, (const double*)e->d_head.p, (const double*)e->d_tail.p, dout);
+        long long copied = 0;  // frames already sent
+        Trail tr;
+        for (long long k = 0; k < chunks; k++) {
+            const long long b0 = nblk * k / chunks, b1 = nblk * (k + 1) / chunks;
+            if (b0 == b1) continue;
+            const long long f_hi = std::min(d.frames, std::max(0LL, (b1 - 1) * hopQ + e->Nb - d.lead));
+            if (f_hi > copied) {
+                KB_CUDA(cudaMemcpyAsync(e->d_in.p ? (double*)e->d_in.p + copied * ch : nullptr, in + copied * ch,
+                                        (size_t)((f_hi - copied) * ch * 8), cudaMemcpyHostToDevice, hs));
+                copied = f_hi;
+            }
+            KB_CUDA(cudaEventRecord(e->ev_in[k % 2], hs));
+            KB_CUDA(cudaStreamWaitEvent(cs, e->ev_in[k % 2], 0));
+            if ((rc = enqueue_any(*e, w, b0 * ch, b1 * ch, e->bufA.p, e->bufB.p, e->stride, e->wave, cs, tr)) !=
+                KBSRC_GPU_OK)
+                return rc;
+            KB_CUDA(cudaEventRecord(e->ev_done[k % 2], cs));
+            KB_CUDA(cudaStreamWaitEvent(ds, e->ev_done[k % 2], 0));
+            const long long o0 = std::max(0LL, b0 * hopP - d.o), o1 = k == chunks - 1 ? d.nout
+                                                                                    : std::min(d.nout, b1 * hopP - d.o);
+            if (o1 > o0)
+                KB_CUDA(cudaMemcpy2DAsync(out + o0, (size_t)d.nout * 8, dout + o0, (size_t)d.nout * 8,
+                                          (size_t)(o1 - o0) * 8, (size_t)ch, cudaMemcpyDeviceToHost, ds));
+        }
+        if (copied < d.frames && nin)  // frames no block reads (none in a valid plan)
+            KB_CUDA(cudaMemcpyAsync((double*)e->d_in.p + copied * ch, in + copied * ch,
+                                    (size_t)((d.frames - copied) * ch * 8), cudaMemcpyHostToDevice, hs));
+        e->launches = tr.launches;
+        KB_CUDA(cudaGetLastError());
+        KB_CUDA(cudaStreamSynchronize(hs));
+        KB_CUDA(cudaStreamSynchronize(cs));
+        KB_CUDA(cudaStreamSynchronize(ds));
         return KBSRC_GPU_OK;
     } catch (const std::exception& x) {
         return fail(KBSRC_GPU_E_CUDA, x.what());
