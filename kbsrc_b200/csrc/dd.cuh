@@ -7,13 +7,20 @@
 #pragma once
 #include <cuda_runtime.h>
 
-// Occupancy targets of the shared-memory passes (256-thread CTAs per SM): they cap registers at 64K/(256*n).
-// Double-double butterflies need about 128 registers (2 CTAs); f64 ones fit 3.
+// Launch shapes the shared-memory passes are compiled for: at most KB_MAXT_* threads per CTA and KB_MINB_*
+// resident CTAs per SM, which caps registers at 64K / (threads * CTAs). Double-double: 192 x 3 (96 registers,
+// 18 warps per SM, measured fastest); f64: 256 x 3 (80 registers).
 #ifndef KB_MINB_DD
-#define KB_MINB_DD 2
+#define KB_MINB_DD 3
+#endif
+#ifndef KB_MAXT_DD
+#define KB_MAXT_DD 192
 #endif
 #ifndef KB_MINB_F64
 #define KB_MINB_F64 3
+#endif
+#ifndef KB_MAXT_F64
+#define KB_MAXT_F64 256
 #endif
 
 namespace kbsrc::dev {
@@ -79,7 +86,7 @@ struct ArF64 {  // Precision::Fast: float64 everywhere (V4 lanes and scalar alik
     using R = double;
     using W = double;
     static constexpr bool kLanes = true, kLaneRenorm = false, kDD = false;
-    static constexpr int kMinBlocks = KB_MINB_F64;  // resident 256-thread CTAs per SM the passes are built for
+    static constexpr int kMinBlocks = KB_MINB_F64, kMaxThreads = KB_MAXT_F64;
     static __device__ __forceinline__ R add(R a, R b) { return __dadd_rn(a, b); }
     static __device__ __forceinline__ R sub(R a, R b) { return __dsub_rn(a, b); }
     static __device__ __forceinline__ R mul(R a, R b) { return __dmul_rn(a, b); }
@@ -94,7 +101,7 @@ struct ArDDShort {  // four-step sub-FFTs of Precision::Exact (DD4 lanes)
     using R = dd;
     using W = dd;
     static constexpr bool kLanes = true, kLaneRenorm = true, kDD = true;
-    static constexpr int kMinBlocks = KB_MINB_DD;
+    static constexpr int kMinBlocks = KB_MINB_DD, kMaxThreads = KB_MAXT_DD;
     static __device__ __forceinline__ R add(R a, R b) { return add_short(a, b); }
     static __device__ __forceinline__ R sub(R a, R b) { return add_short(a, dd_neg(b)); }
     static __device__ __forceinline__ R mul(R a, R b) { return mul_dd(a, b); }
@@ -110,7 +117,7 @@ struct ArDDAccurate {  // scalar dd: direct SFFT, Bluestein, RFFT split/merge, s
     using R = dd;
     using W = dd;
     static constexpr bool kLanes = false, kLaneRenorm = false, kDD = true;
-    static constexpr int kMinBlocks = KB_MINB_DD;
+    static constexpr int kMinBlocks = KB_MINB_DD, kMaxThreads = KB_MAXT_DD;
     static __device__ __forceinline__ R add(R a, R b) { return add_accurate(a, b); }
     static __device__ __forceinline__ R sub(R a, R b) { return add_accurate(a, dd_neg(b)); }
     static __device__ __forceinline__ R mul(R a, R b) { return mul_dd(a, b); }

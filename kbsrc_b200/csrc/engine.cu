@@ -186,7 +186,7 @@ __device__ __forceinline__ CxW<Ar>* twiddle_smem(unsigned char* after_planes) {
 // Column pass: sequences n2 in [c0, c0+F) of length N1 (stride N2), twiddle, store in place
 // (fft.hpp:283-299). blockIdx.x: column group; blockIdx.y: task slot.
 template <class Ar, int SRC>
-__global__ void __launch_bounds__(256, Ar::kMinBlocks) k_column(const __grid_constant__ PassParams<Ar> P) {
+__global__ void __launch_bounds__(Ar::kMaxThreads, Ar::kMinBlocks) k_column(const __grid_constant__ PassParams<Ar> P) {
     extern __shared__ __align__(16) unsigned char smem[];
     using C = CxR<Ar>;
     const int F = P.F, N1 = P.N1, N2 = P.N2, total = N1 * F;
@@ -234,7 +234,7 @@ __global__ void __launch_bounds__(256, Ar::kMinBlocks) k_column(const __grid_con
 // Row pass: rows r in [r0, r0+F) of length N2 (contiguous), stored transposed to [N1*k2 + r]
 // (fft.hpp:300-311), or written straight to the output as real samples (fft.hpp:459-460).
 template <class Ar, int DST>
-__global__ void __launch_bounds__(256, Ar::kMinBlocks) k_row(const __grid_constant__ PassParams<Ar> P) {
+__global__ void __launch_bounds__(Ar::kMaxThreads, Ar::kMinBlocks) k_row(const __grid_constant__ PassParams<Ar> P) {
     extern __shared__ __align__(16) unsigned char smem[];
     using C = CxR<Ar>;
     const int F = P.F, N1 = P.N1, N2 = P.N2, total = N2 * F;
@@ -279,7 +279,7 @@ __global__ void __launch_bounds__(256, Ar::kMinBlocks) k_row(const __grid_consta
 
 // Whole FFT of n <= 2048 points in one CTA (the reference's direct SFFT path, fft.hpp:241-244,279).
 template <class Ar, int SRC, int DST>
-__global__ void __launch_bounds__(256, Ar::kMinBlocks) k_direct(const __grid_constant__ PassParams<Ar> P) {
+__global__ void __launch_bounds__(Ar::kMaxThreads, Ar::kMinBlocks) k_direct(const __grid_constant__ PassParams<Ar> P) {
     extern __shared__ __align__(16) unsigned char smem[];
     using C = CxR<Ar>;
     const int n = P.sp.n;
@@ -674,13 +674,13 @@ Shape pick_shape(const SubPlan& sp, int count, size_t esize, int fmax) {
         if (count % f == 0) { F = f; break; }
     }
     int T = ((max_bfly(sp) * F + 31) / 32) * 32;
-    T = std::max(64, std::min(env_int("KBSRC_GPU_THREADS", 256), T));
+    T = std::max(64, std::min(env_int("KBSRC_GPU_THREADS", esize == 32 ? KB_MAXT_DD : KB_MAXT_F64), T));
     return Shape{F, T, 2 * (size_t)sp.n * F * esize + tw};
 }
 
 Shape direct_shape(const SubPlan& sp, size_t esize) {
     int T = ((max_bfly(sp) + 31) / 32) * 32;
-    T = std::max(64, std::min(256, T));
+    T = std::max(64, std::min(env_int("KBSRC_GPU_THREADS", esize == 32 ? KB_MAXT_DD : KB_MAXT_F64), T));
     return Shape{1, T, 2 * (size_t)sp.n * esize + (esize == 32 ? (size_t)sp.twn * esize : 0)};
 }
 
@@ -1309,8 +1309,7 @@ int enqueue_pack(const double* y, int ch, long long frames, long long stride, in
 
 }  // namespace
 
-// Chunks of blocks for run_host's copy pipeline: about 16, none smaller than a wave's worth of full-GPU work
-// (KBSRC_GPU_CHUNKS overrides).
+// Chunks of blocks for run_host's copy pipeline: 16, at most one per block (KBSRC_GPU_CHUNKS overrides).
 long long nout_chunks(const kbsrc_gpu_engine* e, long long nblk) {
     const long long want = env_int("KBSRC_GPU_CHUNKS", 16);
     return std::max(1LL, std::min(want, nblk));
