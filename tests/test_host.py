@@ -161,3 +161,50 @@ def test_wav_writer_bytes_equal_reference_cli(tmp_path, fmt, dither):
     assert ra.returncode == rb.returncode == 0, (ra.stderr, rb.stderr)
     assert ra.stderr == rb.stderr  # the clipped-samples warning
     assert a.read_bytes() == b.read_bytes()
+
+
+def test_gpu_path_fails_loudly_without_a_device():
+    """No silent CPU fallback: with no usable CUDA device a conversion raises with the runtime's reason."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(RuntimeError, match="CUDA device"):
+        kbsrc_b200.resample(np.zeros((1000, 1)), 48000, 44100)
+    rc = kbsrc_b200.gpu_lib().kbsrc_gpu_kernel_spectrum(np.zeros(4).ctypes.data_as(kbsrc_b200._dp), 1, 8, 1.0,
+                                                        np.zeros(10).ctypes.data_as(kbsrc_b200._dp))
+    assert rc == kbsrc_b200.GPU_E_NODEVICE
+
+
+def test_c_abi_rejects_bad_descriptors():
+    d = kbsrc_b200.GpuDesc()
+    e = ctypes_void_p()
+    assert kbsrc_b200.gpu_lib().kbsrc_gpu_engine_create(None, e) == kbsrc_b200.GPU_E_ARG
+    d.precision, d.channels, d.P, d.Q, d.nb, d.marg = 7, 1, 1, 2, 10, 2
+    assert kbsrc_b200.gpu_lib().kbsrc_gpu_engine_create(d, e) == kbsrc_b200.GPU_E_ARG
+    assert "precision" in kbsrc_b200.gpu_error()
+    d.precision, d.nb = 1, 3  # odd block
+    assert kbsrc_b200.gpu_lib().kbsrc_gpu_engine_create(d, e) == kbsrc_b200.GPU_E_ARG
+
+
+def ctypes_void_p():
+    import ctypes
+    return ctypes.c_void_p()
+
+
+def test_two_rank_reference_bench_on_cpu():
+    """bench.py under torchrun with 2 gloo ranks: rank 0 alone runs the reference arm and prints one JSON line,
+    the other rank exits cleanly (the launch the driver uses for N > 1)."""
+    from oracle import oracle
+    if not oracle.ref_available():
+        pytest.skip("reference not built (oracle/_ref)")
+    import json
+    import sys
+    r = subprocess.run([sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
+                        "--master-addr", "127.0.0.1", "--master-port", "29517", os.path.join(ROOT, "bench.py"),
+                        "--impl", "reference", "--gpus", "2", "--workload", "c1_exact", "--steps", "1", "--warmup",
+                        "0"], capture_output=True, text=True, timeout=300, cwd=ROOT)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["value"] > 0 and d["n_gpus"] == 2
