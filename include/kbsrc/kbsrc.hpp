@@ -2,7 +2,7 @@
 //
 // Same API as HongYue1/KBSRC 1.3.0 include/kbsrc/kbsrc.hpp:8-45 (Precision, Options, Stats, resample,
 // version), so code written against the reference library builds unchanged. The block engine runs on the
-// GPU (sm_100a); its output is byte-identical to the reference CPU engines for Fast and Exact.
+// GPU (sm_100a); its output is byte-identical to the reference CPU engines in all three precisions.
 #pragma once
 
 #include <vector>
@@ -12,7 +12,7 @@ namespace kbsrc {
 enum class Precision {
     Fast,        // float64 pipeline
     Exact,       // double-double (~106-bit) pipeline
-    LongDouble,  // x87 80-bit in the reference; rejected here (the GPU has no 80-bit type)
+    LongDouble,  // x87 80-bit extended; the GPU emulates its arithmetic in integers, bit for bit
 };
 
 struct Options {

@@ -8,7 +8,7 @@ extern "C" {
 #endif
 
 typedef struct {
-    int precision; /* 0 fast, 1 exact (2 long double: rejected) */
+    int precision; /* 0 fast, 1 exact, 2 long double (x87 extended, emulated on the GPU) */
     double length; /* one-sided kernel length, seconds (reference default 0.2) */
     double beta;   /* Kaiser beta (default 40) */
     int threads;   /* host threads, 0 = automatic */

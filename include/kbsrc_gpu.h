@@ -28,6 +28,7 @@ extern "C" {
 
 #define KBSRC_GPU_FAST 0  /* float64 pipeline (reference Precision::Fast) */
 #define KBSRC_GPU_EXACT 1 /* double-double pipeline (reference Precision::Exact) */
+#define KBSRC_GPU_LD 2    /* x87 extended pipeline, emulated in integers (reference Precision::LongDouble) */
 
 typedef struct kbsrc_gpu_engine kbsrc_gpu_engine;
 
@@ -36,7 +37,7 @@ typedef struct kbsrc_gpu_engine kbsrc_gpu_engine;
  * `lead` zeros/edge samples before input frame 0 (lead = marg*Q + pre), and writes output samples
  * [b*hop*P - o, (b+1)*hop*P - o) clipped to [0, nout). */
 typedef struct {
-    int precision;      /* KBSRC_GPU_FAST or KBSRC_GPU_EXACT */
+    int precision;      /* KBSRC_GPU_FAST, KBSRC_GPU_EXACT or KBSRC_GPU_LD */
     int channels;       /* >= 1 */
     long long P, Q;     /* reduced rate ratio rate_out/rate_in = P/Q */
     int nb;             /* block size factor: forward FFT nb*Q points, inverse nb*P */

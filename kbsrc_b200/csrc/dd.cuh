@@ -1,4 +1,5 @@
-// Device arithmetic for the block engine: float64 and double-double in the three flavours KBSRC uses.
+// Device arithmetic for the block engine: float64, double-double in the two flavours KBSRC uses, and x87
+// extended (x80.cuh) for Precision::LongDouble.
 //
 // Output must be byte-identical to the reference CPU engines, so every value is produced by the same IEEE
 // operations in the same order (HongYue1/KBSRC src/dsp/double_double.hpp:59-79, src/dsp/simd.hpp:44-66).
@@ -7,14 +8,23 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include "x80.cuh"
+
 // Launch shapes the shared-memory passes are compiled for: at most KB_MAXT_* threads per CTA and KB_MINB_*
 // resident CTAs per SM, which caps registers at 64K / (threads * CTAs). Double-double: 192 x 3 (96 registers,
-// 18 warps per SM, measured fastest); f64: 256 x 3 (80 registers).
+// 18 warps per SM, measured fastest); f64: 256 x 3 (80 registers); x87 extended: 192 x 2 (170 registers: the
+// integer emulation holds 128-bit intermediates).
 #ifndef KB_MINB_DD
 #define KB_MINB_DD 3
 #endif
 #ifndef KB_MAXT_DD
 #define KB_MAXT_DD 192
+#endif
+#ifndef KB_MINB_X80
+#define KB_MINB_X80 2
+#endif
+#ifndef KB_MAXT_X80
+#define KB_MAXT_X80 192
 #endif
 #ifndef KB_MINB_F64
 #define KB_MINB_F64 3
@@ -52,6 +62,7 @@ __device__ __forceinline__ dd dd_neg(dd a) { return dd{-a.hi, -a.lo}; }
 // negation of a table value (exact, both parts)
 __device__ __forceinline__ double w_neg(double a) { return -a; }
 __device__ __forceinline__ dd w_neg(dd a) { return dd_neg(a); }
+__device__ __forceinline__ x80 w_neg(x80 a) { return x80_neg(a); }
 
 // Accurate sum of the scalar dd type (double_double.hpp:67-70): two two-sums and two renormalisations.
 __device__ __forceinline__ dd add_accurate(dd a, dd b) {
@@ -81,11 +92,13 @@ __device__ __forceinline__ dd mul_dd(dd a, dd b) {
 // Arithmetic flavours. R: register type, W: table (twiddle / kernel) type.
 // kLanes: used by the reference's 4-lane four-step, whose twiddle multiply includes column 0
 // (fft.hpp:294); the 1-lane four-step skips it (fft.hpp:293). kLaneRenorm: four-step results are stored
-// through qts(hi, lo) (fft.hpp:200-204).
+// through qts(hi, lo) (fft.hpp:200-204). kWide: the real type is wider than float64, so the RFFT split and merge
+// take conjugate pairs together (the reference's non-double branch, fft.hpp:374-407,417-457), and the passes stage
+// their sub-FFT twiddles in shared memory.
 struct ArF64 {  // Precision::Fast: float64 everywhere (V4 lanes and scalar alike)
     using R = double;
     using W = double;
-    static constexpr bool kLanes = true, kLaneRenorm = false, kDD = false;
+    static constexpr bool kLanes = true, kLaneRenorm = false, kWide = false;
     static constexpr int kMinBlocks = KB_MINB_F64, kMaxThreads = KB_MAXT_F64;
     static __device__ __forceinline__ R add(R a, R b) { return __dadd_rn(a, b); }
     static __device__ __forceinline__ R sub(R a, R b) { return __dsub_rn(a, b); }
@@ -100,7 +113,7 @@ struct ArF64 {  // Precision::Fast: float64 everywhere (V4 lanes and scalar alik
 struct ArDDShort {  // four-step sub-FFTs of Precision::Exact (DD4 lanes)
     using R = dd;
     using W = dd;
-    static constexpr bool kLanes = true, kLaneRenorm = true, kDD = true;
+    static constexpr bool kLanes = true, kLaneRenorm = true, kWide = true;
     static constexpr int kMinBlocks = KB_MINB_DD, kMaxThreads = KB_MAXT_DD;
     static __device__ __forceinline__ R add(R a, R b) { return add_short(a, b); }
     static __device__ __forceinline__ R sub(R a, R b) { return add_short(a, dd_neg(b)); }
@@ -116,7 +129,7 @@ struct ArDDShort {  // four-step sub-FFTs of Precision::Exact (DD4 lanes)
 struct ArDDAccurate {  // scalar dd: direct SFFT, Bluestein, RFFT split/merge, spectrum, kernel design
     using R = dd;
     using W = dd;
-    static constexpr bool kLanes = false, kLaneRenorm = false, kDD = true;
+    static constexpr bool kLanes = false, kLaneRenorm = false, kWide = true;
     static constexpr int kMinBlocks = KB_MINB_DD, kMaxThreads = KB_MAXT_DD;
     static __device__ __forceinline__ R add(R a, R b) { return add_accurate(a, b); }
     static __device__ __forceinline__ R sub(R a, R b) { return add_accurate(a, dd_neg(b)); }
@@ -127,6 +140,22 @@ struct ArDDAccurate {  // scalar dd: direct SFFT, Bluestein, RFFT split/merge, s
     static __device__ __forceinline__ R from_f64(double v) { return dd{v, 0.0}; }
     static __device__ __forceinline__ double to_f64(R v) { return __dadd_rn(v.hi, v.lo); }
     static __device__ __forceinline__ R renorm(R v) { return qts(v.hi, v.lo); }
+};
+
+struct ArX80 {  // Precision::LongDouble: x87 extended everywhere, one lane (CFFT<long double, long double, long double>)
+    using R = x80;
+    using W = x80;
+    static constexpr bool kLanes = false, kLaneRenorm = false, kWide = true;
+    static constexpr int kMinBlocks = KB_MINB_X80, kMaxThreads = KB_MAXT_X80;
+    static __device__ __forceinline__ R add(R a, R b) { return x80_add(a, b); }
+    static __device__ __forceinline__ R sub(R a, R b) { return x80_sub(a, b); }
+    static __device__ __forceinline__ R mul(R a, R b) { return x80_mul(a, b); }
+    static __device__ __forceinline__ R neg(R a) { return x80_neg(a); }
+    static __device__ __forceinline__ R zero() { return x80{0ull, 0, 0}; }
+    static __device__ __forceinline__ R from_w(W w) { return w; }
+    static __device__ __forceinline__ R from_f64(double v) { return x80_from_f64(v); }
+    static __device__ __forceinline__ double to_f64(R v) { return x80_to_f64(v); }
+    static __device__ __forceinline__ R renorm(R v) { return v; }
 };
 
 template <class Ar>

@@ -13,7 +13,8 @@
 // memory (fft.cuh). Smaller FFTs run whole in one CTA.
 //
 // Arithmetic (dd.cuh): fast = f64; exact = short-add dd in the four-step sub-FFTs and accurate-add dd
-// elsewhere, exactly as the reference instantiates its templates, so the output is byte-identical.
+// elsewhere; long double = x87 extended emulated in integers (x80.cuh) everywhere, exactly as the reference
+// instantiates its templates, so the output is byte-identical.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -23,6 +24,7 @@
 #include <mutex>
 #include <new>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../host/ddh.hpp"
@@ -160,7 +162,7 @@ __device__ __forceinline__ CxR<Ar> load_input(const PassParams<Ar>& P, const Tas
         return CxR<Ar>{Ar::from_f64(x0), Ar::from_f64(x1)};
     } else if constexpr (SRC == kSrcComplex) {
         return src[i];
-    } else if constexpr (Ar::kDD) {
+    } else if constexpr (Ar::kWide) {
         const double2 a = __ldg(reinterpret_cast<const double2*>(P.ddreal) + 2 * i);
         const double2 b = __ldg(reinterpret_cast<const double2*>(P.ddreal) + 2 * i + 1);
         return CxR<Ar>{R{a.x, a.y}, R{b.x, b.y}};
@@ -382,7 +384,7 @@ __global__ void k_split(const __grid_constant__ SpecParams<Ar> P) {
     C* X = P.X + blockIdx.y * P.stride;
     const int h = P.h;
     const typename Ar::R half = Ar::from_f64(0.5);
-    const int last = Ar::kDD ? h / 2 : h - 1;
+    const int last = Ar::kWide ? h / 2 : h - 1;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k <= last; k += gridDim.x * blockDim.x) {
         if (k == 0) {
             const C z0 = Z[0];
@@ -395,7 +397,7 @@ __global__ void k_split(const __grid_constant__ SpecParams<Ar> P) {
         const C E = c_add<Ar>(a, bb), O = c_mul_mi<Ar>(c_sub<Ar>(a, bb));
         const C v = c_add<Ar>(E, c_mulw<Ar>(O, ld_tw(P.w_fw + k)));
         X[k] = c_scale<Ar>(v, half);
-        if (Ar::kDD && j != k) {
+        if (Ar::kWide && j != k) {
             const C u = c_add<Ar>(c_conj<Ar>(E), c_mulw<Ar>(c_conj<Ar>(O), ld_tw(P.w_fw + j)));
             X[j] = c_scale<Ar>(u, half);
         }
@@ -410,6 +412,11 @@ template <>
 __device__ __forceinline__ dd ld_w<dd>(const dd* p) {
     const double2 a = __ldg(reinterpret_cast<const double2*>(p));
     return dd{a.x, a.y};
+}
+template <>
+__device__ __forceinline__ x80 ld_w<x80>(const x80* p) {
+    const longlong2 a = __ldg(reinterpret_cast<const longlong2*>(p));
+    return x80{(unsigned long long)a.x, (int)a.y, 0};
 }
 
 // Y[k]: spectrum multiply with fold (down) or periodic extension (up) (resampler.cpp:64-78)
@@ -464,7 +471,7 @@ __global__ void k_merge(const __grid_constant__ SpecParams<Ar> P) {
     const C* X = P.X + blockIdx.y * P.stride;
     C* Zi = P.Zi + blockIdx.y * P.stride;
     const int hi = P.hi;
-    const int last = Ar::kDD ? hi / 2 : hi - 1;
+    const int last = Ar::kWide ? hi / 2 : hi - 1;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k <= last; k += gridDim.x * blockDim.x) {
         const int j = hi - k;
         const C a = spectrum_bin<Ar>(P, X, k), bb = c_conj<Ar>(spectrum_bin<Ar>(P, X, j));
@@ -473,7 +480,7 @@ __global__ void k_merge(const __grid_constant__ SpecParams<Ar> P) {
         const C D = c_mulw<Ar>(split, CxW<Ar>{wk.re, w_neg(wk.im)});
         const C v = {Ar::sub(E.re, D.im), Ar::add(E.im, D.re)};
         Zi[k] = c_conj<Ar>(v);
-        if (Ar::kDD && k && j != k) {
+        if (Ar::kWide && k && j != k) {
             const C Ej = c_conj<Ar>(E);
             const CxW<Ar> wj = ld_tw(P.w_iv + j);
             const C Dj = c_mulw<Ar>(C{Ar::neg(split.re), split.im}, CxW<Ar>{wj.re, w_neg(wj.im)});
@@ -611,9 +618,38 @@ struct DevBuf {
     }
 };
 
-int upload_cx(const std::vector<HostCx>& v, bool dd_tables, DevBuf& out) {
+// Table formats on the device: the high parts (f64), (hi, lo) pairs (double-double), or the x87 extended value
+// (long double)hi + (long double)lo (fft.hpp:16-17), 16 bytes each.
+enum TabFmt { kTabF64 = 0, kTabDD = 1, kTabX80 = 2 };
+
+size_t tab_esize(int tab) { return tab == kTabF64 ? 16 : 32; }
+
+// from_dd<long double> with the host's own x87 arithmetic, stored as the device's x80 (significand, sign and
+// exponent)
+x80 host_x80(const hd::dd& v) {
+    const long double x = (long double)v.hi + (long double)v.lo;
+    unsigned char b[sizeof(long double)] = {};
+    std::memcpy(b, &x, 10);
+    x80 r{};
+    std::memcpy(&r.m, b, 8);
+    r.se = b[8] | b[9] << 8;
+    return r;
+}
+
+int upload_cx(const std::vector<HostCx>& v, int tab, DevBuf& out) {
+    if (tab == kTabX80) {
+        std::vector<x80> flat(v.size() * 2);
+        for (size_t i = 0; i < v.size(); i++) {
+            flat[2 * i] = host_x80(v[i].re);
+            flat[2 * i + 1] = host_x80(v[i].im);
+        }
+        int rc = out.alloc(flat.size() * sizeof(x80));
+        if (rc) return rc;
+        KB_CUDA(cudaMemcpy(out.p, flat.data(), flat.size() * sizeof(x80), cudaMemcpyHostToDevice));
+        return KBSRC_GPU_OK;
+    }
     std::vector<double> flat;
-    if (dd_tables) {
+    if (tab == kTabDD) {
         flat.resize(v.size() * 4);
         for (size_t i = 0; i < v.size(); i++) {
             flat[4 * i] = v[i].re.hi; flat[4 * i + 1] = v[i].re.lo;
@@ -640,6 +676,9 @@ OddRoots<W> odd_roots() {
             if constexpr (sizeof(W) == sizeof(double)) {
                 o.c[i][k] = c.hi;
                 o.s[i][k] = s.hi;
+            } else if constexpr (std::is_same_v<W, x80>) {
+                o.c[i][k] = host_x80(c);
+                o.s[i][k] = host_x80(s);
             } else {
                 o.c[i][k] = W{c.hi, c.lo};
                 o.s[i][k] = W{s.hi, s.lo};
@@ -704,27 +743,27 @@ struct DevCfft {
     long long slot() const { return m ? m : n; }  // complex values one task slot must hold
 };
 
-int bluestein_kernel(DevCfft& d, bool dd_tables, cudaStream_t st);  // Vf, defined with the launchers
+int bluestein_kernel(DevCfft& d, int tab, cudaStream_t st);  // Vf, defined with the launchers
 
-int make_dev_cfft(int n, bool dd_tables, int fmax, DevCfft& d, cudaStream_t st) {
+int make_dev_cfft(int n, int tab, int fmax, DevCfft& d, cudaStream_t st) {
     d.n = n;
     int rc;
-    const size_t esize = dd_tables ? 32 : 16;
+    const size_t esize = tab_esize(tab);
     if (!hd::smooth7(n)) {
         d.m = (int)next_smooth7(2LL * n - 1);
         d.inner = std::make_unique<DevCfft>();
-        if ((rc = make_dev_cfft(d.m, dd_tables, fmax, *d.inner, st)) != KBSRC_GPU_OK) return rc;
+        if ((rc = make_dev_cfft(d.m, tab, fmax, *d.inner, st)) != KBSRC_GPU_OK) return rc;
         std::vector<HostCx> bc((size_t)n);
         for (long long t = 0; t < n; t++) {
             const long long e = (long long)((__int128)t * t % (2LL * n));
             hd::unit_root(e, 2LL * n, bc[t].re, bc[t].im);
         }
-        if ((rc = upload_cx(bc, dd_tables, d.bc)) != KBSRC_GPU_OK) return rc;
-        return bluestein_kernel(d, dd_tables, st);
+        if ((rc = upload_cx(bc, tab, d.bc)) != KBSRC_GPU_OK) return rc;
+        return bluestein_kernel(d, tab, st);
     }
     if ((rc = build_cfft(n, d.host)) != KBSRC_GPU_OK) return rc;
-    if ((rc = upload_cx(d.host.tw_stage, dd_tables, d.tw_stage)) != KBSRC_GPU_OK) return rc;
-    if (d.host.four && (rc = upload_cx(d.host.tw4, dd_tables, d.tw4)) != KBSRC_GPU_OK) return rc;
+    if ((rc = upload_cx(d.host.tw_stage, tab, d.tw_stage)) != KBSRC_GPU_OK) return rc;
+    if (d.host.four && (rc = upload_cx(d.host.tw4, tab, d.tw4)) != KBSRC_GPU_OK) return rc;
     std::vector<HostCx>().swap(d.host.tw_stage);
     std::vector<HostCx>().swap(d.host.tw4);
     if (d.host.four) {
@@ -751,6 +790,7 @@ int env_int(const char* name, int dflt) {
 struct PlanCore {
     kbsrc_gpu_desc d{};  // the shape (H is not kept)
     bool exact = false;
+    int tab = 0;  // TabFmt of the tables and of the values in the work buffers
     int Nb = 0, Mb = 0, hf = 0, hi = 0, hop = 0;
     DevCfft fw, iv;
     DevBuf w_fw, w_iv, H;
@@ -759,7 +799,7 @@ struct PlanCore {
         const long long n = std::max({(long long)hf + 1, (long long)hi + 1, fw.slot(), iv.slot()});
         return (n + 7) / 8 * 8;
     }
-    size_t esize() const { return exact ? 32 : 16; }
+    size_t esize() const { return tab_esize(tab); }
 };
 
 // A batch group: conversions with one plan, their tasks listed block-major per conversion.
@@ -847,6 +887,13 @@ int allow_large_smem() {
     KB_SMEM((k_direct<ArDDAccurate, kSrcComplex, kDstComplex>));
     KB_SMEM((k_direct<ArDDAccurate, kSrcComplex, kDstOutput>));
     KB_SMEM((k_direct<ArDDAccurate, kSrcDDReal, kDstComplex>));
+    KB_SMEM((k_column<ArX80, kSrcSignal>));
+    KB_SMEM((k_column<ArX80, kSrcComplex>));
+    KB_SMEM((k_row<ArX80, kDstComplex>));
+    KB_SMEM((k_row<ArX80, kDstOutput>));
+    KB_SMEM((k_direct<ArX80, kSrcSignal, kDstComplex>));
+    KB_SMEM((k_direct<ArX80, kSrcComplex, kDstComplex>));
+    KB_SMEM((k_direct<ArX80, kSrcComplex, kDstOutput>));
 #undef KB_SMEM
     if (dev < 64) done[dev] = true;
     return KBSRC_GPU_OK;
@@ -970,10 +1017,14 @@ int launch_cfft(const DevCfft& c, const Slots& sl, void* x, void* a, void* b, vo
 
 // Vf = FFT(v)/m for Bluestein, v[t] = v[m-t] = e^{+i pi t^2/n} (fft.hpp:230-238): the m-point transform in
 // scalar double-double (the reference's CFFT<dd,dd,dd>), divided by m in dd, stored in the engine's precision.
-__global__ void k_vf_scale(const cx<dd>* __restrict__ V, int m, double* __restrict__ out, int dd_out) {
+__global__ void k_vf_scale(const cx<dd>* __restrict__ V, int m, double* __restrict__ out, int tab) {
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x) {
         const dd re = div_dd_f64(V[k].re, (double)m), im = div_dd_f64(V[k].im, (double)m);
-        if (dd_out) {
+        if (tab == kTabX80) {  // from_dd<long double>: (long double)hi + (long double)lo
+            x80* o = reinterpret_cast<x80*>(out);
+            o[2 * k] = x80_add(x80_from_f64(re.hi), x80_from_f64(re.lo));
+            o[2 * k + 1] = x80_add(x80_from_f64(im.hi), x80_from_f64(im.lo));
+        } else if (tab == kTabDD) {
             out[4 * k] = re.hi; out[4 * k + 1] = re.lo; out[4 * k + 2] = im.hi; out[4 * k + 3] = im.lo;
         } else {
             out[2 * k] = re.hi; out[2 * k + 1] = im.hi;
@@ -981,7 +1032,7 @@ __global__ void k_vf_scale(const cx<dd>* __restrict__ V, int m, double* __restri
     }
 }
 
-int bluestein_kernel(DevCfft& d, bool dd_tables, cudaStream_t st) {
+int bluestein_kernel(DevCfft& d, int tab, cudaStream_t st) {
     const int n = d.n, m = d.m;
     std::vector<HostCx> v((size_t)m);
     for (long long t = 0; t < n; t++) {
@@ -991,11 +1042,11 @@ int bluestein_kernel(DevCfft& d, bool dd_tables, cudaStream_t st) {
     }
     DevCfft des;  // the same m-point plan with double-double tables, run in scalar dd
     int rc;
-    if ((rc = make_dev_cfft(m, true, 4, des, st)) != KBSRC_GPU_OK) return rc;
+    if ((rc = make_dev_cfft(m, kTabDD, 4, des, st)) != KBSRC_GPU_OK) return rc;
     DevBuf vin, vout;
-    if ((rc = upload_cx(v, true, vin)) != KBSRC_GPU_OK) return rc;
+    if ((rc = upload_cx(v, kTabDD, vin)) != KBSRC_GPU_OK) return rc;
     if ((rc = vout.alloc((size_t)m * 32)) != KBSRC_GPU_OK) return rc;
-    if ((rc = d.vf.alloc((size_t)m * (dd_tables ? 32 : 16))) != KBSRC_GPU_OK) return rc;
+    if ((rc = d.vf.alloc((size_t)m * tab_esize(tab))) != KBSRC_GPU_OK) return rc;
     Slots sl{};
     sl.nt = 1;
     Trail tr;
@@ -1003,7 +1054,7 @@ int bluestein_kernel(DevCfft& d, bool dd_tables, cudaStream_t st) {
                                                                                   -1)) != KBSRC_GPU_OK)
         return rc;
     k_vf_scale<<<grid_for(m, 256), 256, 0, st>>>(static_cast<const cx<dd>*>(vout.p), m, static_cast<double*>(d.vf.p),
-                                                  dd_tables ? 1 : 0);
+                                                  tab);
     KB_CUDA(cudaGetLastError());
     KB_CUDA(cudaStreamSynchronize(st));  // the temporaries are freed on return
     return KBSRC_GPU_OK;
@@ -1048,9 +1099,9 @@ int enqueue_plan(const PlanCore& pc, const Work& work, long long t_begin, long l
         s.w_iv = static_cast<const CxW<ArS>*>(pc.w_iv.p);
         s.H = static_cast<const WS*>(pc.H.p);
         s.h = pc.hf; s.hi = pc.hi; s.Nb = pc.Nb; s.Mb = pc.Mb; s.up = d.up; s.Jg = d.Jg;
-        k_split<ArS><<<dim3(grid_for(pc.hf / 2 + 1 + (ArS::kDD ? 0 : pc.hf / 2), 256), sl.nt), 256, 0, st>>>(s);
+        k_split<ArS><<<dim3(grid_for(pc.hf / 2 + 1 + (ArS::kWide ? 0 : pc.hf / 2), 256), sl.nt), 256, 0, st>>>(s);
         if ((rc = tr.mark(st, kSplit)) != KBSRC_GPU_OK) return rc;
-        k_merge<ArS><<<dim3(grid_for(pc.hi / 2 + 1 + (ArS::kDD ? 0 : pc.hi / 2), 256), sl.nt), 256, 0, st>>>(s);
+        k_merge<ArS><<<dim3(grid_for(pc.hi / 2 + 1 + (ArS::kWide ? 0 : pc.hi / 2), 256), sl.nt), 256, 0, st>>>(s);
         if ((rc = tr.mark(st, kMerge)) != KBSRC_GPU_OK) return rc;
         // inverse complex FFT of buf[z] and the output epilogue
         rc = launch_cfft<ArL, ArS, kSrcComplex, kDstOutput>(pc.iv, sl, buf[z], buf[1 - z], buf[z], nullptr, st, tr,
@@ -1062,6 +1113,7 @@ int enqueue_plan(const PlanCore& pc, const Work& work, long long t_begin, long l
 
 int enqueue_any(const PlanCore& pc, const Work& work, long long t_begin, long long t_end, void* a, void* b,
                 long long stride, long long wave, cudaStream_t st, Trail& tr) {
+    if (pc.tab == kTabX80) return enqueue_plan<ArX80, ArX80>(pc, work, t_begin, t_end, a, b, stride, wave, st, tr);
     if (pc.exact) return enqueue_plan<ArDDShort, ArDDAccurate>(pc, work, t_begin, t_end, a, b, stride, wave, st, tr);
     return enqueue_plan<ArF64, ArF64>(pc, work, t_begin, t_end, a, b, stride, wave, st, tr);
 }
@@ -1088,7 +1140,8 @@ size_t cfft_bytes(const DevCfft& c) {
 
 int check_desc(const kbsrc_gpu_desc* d) {
     if (!d) return fail(KBSRC_GPU_E_ARG, "null descriptor");
-    if (d->precision != KBSRC_GPU_FAST && d->precision != KBSRC_GPU_EXACT) return fail(KBSRC_GPU_E_ARG, "precision");
+    if (d->precision != KBSRC_GPU_FAST && d->precision != KBSRC_GPU_EXACT && d->precision != KBSRC_GPU_LD)
+        return fail(KBSRC_GPU_E_ARG, "precision");
     if (d->channels < 1 || d->P < 1 || d->Q < 1 || d->nb < 2 || d->nb % 2 || d->marg < 0 || d->nb <= 2 * d->marg)
         return fail(KBSRC_GPU_E_ARG, "bad plan shape");
     if (d->frames < 0 || d->nout < 0 || d->nblk < 0 || d->edge_len < 0 || d->lead < 0 || d->Jg < 0)
@@ -1099,9 +1152,17 @@ int check_desc(const kbsrc_gpu_desc* d) {
     return KBSRC_GPU_OK;
 }
 
-int upload_real(const double* hilo, long long n, bool dd_tables, DevBuf& out) {
+int upload_real(const double* hilo, long long n, int tab, DevBuf& out) {
+    if (tab == kTabX80) {
+        std::vector<x80> v((size_t)n);
+        for (long long i = 0; i < n; i++) v[i] = host_x80(hd::dd{hilo[2 * i], hilo[2 * i + 1]});
+        int rc = out.alloc(v.size() * sizeof(x80));
+        if (rc) return rc;
+        KB_CUDA(cudaMemcpy(out.p, v.data(), v.size() * sizeof(x80), cudaMemcpyHostToDevice));
+        return KBSRC_GPU_OK;
+    }
     std::vector<double> v;
-    if (dd_tables) v.assign(hilo, hilo + 2 * n);
+    if (tab == kTabDD) v.assign(hilo, hilo + 2 * n);
     else {
         v.resize((size_t)n);
         for (long long i = 0; i < n; i++) v[i] = hilo[2 * i];
@@ -1118,17 +1179,18 @@ int make_core(const kbsrc_gpu_desc* desc, PlanCore& pc, cudaStream_t st) {
     pc.d = *desc;
     pc.d.H = nullptr;
     pc.exact = desc->precision == KBSRC_GPU_EXACT;
+    pc.tab = desc->precision == KBSRC_GPU_FAST ? kTabF64 : desc->precision == KBSRC_GPU_EXACT ? kTabDD : kTabX80;
     pc.Nb = (int)(desc->nb * desc->Q);
     pc.Mb = (int)(desc->nb * desc->P);
     pc.hf = pc.Nb / 2;
     pc.hi = pc.Mb / 2;
     pc.hop = desc->nb - 2 * desc->marg;
-    const int fmax = env_int("KBSRC_GPU_FMAX", pc.exact ? 8 : 16);
-    if ((rc = make_dev_cfft(pc.hf, pc.exact, fmax, pc.fw, st)) != KBSRC_GPU_OK) return rc;
-    if ((rc = make_dev_cfft(pc.hi, pc.exact, fmax, pc.iv, st)) != KBSRC_GPU_OK) return rc;
-    if ((rc = upload_cx(split_roots(pc.Nb), pc.exact, pc.w_fw)) != KBSRC_GPU_OK) return rc;
-    if ((rc = upload_cx(split_roots(pc.Mb), pc.exact, pc.w_iv)) != KBSRC_GPU_OK) return rc;
-    return upload_real(desc->H, desc->H_len, pc.exact, pc.H);
+    const int fmax = env_int("KBSRC_GPU_FMAX", pc.tab == kTabF64 ? 16 : 8);
+    if ((rc = make_dev_cfft(pc.hf, pc.tab, fmax, pc.fw, st)) != KBSRC_GPU_OK) return rc;
+    if ((rc = make_dev_cfft(pc.hi, pc.tab, fmax, pc.iv, st)) != KBSRC_GPU_OK) return rc;
+    if ((rc = upload_cx(split_roots(pc.Nb), pc.tab, pc.w_fw)) != KBSRC_GPU_OK) return rc;
+    if ((rc = upload_cx(split_roots(pc.Mb), pc.tab, pc.w_iv)) != KBSRC_GPU_OK) return rc;
+    return upload_real(desc->H, desc->H_len, pc.tab, pc.H);
 }
 
 int create_impl(const kbsrc_gpu_desc* desc, kbsrc_gpu_engine** out) {
@@ -1737,9 +1799,9 @@ int kbsrc_gpu_kernel_spectrum(const double* taps, int L, int n, double scale, do
         }
         const int h = n / 2;
         DevCfft c;  // scalar double-double transform (RFFT<dd,dd,dd>), Bluestein when h is not 7-smooth
-        if ((rc = make_dev_cfft(h, true, 4, c, st)) != KBSRC_GPU_OK) return rc;
+        if ((rc = make_dev_cfft(h, kTabDD, 4, c, st)) != KBSRC_GPU_OK) return rc;
         DevBuf w, rin, A, B, Hd;
-        if ((rc = upload_cx(split_roots(n), true, w)) != KBSRC_GPU_OK) return rc;
+        if ((rc = upload_cx(split_roots(n), kTabDD, w)) != KBSRC_GPU_OK) return rc;
         if ((rc = rin.alloc(r.size() * 8)) != KBSRC_GPU_OK) return rc;
         const size_t slot = (size_t)std::max<long long>(h + 1, c.slot()) * 32;
         if ((rc = A.alloc(slot)) != KBSRC_GPU_OK) return rc;

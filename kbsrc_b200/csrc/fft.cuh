@@ -44,11 +44,18 @@ __device__ __forceinline__ cx<dd> ld_tw<dd>(const cx<dd>* p) {
     return cx<dd>{dd{a.x, a.y}, dd{b.x, b.y}};
 }
 
-// Stage twiddles are read from shared memory (double-double: staged once per CTA) or straight from the global
-// table through the read-only path (f64: a CTA's work is too short to amortise the copy).
+template <>
+__device__ __forceinline__ cx<x80> ld_tw<x80>(const cx<x80>* p) {
+    const longlong2* q = reinterpret_cast<const longlong2*>(p);
+    const longlong2 a = __ldg(q), b = __ldg(q + 1);
+    return cx<x80>{x80{(unsigned long long)a.x, (int)a.y, 0}, x80{(unsigned long long)b.x, (int)b.y, 0}};
+}
+
+// Stage twiddles are read from shared memory (double-double and extended: staged once per CTA) or straight from
+// the global table through the read-only path (f64: a CTA's work is too short to amortise the copy).
 template <class Ar>
 __device__ __forceinline__ CxW<Ar> tw_at(const CxW<Ar>* p) {
-    if constexpr (Ar::kDD) return *p;
+    if constexpr (Ar::kWide) return *p;
     else return ld_tw(p);
 }
 
@@ -144,12 +151,12 @@ __device__ __forceinline__ void bfly_odd(const Planes<Ar>& a, int ia, int sin, c
     }
 }
 
-// Twiddles a pass reads: for double-double, the plan's stage twiddles copied to shared memory (tws, sp.twn
+// Twiddles a pass reads: for the wide types, the plan's stage twiddles copied to shared memory (tws, sp.twn
 // entries; the caller synchronises before use); for f64, the global table itself.
 template <class Ar>
 __device__ __forceinline__ const CxW<Ar>* stage_twiddles(const SubPlan& sp, const CxW<Ar>* __restrict__ tw,
                                                          CxW<Ar>* tws) {
-    if constexpr (!Ar::kDD) {
+    if constexpr (!Ar::kWide) {
         return tw + sp.tw0;
     } else {
         for (int i = threadIdx.x; i < sp.twn; i += blockDim.x) tws[i] = ld_tw(tw + sp.tw0 + i);

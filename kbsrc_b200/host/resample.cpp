@@ -291,8 +291,6 @@ std::unique_ptr<Conversion> prepare(const double* in, long long frames, int ch, 
     cv->frames = frames;
     const Plan& pl = cv->pl;
     if (pl.copy) return cv;
-    if (opt.precision == Precision::LongDouble)
-        throw std::runtime_error("mode ld (x87 long double) is not available on the GPU engine");
     const double t0 = now();
     const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
     const int threads = opt.threads ? opt.threads : std::min(hw, 8);
@@ -370,7 +368,9 @@ std::unique_ptr<Conversion> prepare(const double* in, long long frames, int ch, 
         }
     }
     kbsrc_gpu_desc& d = cv->desc;
-    d.precision = opt.precision == Precision::Fast ? KBSRC_GPU_FAST : KBSRC_GPU_EXACT;
+    d.precision = opt.precision == Precision::Fast         ? KBSRC_GPU_FAST
+                  : opt.precision == Precision::LongDouble ? KBSRC_GPU_LD
+                                                           : KBSRC_GPU_EXACT;
     d.channels = ch;
     d.P = P;
     d.Q = Q;

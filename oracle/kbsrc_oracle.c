@@ -816,6 +816,335 @@ static void engine(const Plan* pl, double** xx, double** out, int ch, const dd* 
     rplan_free(&Iv);
 }
 
+/* ------------------------------------------------------------------------------------------------------ */
+/* the long double engine: run_engine<long double, long double, long double> (resampler.cpp:214-215)         */
+/* ------------------------------------------------------------------------------------------------------ */
+/* Every value is an x87 extended real and every +, -, * one x87 operation (long double on x86-64: 64-bit
+ * significand, round to nearest). Tables are the dd tables above converted by from_dd<long double>, i.e.
+ * (long double)hi + (long double)lo (fft.hpp:17). CFFT<LD,LD,LD> has one lane, so its four-step twiddle skips
+ * column 0 (fft.hpp:293); the RFFT split and merge run conjugate pairs (fft.hpp:397-407,447-457). */
+typedef long double LD;
+typedef struct { LD re, im; } cld;
+static inline LD ld_of(dd v) { return (LD)v.hi + (LD)v.lo; }
+static inline cld lc(LD re, LD im) { cld r; r.re = re; r.im = im; return r; }
+static inline cld lc_of(cdd v) { return lc(ld_of(v.re), ld_of(v.im)); }
+static inline cld l_add(cld a, cld b) { return lc(a.re + b.re, a.im + b.im); }
+static inline cld l_sub(cld a, cld b) { return lc(a.re - b.re, a.im - b.im); }
+static inline cld l_mul(cld a, cld b) { return lc(a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re); }
+static inline cld l_conj(cld a) { return lc(a.re, -a.im); }
+static inline cld l_mi(cld a) { return lc(a.im, -a.re); } /* a * (-i) */
+static inline cld l_scale(cld a, LD h) { return lc(a.re * h, a.im * h); }
+
+typedef struct {
+    SPlan sp; /* radices and dd tables */
+    cld* tw[MAXST];
+    LD cr[3][7], sr[3][7];
+} LSPlan;
+
+static int lsfft_init(LSPlan* L, int n) {
+    if (sfft_init(&L->sp, n)) return -1;
+    for (int g = 0; g < L->sp.ns; g++) {
+        const size_t cnt = (size_t)L->sp.m[g] * (L->sp.r[g] - 1);
+        L->tw[g] = malloc(sizeof(cld) * cnt + 1);
+        for (size_t i = 0; i < cnt; i++) L->tw[g][i] = lc_of(L->sp.tw[g][i]);
+    }
+    for (int i = 0; i < 3; i++)
+        for (int k = 0; k < 7; k++) {
+            L->cr[i][k] = ld_of(L->sp.cr[i][k]);
+            L->sr[i][k] = ld_of(L->sp.sr[i][k]);
+        }
+    return 0;
+}
+static void lsfft_free(LSPlan* L) {
+    for (int g = 0; g < L->sp.ns; g++) free(L->tw[g]);
+    sfft_free(&L->sp);
+}
+
+static void l_odd_bfly(int R, const cld* src, size_t sm, cld* dst, int s, int q, const LD* cr, const LD* sr,
+                       const cld* tw, int p0) {
+    const int H = (R - 1) / 2;
+    cld a0 = src[q], S[3], Df[3];
+    for (int t = 1; t <= H; t++) {
+        cld x = src[q + t * sm], y = src[q + (R - t) * sm];
+        S[t - 1] = l_add(x, y);
+        Df[t - 1] = l_sub(x, y);
+    }
+    cld sum = a0;
+    for (int t = 0; t < H; t++) sum = l_add(sum, S[t]);
+    dst[q] = sum;
+    for (int u = 1; u <= H; u++) {
+        cld Aa = a0, B = lc(0.0L, 0.0L);
+        for (int t = 1; t <= H; t++) {
+            int m = (t * u) % R;
+            LD c = cr[m], sn = sr[m];
+            Aa = lc(Aa.re + S[t - 1].re * c, Aa.im + S[t - 1].im * c);
+            B = lc(B.re + Df[t - 1].re * sn, B.im + Df[t - 1].im * sn);
+        }
+        cld xu = lc(Aa.re + B.im, Aa.im - B.re), xr = lc(Aa.re - B.im, Aa.im + B.re);
+        if (p0) {
+            dst[q + u * s] = xu;
+            dst[q + (R - u) * s] = xr;
+        } else {
+            dst[q + u * s] = l_mul(xu, tw[u - 1]);
+            dst[q + (R - u) * s] = l_mul(xr, tw[R - u - 1]);
+        }
+    }
+}
+
+static cld* lsfft_run(const LSPlan* L, cld* x, cld* y) {
+    const SPlan* P = &L->sp;
+    cld *a = x, *b = y;
+    for (int g = 0; g < P->ns; g++) {
+        const int r = P->r[g], m = P->m[g], s = P->s[g];
+        for (int p = 0; p < m; p++) {
+            const cld* tw = L->tw[g] + (size_t)p * (r - 1);
+            const cld* src = a + (size_t)s * p;
+            cld* dst = b + (size_t)s * r * p;
+            const size_t sm = (size_t)s * m;
+            for (int q = 0; q < s; q++) {
+                if (r == 4) {
+                    cld a0 = src[q], a1 = src[q + sm], a2 = src[q + 2 * sm], a3 = src[q + 3 * sm];
+                    cld t0 = l_add(a0, a2), t1 = l_sub(a0, a2), t2 = l_add(a1, a3), t3 = l_mi(l_sub(a1, a3));
+                    dst[q] = l_add(t0, t2);
+                    if (p == 0) {
+                        dst[q + s] = l_add(t1, t3);
+                        dst[q + 2 * s] = l_sub(t0, t2);
+                        dst[q + 3 * s] = l_sub(t1, t3);
+                    } else {
+                        dst[q + s] = l_mul(l_add(t1, t3), tw[0]);
+                        dst[q + 2 * s] = l_mul(l_sub(t0, t2), tw[1]);
+                        dst[q + 3 * s] = l_mul(l_sub(t1, t3), tw[2]);
+                    }
+                } else if (r == 2) {
+                    cld a0 = src[q], a1 = src[q + sm];
+                    dst[q] = l_add(a0, a1);
+                    dst[q + s] = p ? l_mul(l_sub(a0, a1), tw[0]) : l_sub(a0, a1);
+                } else {
+                    int i = r == 3 ? 0 : r == 5 ? 1 : 2;
+                    l_odd_bfly(r, src, sm, dst, s, q, L->cr[i], L->sr[i], tw, p == 0);
+                }
+            }
+        }
+        cld* t = a; a = b; b = t;
+    }
+    return a;
+}
+
+typedef struct LCPlan {
+    int n, four, N1, N2, m;
+    LSPlan s1, s2, sd;
+    cld* tw;
+    struct LCPlan* inner;
+    cld *bc, *Vf;
+} LCPlan;
+
+static void lcplan_free(LCPlan* C) {
+    if (C->m) {
+        lcplan_free(C->inner);
+        free(C->inner);
+        free(C->bc);
+        free(C->Vf);
+        return;
+    }
+    if (C->four) {
+        lsfft_free(&C->s1);
+        lsfft_free(&C->s2);
+        free(C->tw);
+    } else {
+        lsfft_free(&C->sd);
+    }
+}
+
+static int lcplan_init(LCPlan* C, int n) {
+    memset(C, 0, sizeof *C);
+    C->n = n;
+    if (!smooth7(n)) { /* Bluestein (fft.hpp:228-240); Vf from the scalar dd transform, then from_dd */
+        C->m = (int)next_smooth7(2LL * n - 1);
+        C->inner = malloc(sizeof(LCPlan));
+        if (lcplan_init(C->inner, C->m)) return -1;
+        C->bc = malloc(sizeof(cld) * n);
+        cdd* v = calloc((size_t)C->m, sizeof(cdd));
+        cdd* w = calloc((size_t)C->m, sizeof(cdd));
+        for (long long t = 0; t < n; t++) {
+            long long e = (long long)((__int128)t * t % (2LL * n));
+            dd c, sn;
+            dcis(e, 2LL * n, &c, &sn);
+            C->bc[t] = lc(ld_of(c), ld_of(sn));
+            v[t] = cx(c, sn);
+            if (t) v[C->m - t] = cx(c, sn);
+        }
+        CPlan fd;
+        cplan_init(&fd, C->m, MODE_DD);
+        cdd* V = cplan_run(&fd, v, w);
+        C->Vf = malloc(sizeof(cld) * C->m);
+        for (int k = 0; k < C->m; k++)
+            C->Vf[k] = lc(ld_of(ddivd(V[k].re, (double)C->m)), ld_of(ddivd(V[k].im, (double)C->m)));
+        free(v);
+        free(w);
+        oracle_cplan_free(&fd);
+        return 0;
+    }
+    C->four = n > 2048;
+    if (C->four) {
+        int best = 1;
+        for (int d = 1; (long long)d * d <= n; d++)
+            if (n % d == 0) best = d;
+        C->N1 = best;
+        C->N2 = n / best;
+        if (C->N1 < 8) C->four = 0;
+    }
+    if (!C->four) return lsfft_init(&C->sd, n);
+    lsfft_init(&C->s1, C->N1);
+    lsfft_init(&C->s2, C->N2);
+    C->tw = malloc(sizeof(cld) * (size_t)n);
+    CisTab ct;
+    cis_init(&ct, n);
+    for (int k1 = 0; k1 < C->N1; k1++)
+        for (int n2 = 0; n2 < C->N2; n2++) {
+            dd c, sn;
+            cis_get(&ct, -(long long)k1 * n2, &c, &sn);
+            C->tw[(size_t)k1 * C->N2 + n2] = lc(ld_of(c), ld_of(sn));
+        }
+    cis_free(&ct);
+    return 0;
+}
+
+static cld* lcplan_run(const LCPlan* C, cld* x, cld* y) {
+    if (C->m) { /* X_k = conj(b_k) sum_j (x_j conj(b_j)) b_{k-j} (fft.hpp:268-277) */
+        cld* u = malloc(sizeof(cld) * C->m);
+        cld* u2 = malloc(sizeof(cld) * C->m);
+        for (int j = 0; j < C->n; j++) u[j] = l_mul(x[j], l_conj(C->bc[j]));
+        for (int j = C->n; j < C->m; j++) u[j] = lc(0.0L, 0.0L);
+        cld* U = lcplan_run(C->inner, u, u2);
+        for (int k = 0; k < C->m; k++) U[k] = l_conj(l_mul(U[k], C->Vf[k]));
+        cld* other = U == u ? u2 : u;
+        cld* Cc = lcplan_run(C->inner, U, other);
+        for (int k = 0; k < C->n; k++) y[k] = l_mul(l_conj(Cc[k]), l_conj(C->bc[k]));
+        free(u);
+        free(u2);
+        return y;
+    }
+    if (!C->four) return lsfft_run(&C->sd, x, y);
+    const int N1 = C->N1, N2 = C->N2, M = N1 > N2 ? N1 : N2;
+    cld* tile = malloc(sizeof(cld) * M);
+    cld* wk = malloc(sizeof(cld) * M);
+    for (int c0 = 0; c0 < N2; c0++) { /* column pass, one lane: column 0 keeps its values (fft.hpp:283-299) */
+        for (int r = 0; r < N1; r++) tile[r] = x[(size_t)r * N2 + c0];
+        cld* res = lsfft_run(&C->s1, tile, wk);
+        for (int k1 = 0; k1 < N1; k1++) {
+            cld v = res[k1];
+            if (k1 && c0) v = l_mul(v, C->tw[(size_t)k1 * N2 + c0]);
+            x[(size_t)k1 * N2 + c0] = v;
+        }
+    }
+    for (int r0 = 0; r0 < N1; r0++) { /* row pass, transposed store (fft.hpp:300-311) */
+        for (int i = 0; i < N2; i++) tile[i] = x[(size_t)r0 * N2 + i];
+        cld* res = lsfft_run(&C->s2, tile, wk);
+        for (int k2 = 0; k2 < N2; k2++) y[(size_t)N1 * k2 + r0] = res[k2];
+    }
+    free(tile);
+    free(wk);
+    return y;
+}
+
+static void engine_ld(const Plan* pl, double** xx, double** out, int ch, const dd* Hd, long long Hn) {
+    const long long P = pl->P, Q = pl->Q;
+    const int Nb = pl->Nb, Mb = pl->Mb, K = Mb / 2 + 1, up = pl->up, Jg = pl->Jg, h = Nb / 2, hi = Mb / 2;
+    LCPlan Fw, Iv;
+    lcplan_init(&Fw, h);
+    lcplan_init(&Iv, hi);
+    cld* wf = malloc(sizeof(cld) * (h + 1));
+    cld* wi = malloc(sizeof(cld) * (hi + 1));
+    CisTab ct;
+    cis_init(&ct, Nb);
+    for (int k = 0; k <= h; k++) { dd c, s; cis_get(&ct, -k, &c, &s); wf[k] = lc(ld_of(c), ld_of(s)); }
+    cis_free(&ct);
+    cis_init(&ct, Mb);
+    for (int k = 0; k <= hi; k++) { dd c, s; cis_get(&ct, -k, &c, &s); wi[k] = lc(ld_of(c), ld_of(s)); }
+    cis_free(&ct);
+    LD* H = malloc(sizeof(LD) * (size_t)Hn);
+    for (long long k = 0; k < Hn; k++) H[k] = ld_of(Hd[k]);
+    const int mx = Nb > Mb ? Nb : Mb;
+    cld* X = malloc(sizeof(cld) * (size_t)(h + 1));
+    cld* Y = malloc(sizeof(cld) * (size_t)K);
+    cld* z = malloc(sizeof(cld) * (size_t)(mx / 2 + 1));
+    cld* y = malloc(sizeof(cld) * (size_t)(mx / 2 + 1));
+    LD* r = malloc(sizeof(LD) * (size_t)Mb);
+    for (int c = 0; c < ch; c++)
+        for (long long b = 0; b < pl->nblk; b++) {
+            const double* s = xx[c] + b * pl->hop * Q;
+            /* forward real FFT (fft.hpp:362-408): pack, transform, conjugate-pair split */
+            for (int i = 0; i < h; i++) z[i] = lc((LD)s[2 * i], (LD)s[2 * i + 1]);
+            cld* Z = lcplan_run(&Fw, z, y);
+            X[0] = lc(Z[0].re + Z[0].im, 0.0L);
+            X[h] = lc(Z[0].re - Z[0].im, 0.0L);
+            for (int k = 1; k <= h / 2; k++) {
+                const int j = h - k;
+                cld A = Z[k], B = l_conj(Z[j]);
+                cld E = l_add(A, B), O = l_mi(l_sub(A, B));
+                cld v = l_add(E, l_mul(O, wf[k]));
+                X[k] = lc(v.re * 0.5L, v.im * 0.5L);
+                if (j != k) {
+                    cld u = l_add(l_conj(E), l_mul(l_conj(O), wf[j]));
+                    X[j] = lc(u.re * 0.5L, u.im * 0.5L);
+                }
+            }
+            /* spectrum (resampler.cpp:53-78) */
+            if (Jg) {
+                for (int k = 0; k < K; k++) Y[k] = lc(0.0L, 0.0L);
+                for (int j = 0; j <= Jg; j++) {
+                    int jj = j % Nb;
+                    cld x = jj <= Nb / 2 ? X[jj] : l_conj(X[Nb - jj]);
+                    cld v = l_scale(x, H[j]);
+                    int k = j % Mb;
+                    if (j == 0) Y[0] = l_add(Y[0], v);
+                    else if (k == 0 || 2 * k == Mb) Y[k].re = Y[k].re + 2.0L * v.re;
+                    else if (2 * k < Mb) Y[k] = l_add(Y[k], v);
+                    else Y[Mb - k] = l_add(Y[Mb - k], l_conj(v));
+                }
+                Y[0].im = 0.0L;
+                Y[Mb / 2].im = 0.0L;
+            } else if (!up) {
+                for (int k = 0; k < K; k++) Y[k] = l_scale(X[k], H[k]);
+                int jmax = Nb / 2 < Mb - 1 ? Nb / 2 : Mb - 1;
+                for (int j = K; j <= jmax; j++) Y[Mb - j] = l_add(Y[Mb - j], l_conj(l_scale(X[j], H[j])));
+                Y[Mb / 2] = lc(2.0L * X[Mb / 2].re * H[Mb / 2], 0.0L);
+            } else {
+                for (int k = 0; k < K; k++) {
+                    int kk = k % Nb;
+                    cld v = kk <= Nb / 2 ? X[kk] : l_conj(X[Nb - kk]);
+                    Y[k] = l_scale(v, H[k]);
+                }
+                Y[Mb / 2].im = 0.0L;
+            }
+            /* inverse real FFT (fft.hpp:411-461): conjugate-pair merge, transform, unpack */
+            for (int k = 0; k <= hi / 2; k++) {
+                const int j = hi - k;
+                cld A = Y[k], B = l_conj(Y[j]);
+                cld E = l_add(A, B), split = l_sub(A, B);
+                cld Dd = l_mul(split, l_conj(wi[k]));
+                z[k] = l_conj(lc(E.re - Dd.im, E.im + Dd.re));
+                if (k && j != k) {
+                    cld Ej = l_conj(E), Dj = l_mul(lc(-split.re, split.im), l_conj(wi[j]));
+                    z[j] = l_conj(lc(Ej.re - Dj.im, Ej.im + Dj.re));
+                }
+            }
+            cld* Zi = lcplan_run(&Iv, z, y);
+            for (int i = 0; i < hi; i++) {
+                r[2 * i] = Zi[i].re;
+                r[2 * i + 1] = -Zi[i].im;
+            }
+            double* dst = out[c];
+            for (long long i = 0; i < (long long)pl->hop * P; i++) {
+                long long d = b * pl->hop * P + i - pl->o;
+                if (d >= 0 && d < pl->nout) dst[d] = (double)r[pl->marg * P + i];
+            }
+        }
+    free(X); free(Y); free(z); free(y); free(r); free(H); free(wf); free(wi);
+    lcplan_free(&Fw);
+    lcplan_free(&Iv);
+}
+
 /* 32-sample raised-cosine fade (resampler.cpp:170-171) */
 static void fade32(double fd[32]) {
     for (int i = 0; i < 32; i++) {
@@ -845,11 +1174,13 @@ long long oracle_plan(long long frames, int ch, int rate_in, int rate_out, int f
     return pl.nout;
 }
 
-/* Full conversion. out: ch * out_cap doubles, planar. Returns nout, or a negative error code. */
-long long oracle_resample(const double* in, long long frames, int ch, int rate_in, int rate_out, int fast,
+/* Full conversion. mode: 0 exact, 1 fast, 2 long double. out: ch * out_cap doubles, planar. Returns nout, or a
+ * negative error code. */
+long long oracle_resample(const double* in, long long frames, int ch, int rate_in, int rate_out, int mode,
                           double length, double beta, int block, int lpc, double* out, long long out_cap,
                           long long* info) {
     Plan pl;
+    const int fast = mode == 1;
     int rc = make_plan(&pl, in, frames, ch, rate_in, rate_out, fast, length, beta, block);
     if (rc < 0) return rc;
     if (pl.nout > out_cap) return -100;
@@ -885,6 +1216,7 @@ long long oracle_resample(const double* in, long long frames, int ch, int rate_i
     }
     /* kernel (resampler.cpp:187-206) */
     dd* H;
+    long long Hn;
     if (pl.gen) {
         long long Nk = (long long)(pl.Nb > pl.Mb ? pl.Nb : pl.Mb) * 5LL / 4;
         Nk += Nk & 1;
@@ -896,6 +1228,7 @@ long long oracle_resample(const double* in, long long frames, int ch, int rate_i
         int L2 = (int)floor(length * fk2);
         dd* h2 = kernel_taps(L2, (long long)(A / g2), (long long)(B / g2), beta);
         H = kernel_spectrum(h2, L2, (int)Nk, (double)pl.Nb);
+        Hn = Nk / 2 + 1;
         free(h2);
         long long jg = (long long)ceil((pl.mn / 2.0 + 4 * pl.fml) * pl.Nb / pl.fi);
         pl.Jg = (int)(Nk / 2 < jg ? Nk / 2 : jg);
@@ -903,11 +1236,13 @@ long long oracle_resample(const double* in, long long frames, int ch, int rate_i
         long long gc = gcdll(pl.c2, pl.fk);
         dd* h = kernel_taps((int)pl.Lk, pl.c2 / gc, pl.fk / gc, beta);
         H = kernel_spectrum(h, (int)pl.Lk, pl.up ? pl.Mb : pl.Nb, (double)pl.Nb);
+        Hn = (pl.up ? pl.Mb : pl.Nb) / 2 + 1;
         free(h);
     }
     double** op = malloc(sizeof(double*) * ch);
     for (int c = 0; c < ch; c++) op[c] = out + (size_t)c * out_cap;
-    engine(&pl, xx, op, ch, H, fast);
+    if (mode == 2) engine_ld(&pl, xx, op, ch, H, Hn);
+    else engine(&pl, xx, op, ch, H, fast);
     (void)P;
     (void)Q;
     fill_info(&pl, info);

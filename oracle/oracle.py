@@ -80,8 +80,13 @@ def plan(frames, channels, rate_in, rate_out, fast=False, length=0.2, beta=40.0,
     return d
 
 
-def resample(x, rate_in, rate_out, fast=False, length=0.2, beta=40.0, block=0, lpc=True, info=None):
-    """Oracle conversion. x: (frames, channels) float64. Returns planar (channels, nout) float64."""
+MODES = {"exact": 0, "fast": 1, "ld": 2}
+
+
+def resample(x, rate_in, rate_out, fast=False, length=0.2, beta=40.0, block=0, lpc=True, info=None, mode=None):
+    """Oracle conversion. x: (frames, channels) float64; mode "exact", "fast" or "ld" (else `fast` decides).
+    Returns planar (channels, nout) float64."""
+    code = MODES[mode] if mode else int(bool(fast))
     x = np.ascontiguousarray(x, dtype=np.float64)
     if x.ndim == 1:
         x = x[:, None]
@@ -89,7 +94,7 @@ def resample(x, rate_in, rate_out, fast=False, length=0.2, beta=40.0, block=0, l
     cap = max(1, nout_of(frames, rate_in, rate_out))
     out = np.zeros((ch, cap), dtype=np.float64)
     inf = np.zeros(16, dtype=np.int64)
-    n = oracle_lib().oracle_resample(_ptr(x), frames, ch, rate_in, rate_out, int(fast), length, beta, block,
+    n = oracle_lib().oracle_resample(_ptr(x), frames, ch, rate_in, rate_out, code, length, beta, block,
                                      int(lpc), _ptr(out), cap, inf.ctypes.data_as(_lp))
     if n < 0:
         raise ValueError(ORACLE_ERRORS.get(n, f"error {n}"))
@@ -164,8 +169,10 @@ def ref_lib():
 
 
 def ref_resample(x, rate_in, rate_out, fast=False, length=0.2, beta=40.0, block=0, lpc=True, threads=0,
-                 stats=None):
-    """The reference library's kbsrc::resample (precision 0 fast / 1 exact). Returns planar (ch, nout)."""
+                 stats=None, mode=None):
+    """The reference library's kbsrc::resample; mode "exact", "fast" or "ld" (else `fast` decides). Returns
+    planar (ch, nout)."""
+    prec = {"fast": 0, "exact": 1, "ld": 2}[mode] if mode else (0 if fast else 1)
     x = np.ascontiguousarray(x, dtype=np.float64)
     if x.ndim == 1:
         x = x[:, None]
@@ -175,7 +182,7 @@ def ref_resample(x, rate_in, rate_out, fast=False, length=0.2, beta=40.0, block=
     plan_ = np.zeros(5, dtype=np.int64)
     secs = np.zeros(2)
     err = ctypes.create_string_buffer(256)
-    n = ref_lib().kbsrc_ref_resample(_ptr(x), frames, ch, rate_in, rate_out, 0 if fast else 1, length, beta,
+    n = ref_lib().kbsrc_ref_resample(_ptr(x), frames, ch, rate_in, rate_out, prec, length, beta,
                                      threads, block, int(lpc), _ptr(out), cap, plan_.ctypes.data_as(_lp),
                                      _ptr(secs), err, 256)
     if n < 0:

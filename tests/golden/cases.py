@@ -63,6 +63,17 @@ CASES = {
     "s_96k_32k001_exact": (("frames", 34, 4000, 1), 96000, 32001, {"mode": "exact"}),
     "s_96k_32k001_fast": (("frames", 35, 4000, 2), 96000, 32001, {"mode": "fast"}),
     "s_22k05_48k001_exact": (("frames", 36, 3000, 1), 22050, 48001, {"mode": "exact"}),
+    # Precision::LongDouble (x87 extended): the same paths in the third arithmetic
+    "s_48k_96k_ld_97": (("frames", 11, 97, 2), 48000, 96000, {"mode": "ld"}),
+    "s_48k_44k1_ld_97": (("frames", 12, 97, 2), 48000, 44100, {"mode": "ld"}),
+    "s_8k_16k_ld_1_len001": (("frames", 13, 1, 2), 8000, 16000, {"mode": "ld", "length": 0.01}),
+    "s_96k_44k1_ld_20000": (("frames", 15, 20000, 2), 96000, 44100, {"mode": "ld"}),
+    "s_44k1_48k_ld_30000": (("frames", 16, 30000, 1), 44100, 48000, {"mode": "ld"}),
+    "s_96k_48k_ld_nolpc": (("frames", 22, 15000, 2), 96000, 48000, {"mode": "ld", "lpc": False}),
+    "s_48k_44k1_ld_empty": (("frames", 27, 0, 1), 48000, 44100, {"mode": "ld"}),
+    "s_44k1_44k101_ld": (("frames", 29, 3000, 1), 44100, 44101, {"mode": "ld"}),
+    "s_22k05_48k001_ld": (("frames", 36, 3000, 1), 22050, 48001, {"mode": "ld"}),
+    "c1_96k_44k1_ld": (("noise", 1, 10, 96000, 2), 96000, 44100, {"mode": "ld"}),
 }
 
 

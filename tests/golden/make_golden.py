@@ -23,7 +23,7 @@ def main():
     out = {}
     for name, (recipe, fi, fo, opts) in CASES.items():
         x = make_input(recipe)
-        y = oracle.ref_resample(x, fi, fo, fast=opts.get("mode") == "fast", length=opts.get("length", 0.2),
+        y = oracle.ref_resample(x, fi, fo, mode=opts.get("mode", "exact"), length=opts.get("length", 0.2),
                                 beta=opts.get("beta", 40.0), block=opts.get("block", 0), lpc=opts.get("lpc", True))
         y = y.astype("<f8", copy=False)
         out[name] = {"sha256": hashlib.sha256(y.tobytes()).hexdigest(), "shape": list(y.shape),

@@ -19,7 +19,7 @@ def cli(*args, binary=None):
     return subprocess.run([binary or kbsrc_b200.CLI, *map(str, args)], capture_output=True, text=True)
 
 
-@pytest.mark.parametrize("idx", range(5))
+@pytest.mark.parametrize("idx", range(6))
 def test_cli_reproduces_reference_pins(tmp_path, pins, idx):
     name, rate, mode, want = pins["cli"][idx]
     src = tmp_path / "in.wav"

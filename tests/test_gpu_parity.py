@@ -37,14 +37,14 @@ def test_matches_reference_bytes(golden, name):
         assert st["isa"] == "sm_100a"
     got = hashlib.sha256(y.astype("<f8").tobytes()).hexdigest()
     if got != golden[name]["sha256"] and is_small(name):
-        want = oracle.resample(x, fi, fo, fast=opts.get("mode") == "fast", length=opts.get("length", 0.2),
+        want = oracle.resample(x, fi, fo, mode=opts.get("mode", "exact"), length=opts.get("length", 0.2),
                                beta=opts.get("beta", 40.0), block=opts.get("block", 0), lpc=opts.get("lpc", True))
         bad = np.argwhere(y != want)
         pytest.fail(f"{len(bad)} samples differ, first {bad[:3].tolist()}, max diff {np.abs(y - want).max():.3e}")
     assert got == golden[name]["sha256"]
 
 
-@pytest.mark.parametrize("idx", range(5))
+@pytest.mark.parametrize("idx", range(6))
 def test_reference_cli_pins_through_api(pins, idx):
     name, rate, mode, want = pins["cli"][idx]
     samples = refinputs.primary97() if name == "primary" else refinputs.subnormal97()

@@ -80,6 +80,14 @@ def test_tiny_inputs(n):
     assert np.all(np.isfinite(y))
 
 
-def test_ld_mode_is_rejected_clearly():
-    with pytest.raises(RuntimeError, match="ld"):
-        kbsrc_b200.resample(np.zeros((100, 1)), 48000, 44100, mode="ld")
+@pytest.mark.parametrize("fi,fo", [(96000, 44100), (44100, 48000), (44100, 44101)])
+def test_ld_agrees_with_exact(fi, fo):
+    """x87 extended (64-bit significand) and double-double (~106 bits) differ only by the extended rounding:
+    well below 1e-15 of full scale at any length."""
+    x = np.random.default_rng(abs(fi - fo)).uniform(-0.5, 0.5, (fi * 3, 2))
+    st = {}
+    a = kbsrc_b200.resample(x, fi, fo, mode="ld", stats=st)
+    b = kbsrc_b200.resample(x, fi, fo, mode="exact")
+    assert st["isa"] == "sm_100a" and a.shape == b.shape
+    assert np.abs(a - b).max() < 1e-15
+    assert not np.array_equal(a, b)  # a different arithmetic really ran

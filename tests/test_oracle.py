@@ -15,12 +15,12 @@ def test_input_wavs_match_reference_pins(pins):
     assert refinputs.sha(refinputs.wav_f64(refinputs.subnormal97())) == pins["subnormal_wav_sha256"]
 
 
-@pytest.mark.parametrize("idx", range(5))
+@pytest.mark.parametrize("idx", range(6))
 def test_oracle_cli_pins(pins, idx):
     name, rate, mode, want = pins["cli"][idx]
     samples = refinputs.primary97() if name == "primary" else refinputs.subnormal97()
     x = np.array(samples).reshape(-1, 2)
-    y = oracle.resample(x, 48000, rate, fast=mode == "fast")
+    y = oracle.resample(x, 48000, rate, mode=mode)
     assert refinputs.sha(refinputs.wav_f64_planar(y, rate)) == want
 
 
@@ -43,7 +43,7 @@ def test_oracle_frame1_pin(pins):
 def test_oracle_matches_golden(golden, name):
     recipe, fi, fo, opts = CASES[name]
     x = make_input(recipe)
-    y = oracle.resample(x, fi, fo, fast=opts.get("mode") == "fast", length=opts.get("length", 0.2),
+    y = oracle.resample(x, fi, fo, mode=opts.get("mode", "exact"), length=opts.get("length", 0.2),
                         beta=opts.get("beta", 40.0), block=opts.get("block", 0), lpc=opts.get("lpc", True))
     assert list(y.shape) == golden[name]["shape"]
     assert hashlib.sha256(y.astype("<f8").tobytes()).hexdigest() == golden[name]["sha256"]
