@@ -33,12 +33,29 @@ sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
 WORKLOADS = {
     "c2_exact": dict(seed=2, seconds=180, rate_in=96000, rate_out=44100, channels=2, mode="exact"),
     "c2_fast": dict(seed=2, seconds=180, rate_in=96000, rate_out=44100, channels=2, mode="fast"),
+    # the split-precision tensor-core form of the same conversion (not byte-identical; error against exact stated)
+    "c2_split": dict(seed=2, seconds=180, rate_in=96000, rate_out=44100, channels=2, mode="split"),
     "c1_exact": dict(seed=1, seconds=10, rate_in=96000, rate_out=44100, channels=2, mode="exact"),
     "c3_exact": dict(sweep=True, seconds=60, rate_in=44100, rate_out=48000, channels=2, mode="exact"),
     # the uneven queue: 256 files, 1-60 s, 1-8 channels, mixed rate pairs, one GPU batch (exact)
     "c4_exact": dict(batch=True, seed=3, files=256, mode="exact"),
 }
 METRIC = "out Msamples/s 96k->44.1k exact (180 s stereo f64, byte-identical to the reference)"
+METRIC_SPLIT = ("out Msamples/s 96k->44.1k split-precision tensor-core form (180 s stereo f64; error against the "
+                "exact output and throughput against the plain exact GPU engine stated)")
+TENSOR_INT8_PEAK_TOPS = 4500.0  # nominal dense int8 of B200; no measured int8 figure exists for this pool
+
+
+def error_stats(y, ref):
+    """Max and RMS of |y - ref|: absolute (and in dB of full scale 1.0), and in float64 ULPs of each ref sample
+    (samples below 2^-10 of the peak left out of the ULP figures)."""
+    d = np.abs(y - ref)
+    mx, rms = float(d.max(initial=0.0)), float(np.sqrt(np.mean(d * d))) if d.size else 0.0
+    big = np.abs(ref) >= np.abs(ref).max(initial=0.0) * 2.0 ** -10
+    u = d[big] / np.spacing(np.abs(ref[big]))
+    db = lambda v: round(20 * np.log10(v), 2) if v > 0 else None
+    return {"max_abs": mx, "rms_abs": rms, "max_db": db(mx), "rms_db": db(rms),
+            "max_ulps": float(u.max(initial=0.0)), "rms_ulps": float(np.sqrt(np.mean(u * u))) if u.size else 0.0}
 
 
 def make_input(w):
@@ -203,11 +220,13 @@ def product_arm(args, w, world, rank, local, pg):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     exact = w["mode"] == "exact"
+    split = w["mode"] == "split"
     x = make_input(w)
     frames, ch = x.shape
     cv = kbsrc_b200.Conversion(x, w["rate_in"], w["rate_out"], mode=w["mode"])
     plan = kbsrc_b200.plan(frames, ch, w["rate_in"], w["rate_out"], w["mode"])
-    work = roofline.conversion_work(plan, ch, exact)
+    work = roofline.conversion_work(plan, ch, exact or split)
+    twork = roofline.split_work(plan, ch) if split else None
     info = cv.engine_info()
     nout = cv.nout
     d_in = torch.from_numpy(x).to(dev)
@@ -296,7 +315,14 @@ def product_arm(args, w, world, rank, local, pg):
     waves = max(1, int(round(launches_per_step[top])))
     tasks_per_launch = work["tasks"] / waves
     traffic = load_traffic().get(args.workload, {}).get(top)
-    if exact:
+    if split:
+        achieved = twork["int8_ops_per_task"][top] * tasks_per_launch / (avg_ms[top] * 1e-3)
+        roof = {"bound": "tensor", "achieved": round(achieved / 1e12, 3), "peak": TENSOR_INT8_PEAK_TOPS,
+                "unit": "TOPS (int8)", "frac": round(achieved / 1e12 / TENSOR_INT8_PEAK_TOPS, 4), "traffic": traffic,
+                "kernel": top, "peak_source": "nominal dense int8 (of nominal; no measured int8 peak on this pool)",
+                "note": "issued int8 MMA operations (M x N x K x 2, padding included) of the top pass per second; "
+                        "the pass is bound by the slicing and recombination on the CUDA cores, not the tensor pipe"}
+    elif exact:
         peaks = fp64_peak()
         peak = max(peaks.values()) if peaks else None
         achieved = work["ops_per_task"][top] * tasks_per_launch / (avg_ms[top] * 1e-3)
@@ -323,11 +349,33 @@ def product_arm(args, w, world, rank, local, pg):
                    "sample": "one full conversion of the workload by the reference built from source, engine "
                              "time (Stats::process_seconds), all host threads",
                    "value_t8": round(c_8["engine_msps"], 3), "whole_call_msps": round(c_all["wall_msps"], 3)}
+    extra = {}
+    if split:  # the comparison the form exists for: accuracy against exact, throughput against plain exact
+        ref = kbsrc_b200.Conversion(x, w["rate_in"], w["rate_out"], mode="exact")
+        fast = kbsrc_b200.Conversion(x, w["rate_in"], w["rate_out"], mode="fast")
+        y_exact, y_fast = ref.run(x), fast.run(x)
+        extra["error_vs_exact"] = {"split": error_stats(got, y_exact), "fast": error_stats(y_fast, y_exact)}
+        d_out2 = torch.empty_like(d_out)
+        p2 = (d_in.data_ptr(), d_head.data_ptr(), d_tail.data_ptr(), d_out2.data_ptr())
+        for _ in range(args.warmup):
+            ref.run_device(*p2, stream=stream)
+        e0.record()
+        for _ in range(args.steps):
+            ref.run_device(*p2, stream=stream)
+        e1.record()
+        torch.cuda.synchronize()
+        ms_exact = e0.elapsed_time(e1)
+        extra["plain_exact_ms_per_step"] = round(ms_exact / args.steps, 4)
+        extra["vs_plain_exact"] = round(ms_exact / ms, 4)
+        extra["int8_ops_per_step"] = twork["int8_ops_total"]
+        ref.close()
+        fast.close()
     line = {
-        "metric": METRIC, "value": round(value, 3), "unit": "Msamples/s", "n_gpus": world, "steps": args.steps,
+        "metric": METRIC_SPLIT if split else METRIC, "value": round(value, 3), "unit": "Msamples/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None,
-        "dtype": "dd (double-double f64 pairs)" if exact else "f64", "data": "synthetic",
+        "dtype": "dd (double-double f64 pairs)" if exact else ("int8 tensor-core slices, f64" if split else "f64"),
+        "data": "synthetic",
         "config": {"workload": args.workload, **w, "tasks": work["tasks"], "block": plan["nb"],
                    "fft_points": [plan["Nb"], plan["Mb"]], "l2": "inputs larger than L2 (276 MB)",
                    "parallelism": f"independent conversions x{world}"},
@@ -342,6 +390,7 @@ def product_arm(args, w, world, rank, local, pg):
         "cpu_baseline": cpu,
         "clocks": sampler.summary(),
         "output_sha256_matches_reference": golden_sha == digest if golden_sha else None,
+        **extra,
     }
     print(json.dumps(line), flush=True)
     cv.close()

@@ -13,6 +13,8 @@ enum class Precision {
     Fast,        // float64 pipeline
     Exact,       // double-double (~106-bit) pipeline
     LongDouble,  // x87 80-bit extended; the GPU emulates its arithmetic in integers, bit for bit
+    SplitTC,     // not in the reference: the Exact plan with its FFT stages as int8 tensor-core contractions
+                 // (split precision); within float64 rounding of Exact, not byte-identical
 };
 
 struct Options {

@@ -29,6 +29,8 @@ extern "C" {
 #define KBSRC_GPU_FAST 0  /* float64 pipeline (reference Precision::Fast) */
 #define KBSRC_GPU_EXACT 1 /* double-double pipeline (reference Precision::Exact) */
 #define KBSRC_GPU_LD 2    /* x87 extended pipeline, emulated in integers (reference Precision::LongDouble) */
+#define KBSRC_GPU_SPLIT 3 /* split-precision form: tensor-core int8 DFT contractions, float64 elsewhere; not
+                             byte-identical, within float64 rounding of exact (no reference counterpart) */
 
 typedef struct kbsrc_gpu_engine kbsrc_gpu_engine;
 
@@ -37,7 +39,7 @@ typedef struct kbsrc_gpu_engine kbsrc_gpu_engine;
  * `lead` zeros/edge samples before input frame 0 (lead = marg*Q + pre), and writes output samples
  * [b*hop*P - o, (b+1)*hop*P - o) clipped to [0, nout). */
 typedef struct {
-    int precision;      /* KBSRC_GPU_FAST, KBSRC_GPU_EXACT or KBSRC_GPU_LD */
+    int precision;      /* KBSRC_GPU_FAST, KBSRC_GPU_EXACT, KBSRC_GPU_LD or KBSRC_GPU_SPLIT */
     int channels;       /* >= 1 */
     long long P, Q;     /* reduced rate ratio rate_out/rate_in = P/Q */
     int nb;             /* block size factor: forward FFT nb*Q points, inverse nb*P */

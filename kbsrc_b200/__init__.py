@@ -156,7 +156,7 @@ def _ptr(a):
 
 
 def _options(mode, length, beta, block, lpc, threads):
-    prec = {"fast": 0, "exact": 1, "ld": 2}[mode] if isinstance(mode, str) else int(mode)
+    prec = {"fast": 0, "exact": 1, "ld": 2, "split": 3}[mode] if isinstance(mode, str) else int(mode)
     return Options(prec, float(length), float(beta), int(threads), int(block), int(bool(lpc)))
 
 

@@ -18,6 +18,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdlib>
 #include <cstring>
 #include <memory>
@@ -31,6 +32,7 @@
 #include "dd.cuh"
 #include "fft.cuh"
 #include "kbsrc_gpu.h"
+#include "tcfft.cuh"
 
 using namespace kbsrc::dev;
 namespace hd = kbsrc::host;
@@ -513,6 +515,124 @@ __global__ void k_design_out(const __grid_constant__ SpecParams<ArDDAccurate> P)
 }
 
 // ------------------------------------------------------------------------------------------------------
+// split-precision form: the four-step passes with tensor-core sub-FFTs (tcfft.cuh), float64 everywhere else
+// ------------------------------------------------------------------------------------------------------
+struct TcParams {
+    TcSub sub;
+    const double2* tw4;  // four-step twiddles [k1 * N2 + n2] of the column pass (null: none)
+    int N1, N2;
+    int slots;           // task slots of the launch (items = groups x slots)
+    int* err;            // set when a tensor-core stage timed out
+};
+
+// Column pass, persistent: each CTA sets up its tensor memory and tables once, then takes items (column group
+// g, task slot y) in turn, item = y * groups + g. An item: sequences n2 in [c0, c0+F) of length N1 (stride N2),
+// the sub-FFT, the four-step twiddle, stored in place; with N2 == 1 the single column is the whole transform and
+// DST may write it as output samples.
+template <int SRC, int DST>
+__global__ void __launch_bounds__(kTcThreads, 1)
+    k_tc_column(const __grid_constant__ PassParams<ArF64> P, const __grid_constant__ TcParams T) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    using C = CxR<ArF64>;
+    const int F = T.sub.F, N1 = T.N1, N2 = T.N2, total = N1 * F, groups = (N2 + F - 1) / F;
+    Planes<ArF64> A, B;
+    const TcSmem m = tc_carve(carve<ArF64>(smem, total, A, B), T.sub);
+    const uint32_t tmem = tc_setup(m, T.sub);
+    uint32_t phase = 0;
+    for (long long item = blockIdx.x; item < (long long)groups * T.slots; item += gridDim.x) {
+        const int slot = (int)(item / groups), c0 = (int)(item - (long long)slot * groups) * F;
+        const long long task = P.task0 + slot;
+        const C* src = P.src + slot * P.stride;
+        C* dst = P.dst + slot * P.stride;
+        const TaskSource ts = SRC == kSrcSignal ? task_source(P.work, task, 2LL * N1 * N2) : TaskSource{};
+        for (int e0 = threadIdx.x; e0 < total; e0 += kLoadBatch * blockDim.x) {
+            C v[kLoadBatch];
+#pragma unroll
+            for (int j = 0; j < kLoadBatch; j++) {
+                const int e = e0 + j * blockDim.x, r = e / F, n2 = c0 + (e - r * F);
+                if (e < total)
+                    v[j] = n2 < N2 ? load_input<ArF64, SRC>(P, ts, src, (long long)r * N2 + n2) : czero<ArF64>();
+            }
+#pragma unroll
+            for (int j = 0; j < kLoadBatch; j++)
+                if (e0 + j * blockDim.x < total) A.st(e0 + j * blockDim.x, v[j]);
+        }
+        __syncthreads();
+        tc_subfft(T.sub, A, B, m, tmem, phase, T.err);
+        const TaskRef tr = DST == kDstOutput ? task_ref(P.work, task) : TaskRef{0, 0, 0};
+        const Item it = DST == kDstOutput ? item_of(P.work, tr) : Item{};
+        for (int e = threadIdx.x; e < total; e += blockDim.x) {
+            const int k1 = e / F, n2 = c0 + (e - k1 * F);
+            if (n2 >= N2) continue;
+            C v = A.ld(e);
+            if (DST == kDstComplex) {
+                if (T.tw4) {
+                    const double2 w = __ldg(T.tw4 + (long long)k1 * N2 + n2);
+                    v = c_mulw<ArF64>(v, CxW<ArF64>{w.x, w.y});
+                }
+                dst[(long long)k1 * N2 + n2] = v;
+            } else {
+                emit(P.work, it, tr.c, tr.b, 2LL * k1, v.re);
+                emit(P.work, it, tr.c, tr.b, 2LL * k1 + 1, -v.im);
+            }
+        }
+        __syncthreads();
+    }
+    tc_teardown(T.sub, tmem);
+}
+
+// Row pass, persistent like the column pass: items (row group g, task slot y); an item transforms rows r in
+// [r0, r0+F) of length N2 and stores them transposed to [N1*k2 + r], or writes them as output samples.
+template <int DST>
+__global__ void __launch_bounds__(kTcThreads, 1)
+    k_tc_row(const __grid_constant__ PassParams<ArF64> P, const __grid_constant__ TcParams T) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    using C = CxR<ArF64>;
+    const int F = T.sub.F, N1 = T.N1, N2 = T.N2, total = N2 * F, groups = (N1 + F - 1) / F;
+    Planes<ArF64> A, B;
+    const TcSmem m = tc_carve(carve<ArF64>(smem, total, A, B), T.sub);
+    const uint32_t tmem = tc_setup(m, T.sub);
+    uint32_t phase = 0;
+    for (long long item = blockIdx.x; item < (long long)groups * T.slots; item += gridDim.x) {
+        const int slot = (int)(item / groups), r0 = (int)(item - (long long)slot * groups) * F;
+        const long long task = P.task0 + slot;
+        const C* src = P.src + slot * P.stride;
+        for (int e0 = threadIdx.x; e0 < total; e0 += kLoadBatch * blockDim.x) {
+            C v[kLoadBatch];
+#pragma unroll
+            for (int j = 0; j < kLoadBatch; j++) {
+                const int e = e0 + j * blockDim.x, f = e / N2, i = e - f * N2, row = r0 + f;
+                if (e < total) v[j] = row < N1 ? src[(long long)row * N2 + i] : czero<ArF64>();
+            }
+#pragma unroll
+            for (int j = 0; j < kLoadBatch; j++) {
+                const int e = e0 + j * blockDim.x, f = e / N2, i = e - f * N2;
+                if (e < total) A.st(i * F + f, v[j]);
+            }
+        }
+        __syncthreads();
+        tc_subfft(T.sub, A, B, m, tmem, phase, T.err);
+        C* dst = P.dst + slot * P.stride;
+        const TaskRef tr = DST == kDstOutput ? task_ref(P.work, task) : TaskRef{0, 0, 0};
+        const Item it = DST == kDstOutput ? item_of(P.work, tr) : Item{};
+        for (int e = threadIdx.x; e < total; e += blockDim.x) {
+            const int k2 = e / F, f = e - k2 * F, row = r0 + f;
+            if (row >= N1) continue;
+            const C v = A.ld(e);
+            const long long iz = (long long)N1 * k2 + row;
+            if (DST == kDstComplex) {
+                dst[iz] = v;
+            } else {
+                emit(P.work, it, tr.c, tr.b, 2 * iz, v.re);
+                emit(P.work, it, tr.c, tr.b, 2 * iz + 1, -v.im);
+            }
+        }
+        __syncthreads();
+    }
+    tc_teardown(T.sub, tmem);
+}
+
+// ------------------------------------------------------------------------------------------------------
 // host side: FFT plans and tables (built in dd on the host, as the reference builds them)
 // ------------------------------------------------------------------------------------------------------
 struct HostCx {
@@ -775,6 +895,151 @@ int make_dev_cfft(int n, int tab, int fmax, DevCfft& d, cudaStream_t st) {
     return KBSRC_GPU_OK;
 }
 
+// ------------------------------------------------------------------------------------------------------
+// split-precision plans: n = N1 * N2 (four-step, or N2 = 1 for one direct sub-FFT), each sub-FFT N = Ra * Rb
+// with radices <= 32, so that every stage is one tcgen05 contraction with K, N <= 64.
+// ------------------------------------------------------------------------------------------------------
+// Ra * Rb = N with both <= 32, Ra the largest such divisor <= sqrt(N); false when there is none.
+bool tc_factor(int N, int& Ra, int& Rb) {
+    int best = 0;
+    for (int a = 1; a <= 32 && a * a <= N; a++)
+        if (N % a == 0 && N / a <= 32) best = a;
+    if (!best) return false;
+    Ra = best;
+    Rb = N / best;
+    return true;
+}
+int tc_kh(int R) { return R <= 16 ? 16 : 32; }
+int tc_nh(int R) { return R <= 16 ? 16 : R <= 24 ? 24 : 32; }
+
+// The real form of DFT_R (outputs n: real parts, then imaginary parts from nh; inputs k: real parts, then
+// imaginary parts from kh), y_re[k1] = sum_j xr_j cos + xi_j sin, y_im[k1] = sum_j xi_j cos - xr_j sin with the
+// angle 2 pi j k1 / R, each entry halved and cut into kTcSlices signed 7-bit slices of floor(|w| 2^55).
+void tc_matrix(int R, std::vector<unsigned char>& out) {
+    const int kh = tc_kh(R), nh = tc_nh(R), kpad = 2 * kh, npad = 2 * nh;
+    const size_t base = out.size();
+    out.resize(base + (size_t)kTcSlices * npad * kpad, 0);
+    auto put = [&](int n, int k, double w) {
+        const unsigned long long v = (unsigned long long)(std::fabs(w) * 36028797018963968.0);  // |w| 2^55, exact
+        for (int i = 0; i < kTcSlices; i++) {
+            int sl = (int)((v >> (49 - 7 * i)) & 127);
+            if (w < 0) sl = -sl;
+            out[base + (size_t)i * npad * kpad + umma_off(n, k, kpad)] = (unsigned char)(signed char)sl;
+        }
+    };
+    hd::RootTable rt(R);
+    for (int k1 = 0; k1 < R; k1++)
+        for (int j = 0; j < R; j++) {
+            hd::dd c, sn;
+            rt.get((long long)j * k1, c, sn);
+            put(k1, j, c.hi);
+            put(k1, kh + j, sn.hi);
+            put(nh + k1, j, -sn.hi);
+            put(nh + k1, kh + j, c.hi);
+        }
+}
+
+// A transform of n points in the split form, resident on the device.
+struct TcFftDev {
+    int n = 0, N1 = 0, N2 = 0;
+    int ctas = 148;  // persistent CTAs per pass: one per SM
+    TcSub col{}, row{};
+    size_t smem_col = 0, smem_row = 0;
+    DevBuf tw4, tw_in, mats;
+    size_t bytes() const { return tw4.bytes + tw_in.bytes + mats.bytes; }
+};
+
+// Sub-FFT of N points over `count` sequences: radices, sequences per CTA within the shared-memory limit
+int tc_sub_plan(int N, int count, TcSub& sub, size_t& smem) {
+    int Ra, Rb;
+    if (!tc_factor(N, Ra, Rb)) return fail(KBSRC_GPU_E_UNSUPPORTED, "split-precision form: no radix-32 factorisation");
+    sub = TcSub{};
+    sub.N = N;
+    sub.a = TcRadix{Ra, tc_kh(Ra), tc_nh(Ra), nullptr};
+    sub.b = TcRadix{Rb, tc_kh(Rb), tc_nh(Rb), nullptr};
+    sub.ncols = 512;  // kTcAcc accumulators of up to 48 columns (or 32 per round): more than 256
+    int F = std::max(1, std::min(kTcRows / std::max(Ra, Rb), count));
+    for (;; F--) {
+        sub.F = F;
+        smem = 2 * (size_t)N * F * 16 + tc_smem_bytes(sub);
+        if (smem <= 227 * 1024 || F == 1) break;
+    }
+    if (smem > 227 * 1024) return fail(KBSRC_GPU_E_UNSUPPORTED, "split-precision form: sub-FFT too large");
+    return KBSRC_GPU_OK;
+}
+
+int make_tc_fft(int n, TcFftDev& t) {
+    int rc, a, b, dev = 0;
+    KB_CUDA(cudaGetDevice(&dev));
+    KB_CUDA(cudaDeviceGetAttribute(&t.ctas, cudaDevAttrMultiProcessorCount, dev));
+    t.n = n;
+    t.N1 = t.N2 = 0;
+    if (n <= 1024 && tc_factor(n, a, b)) {
+        t.N1 = n;
+        t.N2 = 1;
+    } else {
+        for (int N1 = (int)std::sqrt((double)n) + 1; N1 >= 2; N1--) {
+            if ((long long)N1 * N1 > n || n % N1) continue;
+            const int N2 = n / N1;
+            if (N2 <= 1024 && tc_factor(N1, a, b) && tc_factor(N2, a, b)) {
+                t.N1 = N1;
+                t.N2 = N2;
+                break;
+            }
+        }
+    }
+    if (!t.N1)
+        return fail(KBSRC_GPU_E_UNSUPPORTED, "split-precision form: transform length " + std::to_string(n) +
+                                                 " has no factorisation into radices <= 32");
+    if ((rc = tc_sub_plan(t.N1, t.N2, t.col, t.smem_col)) != KBSRC_GPU_OK) return rc;
+    if (t.N2 > 1 && (rc = tc_sub_plan(t.N2, t.N1, t.row, t.smem_row)) != KBSRC_GPU_OK) return rc;
+    // sliced matrices of the (up to four) radices, the inner twiddles of each sub-FFT, and the four-step twiddles
+    std::vector<unsigned char> mats;
+    size_t off[4];
+    TcRadix* rads[4] = {&t.col.a, &t.col.b, &t.row.a, &t.row.b};
+    const int nr = t.N2 > 1 ? 4 : 2;
+    for (int i = 0; i < nr; i++) {
+        off[i] = mats.size();
+        tc_matrix(rads[i]->R, mats);
+    }
+    if ((rc = t.mats.alloc(mats.size())) != KBSRC_GPU_OK) return rc;
+    KB_CUDA(cudaMemcpy(t.mats.p, mats.data(), mats.size(), cudaMemcpyHostToDevice));
+    for (int i = 0; i < nr; i++)
+        rads[i]->slices = reinterpret_cast<const uint4*>(static_cast<unsigned char*>(t.mats.p) + off[i]);
+    std::vector<double> tw;
+    auto inner = [&](const TcSub& sub) {  // [k1 * Rb + m] = e^{-2 pi i m k1 / N}
+        hd::RootTable rt(sub.N);
+        for (int k1 = 0; k1 < sub.a.R; k1++)
+            for (int m = 0; m < sub.b.R; m++) {
+                hd::dd c, sn;
+                rt.get(-(long long)m * k1, c, sn);
+                tw.push_back(c.hi);
+                tw.push_back(sn.hi);
+            }
+    };
+    inner(t.col);
+    const size_t row_off = tw.size();
+    if (t.N2 > 1) inner(t.row);
+    if ((rc = t.tw_in.alloc(tw.size() * sizeof(double))) != KBSRC_GPU_OK) return rc;
+    KB_CUDA(cudaMemcpy(t.tw_in.p, tw.data(), tw.size() * sizeof(double), cudaMemcpyHostToDevice));
+    t.col.tw = static_cast<const double2*>(t.tw_in.p);
+    if (t.N2 > 1) {
+        t.row.tw = reinterpret_cast<const double2*>(static_cast<double*>(t.tw_in.p) + row_off);
+        std::vector<double> w4(2 * (size_t)n);
+        hd::RootTable rt(n);
+        for (int k1 = 0; k1 < t.N1; k1++)
+            for (int n2 = 0; n2 < t.N2; n2++) {
+                hd::dd c, sn;
+                rt.get(-(long long)k1 * n2, c, sn);
+                w4[2 * ((size_t)k1 * t.N2 + n2)] = c.hi;
+                w4[2 * ((size_t)k1 * t.N2 + n2) + 1] = sn.hi;
+            }
+        if ((rc = t.tw4.alloc(w4.size() * sizeof(double))) != KBSRC_GPU_OK) return rc;
+        KB_CUDA(cudaMemcpy(t.tw4.p, w4.data(), w4.size() * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    return KBSRC_GPU_OK;
+}
+
 int env_int(const char* name, int dflt) {
     const char* v = std::getenv(name);
     return v && *v ? std::atoi(v) : dflt;
@@ -790,6 +1055,9 @@ int env_int(const char* name, int dflt) {
 struct PlanCore {
     kbsrc_gpu_desc d{};  // the shape (H is not kept)
     bool exact = false;
+    bool split = false;        // split-precision form: tfw / tiv instead of fw / iv
+    TcFftDev tfw, tiv;
+    DevBuf tc_err;             // int: a tensor-core stage timed out
     int tab = 0;  // TabFmt of the tables and of the values in the work buffers
     int Nb = 0, Mb = 0, hf = 0, hi = 0, hop = 0;
     DevCfft fw, iv;
@@ -894,6 +1162,11 @@ int allow_large_smem() {
     KB_SMEM((k_direct<ArX80, kSrcSignal, kDstComplex>));
     KB_SMEM((k_direct<ArX80, kSrcComplex, kDstComplex>));
     KB_SMEM((k_direct<ArX80, kSrcComplex, kDstOutput>));
+    KB_SMEM((k_tc_column<kSrcSignal, kDstComplex>));
+    KB_SMEM((k_tc_column<kSrcComplex, kDstComplex>));
+    KB_SMEM((k_tc_column<kSrcComplex, kDstOutput>));
+    KB_SMEM((k_tc_row<kDstComplex>));
+    KB_SMEM((k_tc_row<kDstOutput>));
 #undef KB_SMEM
     if (dev < 64) done[dev] = true;
     return KBSRC_GPU_OK;
@@ -1111,8 +1384,78 @@ int enqueue_plan(const PlanCore& pc, const Work& work, long long t_begin, long l
     return KBSRC_GPU_OK;
 }
 
+// One split-form transform of every slot: column pass (x in place, or straight to y / the output when N2 == 1),
+// then the row pass x -> y or to the output epilogue (DST).
+template <int SRC, int DST>
+int launch_tc(const TcFftDev& t, const Slots& sl, void* x, void* y, int* err, cudaStream_t st, Trail& tr, int kA,
+              int kB) {
+    PassParams<ArF64> p{};
+    p.src = static_cast<CxR<ArF64>*>(x);
+    p.dst = static_cast<CxR<ArF64>*>(t.N2 == 1 ? y : x);
+    p.stride = sl.stride;
+    p.task0 = sl.task0;
+    p.work = sl.work;
+    TcParams T{};
+    T.sub = t.col;
+    T.tw4 = t.N2 > 1 ? static_cast<const double2*>(t.tw4.p) : nullptr;
+    T.N1 = t.N1;
+    T.N2 = t.N2;
+    T.slots = (int)sl.nt;
+    T.err = err;
+    auto grid = [&](long long items) { return (unsigned)std::max(1LL, std::min(items, (long long)t.ctas)); };
+    if (t.N2 == 1) {
+        k_tc_column<SRC, DST><<<grid(sl.nt), kTcThreads, t.smem_col, st>>>(p, T);
+        return tr.mark(st, kA);
+    }
+    k_tc_column<SRC, kDstComplex>
+        <<<grid((long long)((t.N2 + t.col.F - 1) / t.col.F) * sl.nt), kTcThreads, t.smem_col, st>>>(p, T);
+    int rc = tr.mark(st, kA);
+    if (rc) return rc;
+    p.src = static_cast<CxR<ArF64>*>(x);
+    p.dst = static_cast<CxR<ArF64>*>(y);
+    T.sub = t.row;
+    T.tw4 = nullptr;
+    k_tc_row<DST><<<grid((long long)((t.N1 + t.row.F - 1) / t.row.F) * sl.nt), kTcThreads, t.smem_row, st>>>(p, T);
+    return tr.mark(st, kB);
+}
+
+// The block loop in the split-precision form: tensor-core transforms, float64 split, spectrum and merge.
+int enqueue_split(const PlanCore& pc, const Work& work, long long t_begin, long long t_end, void* a, void* b,
+                  long long stride, long long wave, cudaStream_t st, Trail& tr) {
+    const kbsrc_gpu_desc& d = pc.d;
+    int* err = static_cast<int*>(pc.tc_err.p);
+    Slots sl{};
+    sl.stride = stride;
+    sl.work = work;
+    int rc;
+    for (long long t0 = t_begin; t0 < t_end; t0 += wave) {
+        sl.task0 = t0;
+        sl.nt = (unsigned)std::min(wave, t_end - t0);
+        if ((rc = launch_tc<kSrcSignal, kDstComplex>(pc.tfw, sl, a, b, err, st, tr, kFwdA, kFwdB)) != KBSRC_GPU_OK)
+            return rc;
+        SpecParams<ArF64> s{};
+        s.Z = static_cast<CxR<ArF64>*>(b);
+        s.X = static_cast<CxR<ArF64>*>(a);
+        s.Zi = static_cast<CxR<ArF64>*>(b);
+        s.stride = stride;
+        s.w_fw = static_cast<const CxW<ArF64>*>(pc.w_fw.p);
+        s.w_iv = static_cast<const CxW<ArF64>*>(pc.w_iv.p);
+        s.H = static_cast<const double*>(pc.H.p);
+        s.h = pc.hf; s.hi = pc.hi; s.Nb = pc.Nb; s.Mb = pc.Mb; s.up = d.up; s.Jg = d.Jg;
+        k_split<ArF64><<<dim3(grid_for(pc.hf, 256), sl.nt), 256, 0, st>>>(s);
+        if ((rc = tr.mark(st, kSplit)) != KBSRC_GPU_OK) return rc;
+        k_merge<ArF64><<<dim3(grid_for(pc.hi, 256), sl.nt), 256, 0, st>>>(s);
+        if ((rc = tr.mark(st, kMerge)) != KBSRC_GPU_OK) return rc;
+        if ((rc = launch_tc<kSrcComplex, kDstOutput>(pc.tiv, sl, b, nullptr, err, st, tr, kInvA, kInvB)) !=
+            KBSRC_GPU_OK)
+            return rc;
+    }
+    return KBSRC_GPU_OK;
+}
+
 int enqueue_any(const PlanCore& pc, const Work& work, long long t_begin, long long t_end, void* a, void* b,
                 long long stride, long long wave, cudaStream_t st, Trail& tr) {
+    if (pc.split) return enqueue_split(pc, work, t_begin, t_end, a, b, stride, wave, st, tr);
     if (pc.tab == kTabX80) return enqueue_plan<ArX80, ArX80>(pc, work, t_begin, t_end, a, b, stride, wave, st, tr);
     if (pc.exact) return enqueue_plan<ArDDShort, ArDDAccurate>(pc, work, t_begin, t_end, a, b, stride, wave, st, tr);
     return enqueue_plan<ArF64, ArF64>(pc, work, t_begin, t_end, a, b, stride, wave, st, tr);
@@ -1138,9 +1481,30 @@ size_t cfft_bytes(const DevCfft& c) {
     return c.m ? b + cfft_bytes(*c.inner) : b;
 }
 
+// Kernel launches of one wave, and the device bytes of the plan's tables
+long long plan_launches(const PlanCore& pc) {
+    if (pc.split) return (pc.tfw.N2 > 1 ? 2 : 1) + 2 + (pc.tiv.N2 > 1 ? 2 : 1);
+    return cfft_launches(pc.fw) + 2 + cfft_launches(pc.iv);
+}
+size_t plan_table_bytes(const PlanCore& pc) {
+    return cfft_bytes(pc.fw) + cfft_bytes(pc.iv) + pc.tfw.bytes() + pc.tiv.bytes() + pc.w_fw.bytes + pc.w_iv.bytes +
+           pc.H.bytes;
+}
+
+// After a synchronous run of the split form: a tensor-core stage that timed out is an error (the flag is reset)
+int check_tc(const PlanCore& pc) {
+    if (!pc.split || !pc.tc_err.p) return KBSRC_GPU_OK;
+    int flag = 0;
+    KB_CUDA(cudaMemcpy(&flag, pc.tc_err.p, sizeof flag, cudaMemcpyDeviceToHost));
+    if (!flag) return KBSRC_GPU_OK;
+    KB_CUDA(cudaMemset(pc.tc_err.p, 0, sizeof flag));
+    return fail(KBSRC_GPU_E_CUDA, "split-precision form: a tensor-core stage did not complete");
+}
+
 int check_desc(const kbsrc_gpu_desc* d) {
     if (!d) return fail(KBSRC_GPU_E_ARG, "null descriptor");
-    if (d->precision != KBSRC_GPU_FAST && d->precision != KBSRC_GPU_EXACT && d->precision != KBSRC_GPU_LD)
+    if (d->precision != KBSRC_GPU_FAST && d->precision != KBSRC_GPU_EXACT && d->precision != KBSRC_GPU_LD &&
+        d->precision != KBSRC_GPU_SPLIT)
         return fail(KBSRC_GPU_E_ARG, "precision");
     if (d->channels < 1 || d->P < 1 || d->Q < 1 || d->nb < 2 || d->nb % 2 || d->marg < 0 || d->nb <= 2 * d->marg)
         return fail(KBSRC_GPU_E_ARG, "bad plan shape");
@@ -1179,15 +1543,25 @@ int make_core(const kbsrc_gpu_desc* desc, PlanCore& pc, cudaStream_t st) {
     pc.d = *desc;
     pc.d.H = nullptr;
     pc.exact = desc->precision == KBSRC_GPU_EXACT;
-    pc.tab = desc->precision == KBSRC_GPU_FAST ? kTabF64 : desc->precision == KBSRC_GPU_EXACT ? kTabDD : kTabX80;
+    pc.split = desc->precision == KBSRC_GPU_SPLIT;
+    pc.tab = desc->precision == KBSRC_GPU_FAST || pc.split ? kTabF64
+             : desc->precision == KBSRC_GPU_EXACT          ? kTabDD
+                                                           : kTabX80;
     pc.Nb = (int)(desc->nb * desc->Q);
     pc.Mb = (int)(desc->nb * desc->P);
     pc.hf = pc.Nb / 2;
     pc.hi = pc.Mb / 2;
     pc.hop = desc->nb - 2 * desc->marg;
     const int fmax = env_int("KBSRC_GPU_FMAX", pc.tab == kTabF64 ? 16 : 8);
-    if ((rc = make_dev_cfft(pc.hf, pc.tab, fmax, pc.fw, st)) != KBSRC_GPU_OK) return rc;
-    if ((rc = make_dev_cfft(pc.hi, pc.tab, fmax, pc.iv, st)) != KBSRC_GPU_OK) return rc;
+    if (pc.split) {
+        if ((rc = make_tc_fft(pc.hf, pc.tfw)) != KBSRC_GPU_OK) return rc;
+        if ((rc = make_tc_fft(pc.hi, pc.tiv)) != KBSRC_GPU_OK) return rc;
+        if ((rc = pc.tc_err.alloc(16)) != KBSRC_GPU_OK) return rc;
+        KB_CUDA(cudaMemset(pc.tc_err.p, 0, 16));
+    } else {
+        if ((rc = make_dev_cfft(pc.hf, pc.tab, fmax, pc.fw, st)) != KBSRC_GPU_OK) return rc;
+        if ((rc = make_dev_cfft(pc.hi, pc.tab, fmax, pc.iv, st)) != KBSRC_GPU_OK) return rc;
+    }
     if ((rc = upload_cx(split_roots(pc.Nb), pc.tab, pc.w_fw)) != KBSRC_GPU_OK) return rc;
     if ((rc = upload_cx(split_roots(pc.Mb), pc.tab, pc.w_iv)) != KBSRC_GPU_OK) return rc;
     return upload_real(desc->H, desc->H_len, pc.tab, pc.H);
@@ -1594,6 +1968,7 @@ int kbsrc_gpu_engine_run_device_timed(kbsrc_gpu_engine* e, const double* d_in, c
             if (pass_launches) pass_launches[k] = 0;
         }
         if (tr.n > 0) KB_CUDA(cudaEventSynchronize(e->events[tr.n - 1]));
+        if ((rc = check_tc(*e)) != KBSRC_GPU_OK) return rc;
         for (size_t i = 1; i < tr.n; i++) {
             float ms = 0;
             KB_CUDA(cudaEventElapsedTime(&ms, e->events[i - 1], e->events[i]));
@@ -1678,7 +2053,7 @@ int kbsrc_gpu_engine_run_host(kbsrc_gpu_engine* e, const double* in, const doubl
         KB_CUDA(cudaStreamSynchronize(hs));
         KB_CUDA(cudaStreamSynchronize(cs));
         KB_CUDA(cudaStreamSynchronize(ds));
-        return KBSRC_GPU_OK;
+        return check_tc(*e);
     } catch (const std::exception& x) {
         return fail(KBSRC_GPU_E_CUDA, x.what());
     }
@@ -1763,12 +2138,11 @@ int kbsrc_gpu_engine_info(const kbsrc_gpu_engine* e, long long* tasks, long long
     if (!e) return fail(KBSRC_GPU_E_ARG, "null engine");
     if (tasks) *tasks = e->tasks;
     if (launches) {
-        const long long per_wave = cfft_launches(e->fw) + 2 + cfft_launches(e->iv);
+        const long long per_wave = plan_launches(*e);
         *launches = e->tasks ? per_wave * ((e->tasks + e->wave - 1) / e->wave) : 0;
     }
     if (device_bytes) {
-        *device_bytes = (long long)(cfft_bytes(e->fw) + cfft_bytes(e->iv) + e->w_fw.bytes + e->w_iv.bytes +
-                                    e->H.bytes + e->bufA.bytes + e->bufB.bytes + e->d_in.bytes + e->d_head.bytes +
+        *device_bytes = (long long)(plan_table_bytes(*e) + e->bufA.bytes + e->bufB.bytes + e->d_in.bytes + e->d_head.bytes +
                                     e->d_tail.bytes + e->d_out.bytes);
     }
     return KBSRC_GPU_OK;
@@ -2000,7 +2374,7 @@ int kbsrc_gpu_batch_info(const kbsrc_gpu_batch* b, long long* groups, long long*
     long long t = 0, l = 0;
     for (const auto& g : b->groups) {
         t += g->tasks;
-        l += (cfft_launches(g->fw) + 2 + cfft_launches(g->iv)) * ((g->tasks + g->wave - 1) / g->wave);
+        l += plan_launches(*g) * ((g->tasks + g->wave - 1) / g->wave);
     }
     if (groups) *groups = (long long)b->groups.size();
     if (tasks) *tasks = t;

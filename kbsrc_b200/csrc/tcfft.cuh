@@ -1,0 +1,273 @@
+// Split-precision DFT on the tensor cores: each stage of a sub-FFT is a dense DFT-matrix contraction of int8
+// slices on tcgen05, accumulated exactly in int32 in TMEM and recombined in float64.
+//
+// A stage transforms up to 128 row vectors of R complex float64 values. Each row is scaled by its own power of
+// two 2^E (the smallest above every |value| of the row) and cut into kTcSlices signed 7-bit slices,
+//     x = 2^E * sum_i a_i 2^(-7(i+1)),  a_i in [-127, 127]   (56 bits: every float64 digit of the row's maximum),
+// and the real form of the DFT_R matrix W (entries cos and +-sin, |w| <= 1) is cut the same way after halving,
+// w = 2 * sum_j b_j 2^(-7(j+1)). The products a_i b_j with i + j = d accumulate exactly in int32 accumulator d
+// for d <= 8 (43 of the 64 products; the dropped ones sum to below 2^-60 of the row's scale per term), and
+//     y = 2^(E+1) * sum_d C_d 2^(-7(d+2))
+// is formed from two exact int64 Horner sums, two exact conversions and one rounded float64 addition. The
+// result is within float64 rounding of the exact stage output: the accuracy of a float64 engine, not the bit
+// pattern of any reference engine.
+//
+// Shared-memory operands use the canonical K-major layout of tc.cuh: K = [real half | imaginary half] of 2*kh
+// bytes, N = [real outputs | imaginary outputs] of 2*nh columns.
+#pragma once
+#include "fft.cuh"
+#include "tc.cuh"
+
+namespace kbsrc::dev {
+
+constexpr int kTcSlices = 8;
+constexpr int kTcAcc = kTcSlices + 1;  // accumulators d = i + j = 0..8: the triangle plus its first diagonal
+constexpr int kTcRows = 128;          // MMA M: row vectors per stage
+constexpr int kTcThreads = 256;       // two threads per row while slicing; two warpgroups while recombining
+constexpr int kTcWaitLimit = 1 << 22; // mbarrier polls before a stage reports a timeout
+
+// One radix of the split form: the sliced real DFT_R matrix (global memory, kTcSlices * 2nh * 2kh bytes).
+struct TcRadix {
+    int R, kh, nh;
+    const uint4* slices;
+};
+
+// A sub-FFT of N = a.R * b.R points on F sequences per CTA (F * max(a.R, b.R) <= 128); tw[k1 * b.R + m] =
+// e^{-2 pi i m k1 / N}; ncols: TMEM columns to allocate.
+struct TcSub {
+    int N, F, ncols;
+    TcRadix a, b;
+    const double2* tw;
+};
+
+// Per-CTA shared memory of the split form after the two data plane pairs.
+struct TcSmem {
+    unsigned char* slices;  // kTcSlices * 128 * kpad_max
+    unsigned char* bm_a;    // sliced DFT matrices
+    unsigned char* bm_b;
+    double2* tw;            // N inner twiddles
+    int* emax;              // row exponents (two per row while slicing)
+    uint64_t* mbar;
+    uint32_t* tmem_slot;
+};
+
+__host__ __device__ inline int tc_bm_bytes(const TcRadix& r) { return kTcSlices * (2 * r.nh) * (2 * r.kh); }
+__host__ __device__ inline size_t tc_align(size_t v) { return (v + 127) & ~(size_t)127; }
+
+// Shared bytes the split-form part of a CTA needs after its data planes.
+__host__ __device__ inline size_t tc_smem_bytes(const TcSub& s) {
+    const int kpad = 2 * (s.a.kh > s.b.kh ? s.a.kh : s.b.kh);
+    return tc_align((size_t)kTcSlices * kTcRows * kpad) + tc_align(tc_bm_bytes(s.a)) + tc_align(tc_bm_bytes(s.b)) +
+           tc_align((size_t)s.N * 16) + tc_align(2 * kTcRows * 4) + 128;
+}
+
+__device__ inline TcSmem tc_carve(unsigned char* p, const TcSub& s) {
+    TcSmem m;
+    const int kpad = 2 * (s.a.kh > s.b.kh ? s.a.kh : s.b.kh);
+    m.slices = p;
+    p += tc_align((size_t)kTcSlices * kTcRows * kpad);
+    m.bm_a = p;
+    p += tc_align(tc_bm_bytes(s.a));
+    m.bm_b = p;
+    p += tc_align(tc_bm_bytes(s.b));
+    m.tw = reinterpret_cast<double2*>(p);
+    p += tc_align((size_t)s.N * 16);
+    m.emax = reinterpret_cast<int*>(p);
+    p += tc_align(2 * kTcRows * 4);
+    m.mbar = reinterpret_cast<uint64_t*>(p);
+    m.tmem_slot = reinterpret_cast<uint32_t*>(p + 8);
+    return m;
+}
+
+// TMEM allocation, the mbarrier, and the CTA's copies of the sliced matrices and inner twiddles. Ends with the
+// CTA synchronised; returns the TMEM base address.
+__device__ inline uint32_t tc_setup(const TcSmem& m, const TcSub& s) {
+    if (threadIdx.x < 32) tmem_alloc(m.tmem_slot, (uint32_t)s.ncols);
+    if (threadIdx.x == 0) mbar_init(m.mbar, 1);
+    const int na = tc_bm_bytes(s.a) / 16, nb = tc_bm_bytes(s.b) / 16;
+#pragma unroll 4
+    for (int i = threadIdx.x; i < na; i += blockDim.x) reinterpret_cast<uint4*>(m.bm_a)[i] = __ldg(s.a.slices + i);
+#pragma unroll 4
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) reinterpret_cast<uint4*>(m.bm_b)[i] = __ldg(s.b.slices + i);
+    for (int i = threadIdx.x; i < s.N; i += blockDim.x) m.tw[i] = __ldg(s.tw + i);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    return *m.tmem_slot;
+}
+
+__device__ inline void tc_teardown(const TcSub& s, uint32_t tmem) {
+    tc_fence_before();
+    __syncthreads();
+    if (threadIdx.x < 32) tmem_dealloc(tmem, (uint32_t)s.ncols);
+}
+
+// Exponent bound of x: |x| < 2^tc_expo(x) (zero and subnormals: -1022)
+__device__ __forceinline__ int tc_expo(double x) {
+    const int ex = (int)((__double_as_longlong(x) >> 52) & 0x7ff);
+    return ex ? ex - 1022 : -1022;
+}
+// floor(|x| * 2^(56 - e)) for |x| < 2^e: the 56-bit magnitude the slices are cut from
+__device__ __forceinline__ unsigned long long tc_mag(double x, int e) {
+    const unsigned long long b = (unsigned long long)__double_as_longlong(x);
+    int ex = (int)((b >> 52) & 0x7ff);
+    unsigned long long m = b & ((1ull << 52) - 1);
+    if (ex) m |= 1ull << 52;
+    else ex = 1;
+    const int sh = ex - 1019 - e;
+    return sh >= 0 ? m << sh : (sh > -64 ? m >> -sh : 0ull);
+}
+// 2^k as a float64 for k in the normal range
+__device__ __forceinline__ double tc_pow2(int k) {
+    if (k < -1022 || k > 1023) return ldexp(1.0, k);
+    return __longlong_as_double((long long)(k + 1023) << 52);
+}
+
+// One contraction stage: `nrows` rows of R complex values, load(row, j, part) -> double (part 0 the real, 1 the
+// imaginary part); store(row, k, part, y) for output k. `phase` counts the mbarrier phases completed so far.
+template <class Load, class Store>
+__device__ inline void tc_stage(const TcRadix& rad, int nrows, const TcSmem& m, const unsigned char* bmat,
+                                uint32_t tmem, uint32_t& phase, int* err, Load load, Store store) {
+    const int R = rad.R, kh = rad.kh, nh = rad.nh, kpad = 2 * kh, npad = 2 * nh;
+    const int t = threadIdx.x;
+    {  // slicing: two threads per row, one per K half (real, imaginary parts); the row exponent through smem
+        const int row = t & (kTcRows - 1), part = t >> 7;
+        double vals[32];
+        int e = -1022;
+#pragma unroll
+        for (int j = 0; j < 32; j++) {
+            vals[j] = (row < nrows && j < R) ? load(row, j, part) : 0.0;
+            e = max(e, tc_expo(vals[j]));
+        }
+        m.emax[part * kTcRows + row] = e;
+        __syncthreads();
+        e = max(m.emax[row], m.emax[kTcRows + row]);
+        if (row < nrows) {
+#pragma unroll
+            for (int c = 0; c < 32; c += 16) {
+                if (c >= kh) break;
+                unsigned long long mag[16];
+                unsigned neg = 0;
+#pragma unroll
+                for (int q = 0; q < 16; q++) {
+                    mag[q] = tc_mag(vals[c + q], e);
+                    if (__double_as_longlong(vals[c + q]) < 0) neg |= 1u << q;
+                }
+#pragma unroll
+                for (int i = 0; i < kTcSlices; i++) {
+                    uint32_t w[4] = {0, 0, 0, 0};
+#pragma unroll
+                    for (int q = 0; q < 16; q++) {
+                        int sl = (int)((mag[q] >> (49 - 7 * i)) & 127);
+                        if ((neg >> q) & 1) sl = -sl;
+                        w[q >> 2] |= (uint32_t)(sl & 0xff) << (8 * (q & 3));
+                    }
+                    *reinterpret_cast<uint4*>(m.slices + i * kTcRows * kpad + umma_off(row, part * kh + c, kpad)) =
+                        make_uint4(w[0], w[1], w[2], w[3]);
+                }
+            }
+        }
+        __syncthreads();
+        if (part == 0) m.emax[row] = e;
+    }
+    fence_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    // Accumulators d = 0..kTcAcc-1 of nr columns each; when they do not fit TMEM at once the real and the
+    // imaginary outputs go in two rounds.
+    const int rounds = kTcAcc * npad <= 512 ? 1 : 2, nr = npad / rounds;
+    const uint32_t sbo = 8 * kpad;
+    for (int rd = 0; rd < rounds; rd++) {
+        if (t == 0) {  // the product triangle i + j <= kTcAcc - 1, accumulator d collecting every i + j = d
+            const uint32_t idesc = umma_idesc_s8(kTcRows, nr), sa = smem_u32(m.slices),
+                           sb = smem_u32(bmat) + rd * nr * kpad;
+            for (int d = 0; d < kTcAcc; d++) {
+                const int i0 = d < kTcSlices ? 0 : d - kTcSlices + 1, i1 = d < kTcSlices ? d : kTcSlices - 1;
+                for (int i = i0; i <= i1; i++)
+                    for (int ks = 0; ks < kpad / 32; ks++)
+                        umma_s8(tmem + d * nr, umma_desc(sa + i * kTcRows * kpad + 256 * ks, 128, sbo),
+                                umma_desc(sb + (d - i) * npad * kpad + 256 * ks, 128, sbo), idesc,
+                                (i > i0 || ks) ? 1u : 0u);
+            }
+            umma_commit(m.mbar);
+        }
+        bool ok = mbar_wait(m.mbar, phase & 1u, kTcWaitLimit);
+        phase++;
+        ok = __all_sync(0xffffffffu, ok);  // the TMEM loads below are warp-collective
+        tc_fence_after();
+        if (!ok) {
+            if ((t & 31) == 0) atomicExch(err, 1);
+        } else {  // recombination: warp w reads TMEM lanes 32 (w % 4) .., warpgroup w / 4 one half of the columns
+            const int warp = t >> 5, lane0 = 32 * (warp & 3), row = lane0 + (t & 31), half = nr / 2;
+            const int c_begin = (warp >> 2) * half;
+            const int e = row < nrows ? m.emax[row] : 0;
+            const double s1 = tc_pow2(e - 34), s2 = tc_pow2(e - 69);
+            const uint32_t lane_addr = tmem + ((uint32_t)lane0 << 16);
+            for (int c0 = c_begin; c0 < c_begin + half; c0 += 8) {
+                long long hi[8], lo[8];
+                int32_t v[5][8];
+#pragma unroll
+                for (int d = 0; d < 4; d++) tmem_ld8(lane_addr + d * nr + c0, v[d]);
+                tmem_wait_ld();
+#pragma unroll
+                for (int q = 0; q < 8; q++)
+                    hi[q] = (((long long)v[0][q] * 128 + v[1][q]) * 128 + v[2][q]) * 128 + v[3][q];
+#pragma unroll
+                for (int d = 0; d < 5; d++) tmem_ld8(lane_addr + (d + 4) * nr + c0, v[d]);
+                tmem_wait_ld();
+#pragma unroll
+                for (int q = 0; q < 8; q++)
+                    lo[q] = ((((long long)v[0][q] * 128 + v[1][q]) * 128 + v[2][q]) * 128 + v[3][q]) * 128 + v[4][q];
+                if (row < nrows) {
+#pragma unroll
+                    for (int q = 0; q < 8; q++) {
+                        const int n = rd * nr + c0 + q, part = n >= nh, k = n - part * nh;
+                        if (k < R)
+                            store(row, k, part, __dadd_rn(__dmul_rn(__ll2double_rn(hi[q]), s1),
+                                                          __dmul_rn(__ll2double_rn(lo[q]), s2)));
+                    }
+                }
+            }
+        }
+        tc_fence_before();
+        __syncthreads();
+        tc_fence_after();
+    }
+}
+
+// Sub-FFT of N = Ra * Rb points on F sequences held in X (element j of sequence f at j * F + f), Cooley-Tukey
+// with n = Rb j + m, k = k1 + Ra k2: stage A (DFT_Ra over j for each m), the twiddle w_N^{m k1}, stage B (DFT_Rb
+// over m for each k1). Y is scratch; the result is in X in natural order. `phase`: mbarrier phases completed so
+// far by this CTA.
+__device__ inline void tc_subfft(const TcSub& s, const Planes<ArF64>& X, const Planes<ArF64>& Y, const TcSmem& m,
+                                 uint32_t tmem, uint32_t& phase, int* err) {
+    const int F = s.F, Ra = s.a.R, Rb = s.b.R;
+    tc_stage(s.a, Rb * F, m, m.bm_a, tmem, phase, err,
+             [&](int r, int j, int part) {
+                 const int mm = r / F, f = r - mm * F, i = (Rb * j + mm) * F + f;
+                 return part ? X.im[i] : X.re[i];
+             },
+             [&](int r, int k1, int part, double y) {
+                 const int mm = r / F, f = r - mm * F, i = (k1 * Rb + mm) * F + f;
+                 (part ? Y.im : Y.re)[i] = y;
+             });
+    for (int e = threadIdx.x; e < s.N * F; e += blockDim.x) {
+        const double2 w = m.tw[e / F];
+        const double re = Y.re[e], im = Y.im[e];
+        Y.re[e] = __dsub_rn(__dmul_rn(re, w.x), __dmul_rn(im, w.y));
+        Y.im[e] = __dadd_rn(__dmul_rn(re, w.y), __dmul_rn(im, w.x));
+    }
+    __syncthreads();
+    tc_stage(s.b, Ra * F, m, m.bm_b, tmem, phase, err,
+             [&](int r, int mm, int part) {
+                 const int k1 = r / F, f = r - k1 * F, i = (k1 * Rb + mm) * F + f;
+                 return part ? Y.im[i] : Y.re[i];
+             },
+             [&](int r, int k2, int part, double y) {
+                 const int k1 = r / F, f = r - k1 * F, i = (k1 + Ra * k2) * F + f;
+                 (part ? X.im : X.re)[i] = y;
+             });
+}
+
+}  // namespace kbsrc::dev

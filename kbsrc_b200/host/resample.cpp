@@ -370,6 +370,7 @@ std::unique_ptr<Conversion> prepare(const double* in, long long frames, int ch, 
     kbsrc_gpu_desc& d = cv->desc;
     d.precision = opt.precision == Precision::Fast         ? KBSRC_GPU_FAST
                   : opt.precision == Precision::LongDouble ? KBSRC_GPU_LD
+                  : opt.precision == Precision::SplitTC    ? KBSRC_GPU_SPLIT
                                                            : KBSRC_GPU_EXACT;
     d.channels = ch;
     d.P = P;
@@ -440,7 +441,7 @@ std::vector<std::vector<double>> resample_gpu(const double* in, long long frames
 
 std::vector<std::vector<double>> resample(const double* in, long long frames, int channels, int rate_in, int rate_out,
                                           const Options& opt, Stats* stats) {
-    RoundToNearest rn(opt.precision == Precision::Exact);
+    RoundToNearest rn(opt.precision == Precision::Exact || opt.precision == Precision::SplitTC);
     return resample_gpu(in, frames, channels, rate_in, rate_out, opt, stats);
 }
 
@@ -450,7 +451,7 @@ std::vector<unsigned char> resample_wav_data(const double* in, long long frames,
     const std::string f = format ? format : "";
     const int fmt = f == "f64" ? 0 : f == "f32" ? 1 : f == "s32" ? 2 : f == "s24" ? 3 : f == "s16" ? 4 : -1;
     if (fmt < 0) throw std::invalid_argument("format must be f64, f32, s32, s24 or s16");
-    RoundToNearest rn(opt.precision == Precision::Exact);
+    RoundToNearest rn(opt.precision == Precision::Exact || opt.precision == Precision::SplitTC);
     auto cv = prepare(in, frames, channels, rate_in, rate_out, opt);
     if (cv->pl.copy) throw std::invalid_argument("equal rates: nothing to convert");
     const double t1 = now();
@@ -493,6 +494,7 @@ extern "C" long long kbsrc_resample_c(const double* in, long long frames, int ch
         if (copt) {
             o.precision = copt->precision == 0   ? kbsrc::Precision::Fast
                           : copt->precision == 2 ? kbsrc::Precision::LongDouble
+                          : copt->precision == 3 ? kbsrc::Precision::SplitTC
                                                  : kbsrc::Precision::Exact;
             o.length = copt->length;
             o.beta = copt->beta;
@@ -530,6 +532,7 @@ kbsrc::Options options_from_c(const kbsrc_options_c* copt) {
     if (copt) {
         o.precision = copt->precision == 0   ? kbsrc::Precision::Fast
                       : copt->precision == 2 ? kbsrc::Precision::LongDouble
+                      : copt->precision == 3 ? kbsrc::Precision::SplitTC
                                              : kbsrc::Precision::Exact;
         o.length = copt->length;
         o.beta = copt->beta;
@@ -547,7 +550,7 @@ extern "C" int kbsrc_prepare_c(const double* in, long long frames, int channels,
     *out = nullptr;
     try {
         const kbsrc::Options o = options_from_c(copt);
-        kbsrc::RoundToNearest rn(o.precision == kbsrc::Precision::Exact);
+        kbsrc::RoundToNearest rn(o.precision == kbsrc::Precision::Exact || o.precision == kbsrc::Precision::SplitTC);
         *out = reinterpret_cast<kbsrc_conversion*>(kbsrc::prepare(in, frames, channels, rate_in, rate_out, o).release());
         return 0;
     } catch (const std::invalid_argument& x) {
@@ -657,7 +660,7 @@ extern "C" int kbsrc_batch_prepare_c(const kbsrc_batch_item_c* items, int count,
     *out = nullptr;
     try {
         const kbsrc::Options o = options_from_c(copt);
-        kbsrc::RoundToNearest rn(o.precision == kbsrc::Precision::Exact);
+        kbsrc::RoundToNearest rn(o.precision == kbsrc::Precision::Exact || o.precision == kbsrc::Precision::SplitTC);
         auto b = std::make_unique<kbsrc::BatchRun>();
         b->convs.resize(count);
         kbsrc::SpectrumCache cache;
@@ -667,7 +670,8 @@ extern "C" int kbsrc_batch_prepare_c(const kbsrc_batch_item_c* items, int count,
         kbsrc::Options inner = o;
         inner.threads = 1;  // parallel over conversions instead
         kbsrc::parallel_for(o.threads ? o.threads : hw, count, 1, [&](long long i) {
-            kbsrc::RoundToNearest rn_worker(o.precision == kbsrc::Precision::Exact);
+            kbsrc::RoundToNearest rn_worker(o.precision == kbsrc::Precision::Exact ||
+                                                     o.precision == kbsrc::Precision::SplitTC);
             try {
                 b->convs[i] = kbsrc::prepare(items[i].in, items[i].frames, items[i].channels, items[i].rate_in,
                                              items[i].rate_out, inner, false, &cache);

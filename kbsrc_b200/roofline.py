@@ -134,3 +134,71 @@ def pass_bytes(plan, exact):
             "merge": e * (hf + 1) + e * hi,
             "inv_column": 2 * e * hi if four_i else e * hi + out,
             "inv_row": e * hi + out if four_i else 0}
+
+
+# ---------------------------------------------------------------------------------------------------------------
+# split-precision form: tensor-core work (mirrors the planner of kbsrc_b200/csrc/engine.cu, make_tc_fft)
+# ---------------------------------------------------------------------------------------------------------------
+TC_SLICES, TC_ACC, TC_ROWS = 8, 9, 128
+TC_PRODUCTS = sum(min(d, TC_SLICES - 1) - max(0, d - TC_SLICES + 1) + 1 for d in range(TC_ACC))  # 43
+
+
+def tc_factor(N):
+    """(Ra, Rb) with Ra * Rb = N, both <= 32, Ra the largest such divisor <= sqrt(N); None if there is none."""
+    best = 0
+    a = 1
+    while a <= 32 and a * a <= N:
+        if N % a == 0 and N // a <= 32:
+            best = a
+        a += 1
+    return (best, N // best) if best else None
+
+
+def tc_split(n):
+    """(N1, N2): one direct sub-FFT (N2 = 1) up to 1024 points, else the four-step split nearest sqrt(n)."""
+    if n <= 1024 and tc_factor(n):
+        return n, 1
+    N1 = int(math.isqrt(n)) + 1
+    while N1 >= 2:
+        if N1 * N1 <= n and n % N1 == 0 and n // N1 <= 1024 and tc_factor(N1) and tc_factor(n // N1):
+            return N1, n // N1
+        N1 -= 1
+    return None
+
+
+def _tc_stage_ops(R):
+    kh = 16 if R <= 16 else 32
+    nh = 16 if R <= 16 else 24 if R <= 24 else 32
+    kpad, npad = 2 * kh, 2 * nh
+    rounds = 1 if TC_ACC * npad <= 512 else 2
+    nr = npad // rounds
+    return TC_PRODUCTS * (kpad // 32) * rounds * 2 * TC_ROWS * nr * 32  # issued int8 ops (M x N x K x 2)
+
+
+def _tc_sub_ops(N, count):
+    Ra, Rb = tc_factor(N)
+    F = max(1, min(TC_ROWS // max(Ra, Rb), count))
+    while F > 1 and 2 * N * F * 16 + _tc_smem(Ra, Rb, N) > 227 * 1024:
+        F -= 1
+    items = -(-count // F)
+    return items * (_tc_stage_ops(Ra) + _tc_stage_ops(Rb))
+
+
+def _tc_smem(Ra, Rb, N):
+    al = lambda v: (v + 127) // 128 * 128
+    kh = lambda R: 16 if R <= 16 else 32
+    nh = lambda R: 16 if R <= 16 else 24 if R <= 24 else 32
+    kpad = 2 * max(kh(Ra), kh(Rb))
+    bm = lambda R: TC_SLICES * 2 * nh(R) * 2 * kh(R)
+    return al(TC_SLICES * TC_ROWS * kpad) + al(bm(Ra)) + al(bm(Rb)) + al(N * 16) + al(2 * TC_ROWS * 4) + 128
+
+
+def split_work(plan, channels):
+    """Issued int8 tensor-core operations per task of each split-form pass, and in all."""
+    tasks = channels * plan["nblk"]
+    per = {}
+    for pre, n in (("fwd", plan["Nb"] // 2), ("inv", plan["Mb"] // 2)):
+        N1, N2 = tc_split(n)
+        per[pre + "_column"] = _tc_sub_ops(N1, N2)
+        per[pre + "_row"] = _tc_sub_ops(N2, N1) if N2 > 1 else 0
+    return {"tasks": tasks, "int8_ops_per_task": per, "int8_ops_total": sum(per.values()) * tasks}

@@ -1,0 +1,50 @@
+"""The split-precision tensor-core form (mode "split") against the byte-exact engines.
+
+The split form runs the Exact plan with every FFT stage as an int8-sliced DFT-matrix contraction on the tensor
+cores and float64 everywhere else, so it is not byte-identical to any reference engine. Its promise is accuracy:
+its error against the exact (double-double) output is no worse than that of the reference's fast (float64)
+engine on the same input. These tests hold it to that, at small sizes and at the full 180 s benchmark size."""
+import numpy as np
+import pytest
+
+import kbsrc_b200
+from cases import noise
+
+pytestmark = pytest.mark.gpu
+
+
+def errors(x, fi, fo, **kw):
+    st = {}
+    s = kbsrc_b200.resample(x, fi, fo, mode="split", stats=st, **kw)
+    e = kbsrc_b200.resample(x, fi, fo, mode="exact", **kw)
+    f = kbsrc_b200.resample(x, fi, fo, mode="fast", **kw)
+    assert s.shape == e.shape == f.shape
+    assert st["isa"] == "sm_100a"
+    return np.abs(s - e).max(initial=0.0), np.abs(f - e).max(initial=0.0), np.abs(e).max(initial=0.0)
+
+
+CASES = [(96000, 44100, 20000, 2), (44100, 48000, 30000, 1), (48000, 96000, 97, 2), (192000, 44100, 40000, 2),
+         (44100, 96000, 10000, 2), (48000, 44100, 10, 1)]
+
+
+@pytest.mark.parametrize("fi,fo,n,ch", CASES)
+def test_split_error_within_fast_error(fi, fo, n, ch):
+    x = np.random.default_rng(fi + n).uniform(-0.5, 0.5, (n, ch))
+    es, ef, peak = errors(x, fi, fo)
+    print(f"split {es:.3e} fast {ef:.3e} peak {peak:.3e}")
+    assert es <= max(ef, 4e-17 * peak)
+
+
+def test_split_full_size_c2():
+    """180 s stereo 96 kHz -> 44.1 kHz uniform noise: the headline conversion."""
+    x = noise(2, 180, 96000, 2)
+    es, ef, peak = errors(x, 96000, 44100)
+    print(f"split {es:.3e} fast {ef:.3e} peak {peak:.3e}")
+    assert es <= ef
+
+
+def test_split_runs_twice_the_same():
+    x = np.random.default_rng(3).uniform(-0.5, 0.5, (30000, 2))
+    cv = kbsrc_b200.Conversion(x, 96000, 44100, mode="split")
+    a, b = cv.run(x), cv.run(x)
+    assert np.array_equal(a, b)
