@@ -295,7 +295,7 @@ def product_arm(args, w, world, rank, local, pg):
         with open(os.path.join(ROOT, "tests", "golden", "golden.json")) as f:
             gold = json.load(f)["cases"]
         key = {"c2_exact": "c2_96k_44k1_exact", "c2_fast": "c2_96k_44k1_fast", "c1_exact": "c1_96k_44k1_exact",
-               "c3_exact": "c3_sweep_44k1_48k_exact"}.get(args.workload)
+               "c3_exact": "c3_sweep_44k1_48k_exact"}.get(args.workload) if not args.seconds else None
         golden_sha = gold.get(key, {}).get("sha256")
     except Exception:
         pass
@@ -531,8 +531,12 @@ def main():
     ap.add_argument("--impl", default="product", choices=["product", "reference"])
     ap.add_argument("--workload", default="c2_exact", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    ap.add_argument("--seconds", type=float, default=None,
+                    help="shorter input of the same workload (profiling captures of a small case)")
     args = ap.parse_args()
-    w = WORKLOADS[args.workload]
+    w = dict(WORKLOADS[args.workload])
+    if args.seconds and "seconds" in w:
+        w["seconds"] = args.seconds
     world, rank, local, pg = dist_setup(args)
     if args.impl == "reference":
         reference_arm(args, w, world, rank, pg)
