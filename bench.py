@@ -37,6 +37,9 @@ WORKLOADS = {
     "c2_split": dict(seed=2, seconds=180, rate_in=96000, rate_out=44100, channels=2, mode="split"),
     "c1_exact": dict(seed=1, seconds=10, rate_in=96000, rate_out=44100, channels=2, mode="exact"),
     "c3_exact": dict(sweep=True, seconds=60, rate_in=44100, rate_out=48000, channels=2, mode="exact"),
+    # large multichannel, long kernel: 600 s 8 ch 192k -> 44.1k from 24-bit PCM, --len 1.0 --beta 60
+    "c5_exact": dict(pcm24=True, seed=4, seconds=600, rate_in=192000, rate_out=44100, channels=8, mode="exact",
+                     length=1.0, beta=60.0),
     # the uneven queue: 256 files, 1-60 s, 1-8 channels, mixed rate pairs, one GPU batch (exact)
     "c4_exact": dict(batch=True, seed=3, files=256, mode="exact"),
 }
@@ -59,7 +62,9 @@ def error_stats(y, ref):
 
 
 def make_input(w):
-    from cases import noise, sweep
+    from cases import noise, sweep, pcm24_ints, pcm24_as_f64
+    if w.get("pcm24"):
+        return pcm24_as_f64(pcm24_ints(w["seed"], w["seconds"], w["rate_in"], w["channels"]))
     if w.get("sweep"):
         return sweep(w["seconds"], w["rate_in"], w["channels"])
     return noise(w["seed"], w["seconds"], w["rate_in"], w["channels"])
@@ -157,7 +162,8 @@ def cpu_reference(x, w, threads, runs=1):
     for _ in range(runs):
         st = {}
         t = time.perf_counter()
-        y = oracle.ref_resample(x, w["rate_in"], w["rate_out"], fast=w["mode"] == "fast", threads=threads, stats=st)
+        y = oracle.ref_resample(x, w["rate_in"], w["rate_out"], fast=w["mode"] == "fast", threads=threads, stats=st,
+                                length=w.get("length", 0.2), beta=w.get("beta", 40.0))
         walls += time.perf_counter() - t
         n_out += y.size
         secs += st["process_seconds"]
@@ -223,8 +229,9 @@ def product_arm(args, w, world, rank, local, pg):
     split = w["mode"] == "split"
     x = make_input(w)
     frames, ch = x.shape
-    cv = kbsrc_b200.Conversion(x, w["rate_in"], w["rate_out"], mode=w["mode"])
-    plan = kbsrc_b200.plan(frames, ch, w["rate_in"], w["rate_out"], w["mode"])
+    kw = dict(length=w.get("length", 0.2), beta=w.get("beta", 40.0))
+    cv = kbsrc_b200.Conversion(x, w["rate_in"], w["rate_out"], mode=w["mode"], **kw)
+    plan = kbsrc_b200.plan(frames, ch, w["rate_in"], w["rate_out"], w["mode"], **kw)
     work = roofline.conversion_work(plan, ch, exact or split)
     twork = roofline.split_work(plan, ch) if split else None
     info = cv.engine_info()
@@ -297,6 +304,9 @@ def product_arm(args, w, world, rank, local, pg):
         key = {"c2_exact": "c2_96k_44k1_exact", "c2_fast": "c2_96k_44k1_fast", "c1_exact": "c1_96k_44k1_exact",
                "c3_exact": "c3_sweep_44k1_48k_exact"}.get(args.workload) if not args.seconds else None
         golden_sha = gold.get(key, {}).get("sha256")
+        if args.workload == "c5_exact" and not args.seconds:
+            with open(os.path.join(ROOT, "tests", "golden", "golden_c5.json")) as f:
+                golden_sha = json.load(f)["planar_sha256"]
     except Exception:
         pass
     if rank != 0:
@@ -351,8 +361,8 @@ def product_arm(args, w, world, rank, local, pg):
                    "value_t8": round(c_8["engine_msps"], 3), "whole_call_msps": round(c_all["wall_msps"], 3)}
     extra = {}
     if split:  # the comparison the form exists for: accuracy against exact, throughput against plain exact
-        ref = kbsrc_b200.Conversion(x, w["rate_in"], w["rate_out"], mode="exact")
-        fast = kbsrc_b200.Conversion(x, w["rate_in"], w["rate_out"], mode="fast")
+        ref = kbsrc_b200.Conversion(x, w["rate_in"], w["rate_out"], mode="exact", **kw)
+        fast = kbsrc_b200.Conversion(x, w["rate_in"], w["rate_out"], mode="fast", **kw)
         y_exact, y_fast = ref.run(x), fast.run(x)
         extra["error_vs_exact"] = {"split": error_stats(got, y_exact), "fast": error_stats(y_fast, y_exact)}
         d_out2 = torch.empty_like(d_out)
@@ -377,7 +387,7 @@ def product_arm(args, w, world, rank, local, pg):
         "dtype": "dd (double-double f64 pairs)" if exact else ("int8 tensor-core slices, f64" if split else "f64"),
         "data": "synthetic",
         "config": {"workload": args.workload, **w, "tasks": work["tasks"], "block": plan["nb"],
-                   "fft_points": [plan["Nb"], plan["Mb"]], "l2": "inputs larger than L2 (276 MB)",
+                   "fft_points": [plan["Nb"], plan["Mb"]], "l2": f"inputs larger than L2 ({x.nbytes / 1e6:.0f} MB)",
                    "parallelism": f"independent conversions x{world}"},
         "e2e": {"value": round(e2e, 3), "unit": "Msamples/s", "h2d_bytes_per_step": int(8 * (x.size + cv.head.size
                                                                                                  + cv.tail.size)),

@@ -120,3 +120,32 @@ def c4_samples(seed, i, frames, ch):
 
 # the scaled-down queue of the parity tests: 48 files of 0.2-3 s
 C4_SMALL = dict(seed=3, count=48, min_s=0.2, max_s=3.0)
+
+
+# The large multichannel configuration: 600 s of 8-channel 192 kHz 24-bit PCM, uniform integers in
+# [-2^23, 2^23) from default_rng(4), converted to 44.1 kHz with --len 1.0 --beta 60, s24 output with TPDF dither.
+C5 = dict(seed=4, seconds=600, rate_in=192000, rate_out=44100, channels=8, length=1.0, beta=60.0)
+
+
+def pcm24_ints(seed, seconds, rate, ch):
+    """The 24-bit sample values (frames x channels, int32)."""
+    return np.random.default_rng(seed).integers(-2 ** 23, 2 ** 23, (int(seconds * rate), ch)).astype(np.int32)
+
+
+def write_pcm24_wav(path, ints, rate):
+    """A 24-bit PCM WAV file (16-byte fmt chunk) of the int32 samples, written in slices of frames."""
+    import struct
+    frames, ch = ints.shape
+    data_len = frames * ch * 3
+    with open(path, "wb") as f:
+        f.write(b"RIFF" + struct.pack("<I", 36 + data_len) + b"WAVE" + b"fmt " + struct.pack("<I", 16) +
+                struct.pack("<HHIIHH", 1, ch, rate, rate * ch * 3, ch * 3, 24) + b"data" + struct.pack("<I", data_len))
+        step = 1 << 20
+        for f0 in range(0, frames, step):
+            b = ints[f0:f0 + step].astype("<i4").view(np.uint8).reshape(-1, 4)[:, :3]
+            f.write(np.ascontiguousarray(b).tobytes())
+
+
+def pcm24_as_f64(ints):
+    """The values the WAV reader delivers: v / 2^23."""
+    return ints.astype(np.float64) / 8388608.0
