@@ -218,6 +218,33 @@ def reference_arm(args, w, world, rank, pg):
         pg.destroy_process_group()
 
 
+def cli_e2e(w):
+    """Wall time of the kbsrc command line on the workload's 24-bit WAV file (read, decode, kernel design, LPC,
+    conversion, output step with dither, write), ours and the reference tool built from source."""
+    import subprocess
+    import tempfile
+    import kbsrc_b200
+    from cases import pcm24_ints, write_pcm24_wav
+    from oracle import oracle
+    out = {}
+    with tempfile.TemporaryDirectory() as d:
+        src = os.path.join(d, "in.wav")
+        write_pcm24_wav(src, pcm24_ints(w["seed"], w["seconds"], w["rate_in"], w["channels"]), w["rate_in"])
+        args = ["--rate", str(w["rate_out"]), "--len", str(w["length"]), "--beta", str(w["beta"]), "--format", "s24",
+                "--dither", src]
+        tools = [("ours", kbsrc_b200.CLI)] + ([("reference", oracle.REF_CLI)] if os.path.exists(oracle.REF_CLI) else [])
+        for name, exe in tools:
+            dst = os.path.join(d, name + ".wav")
+            t = time.perf_counter()
+            r = subprocess.run([exe] + args + [dst], capture_output=True, text=True)
+            out[name + "_seconds"] = round(time.perf_counter() - t, 3)
+            out[name + "_ok"] = r.returncode == 0
+            if os.path.exists(dst):
+                os.remove(dst)
+    out["input_bytes"] = int(w["seconds"] * w["rate_in"]) * w["channels"] * 3
+    return out
+
+
 def product_arm(args, w, world, rank, local, pg):
     import torch
     import kbsrc_b200
@@ -288,11 +315,25 @@ def product_arm(args, w, world, rank, local, pg):
         for _ in range(e2e_steps):
             cv.run_host_raw(hx.data_ptr(), hh.data_ptr(), ht.data_ptr(), ho.data_ptr())
         e2e_s = time.perf_counter() - t
+        # the copy floor of that path: the same bytes up (pinned -> device) and down (device -> pinned) on two
+        # streams at once, no compute
+        up, down = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+        d_x2 = torch.empty_like(d_in)
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        for _ in range(e2e_steps):
+            with torch.cuda.stream(up):
+                d_x2.copy_(hx, non_blocking=True)
+            with torch.cuda.stream(down):
+                ho.copy_(d_out, non_blocking=True)
+            torch.cuda.synchronize()
+        copy_s = time.perf_counter() - t
+        del d_x2
     if pg:
         import torch.distributed as dist
-        tt = torch.tensor([ms, e2e_s], dtype=torch.float64, device=dev)
+        tt = torch.tensor([ms, e2e_s, copy_s], dtype=torch.float64, device=dev)
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms, e2e_s = tt.tolist()
+        ms, e2e_s, copy_s = tt.tolist()
     # byte-identity of what was timed, against the reference's hash for this workload
     got = ho[:ch * nout].numpy().reshape(ch, nout)
     import hashlib
@@ -360,6 +401,8 @@ def product_arm(args, w, world, rank, local, pg):
                              "time (Stats::process_seconds), all host threads",
                    "value_t8": round(c_8["engine_msps"], 3), "whole_call_msps": round(c_all["wall_msps"], 3)}
     extra = {}
+    if w.get("pcm24") and not args.seconds:  # the tool a user runs, on the 24-bit file, ours and the reference's
+        extra["cli_e2e"] = cli_e2e(w)
     if split:  # the comparison the form exists for: accuracy against exact, throughput against plain exact
         ref = kbsrc_b200.Conversion(x, w["rate_in"], w["rate_out"], mode="exact", **kw)
         fast = kbsrc_b200.Conversion(x, w["rate_in"], w["rate_out"], mode="fast", **kw)
@@ -391,7 +434,9 @@ def product_arm(args, w, world, rank, local, pg):
                    "parallelism": f"independent conversions x{world}"},
         "e2e": {"value": round(e2e, 3), "unit": "Msamples/s", "h2d_bytes_per_step": int(8 * (x.size + cv.head.size
                                                                                                  + cv.tail.size)),
-                "d2h_bytes_per_step": int(8 * ch * nout), "path": "kbsrc_gpu_engine_run_host (C ABI), pinned"},
+                "d2h_bytes_per_step": int(8 * ch * nout), "path": "kbsrc_gpu_engine_run_host (C ABI), pinned",
+                "copy_floor_ms_per_step": round(copy_s / e2e_steps * 1e3, 3),
+                "frac_of_copy_floor": round(copy_s / e2e_s, 4)},
         "gpu_launches": int(info["launches"] * args.steps),
         "roofline": roof,
         "passes": {k: {"ms": round(avg_ms[k], 4), "share": round(share[k], 4),

@@ -53,6 +53,15 @@ std::vector<unsigned char> resample_wav_data(const double* interleaved, long lon
                                              int rate_out, const char* format, bool dither, long long& clipped,
                                              const Options& options = {}, Stats* stats = nullptr);
 
+// resample_wav_data on the data section of a PCM or float WAV file as it is stored: `pcm` holds frames x channels
+// samples of `sample_format` ("u8", "s16", "s24", "s32", "f32" or "f64", little-endian). The GPU decodes every
+// sample as the reference's WAV reader does while it gathers blocks (a 24-bit file moves 3 bytes per sample to
+// the device instead of 8); the host decodes only the frames the LPC edges need. Output and exceptions as
+// resample_wav_data.
+std::vector<unsigned char> resample_wav_pcm(const void* pcm, const char* sample_format, long long frames,
+                                            int channels, int rate_in, int rate_out, const char* format, bool dither,
+                                            long long& clipped, const Options& options = {}, Stats* stats = nullptr);
+
 const char* version();
 
 }  // namespace kbsrc

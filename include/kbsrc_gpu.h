@@ -32,6 +32,17 @@ extern "C" {
 #define KBSRC_GPU_SPLIT 3 /* split-precision form: tensor-core int8 DFT contractions, float64 elsewhere; not
                              byte-identical, within float64 rounding of exact (no reference counterpart) */
 
+/* Sample formats of the interleaved input (kbsrc_gpu_desc.in_format). The GPU reads each sample as the
+ * reference's WAV reader decodes it (src/io/wav.cpp:299-362): float64 as stored, float32 widened, integer PCM
+ * little-endian times 2^-(8B-1) (8-bit unsigned, offset by 128), all exact. Callers of every run function pass
+ * `in` (or d_in) pointing at samples of this format, cast to the declared pointer type. */
+#define KBSRC_GPU_IN_F64 0
+#define KBSRC_GPU_IN_F32 1
+#define KBSRC_GPU_IN_S32 2
+#define KBSRC_GPU_IN_S24 3 /* 3 bytes per sample */
+#define KBSRC_GPU_IN_S16 4
+#define KBSRC_GPU_IN_U8 5
+
 typedef struct kbsrc_gpu_engine kbsrc_gpu_engine;
 
 /* One conversion plan, as computed by the host planner (reference src/resampler.cpp:98-209).
@@ -54,6 +65,7 @@ typedef struct {
     long long edge_len; /* LPC samples predicted before and after the signal per channel (0: zero padding) */
     const double* H;    /* kernel spectrum, H_len (hi, lo) pairs, host memory; copied at create */
     long long H_len;
+    int in_format;      /* KBSRC_GPU_IN_*: the input's sample format (0, float64, when zero-initialised) */
 } kbsrc_gpu_desc;
 
 /* Creates an engine on the current CUDA device: FFT plans, twiddle tables and the kernel spectrum on the

@@ -55,7 +55,8 @@ class GpuDesc(ctypes.Structure):
                 ("Q", ctypes.c_longlong), ("nb", ctypes.c_int), ("marg", ctypes.c_int), ("nblk", ctypes.c_longlong),
                 ("lead", ctypes.c_longlong), ("o", ctypes.c_longlong), ("frames", ctypes.c_longlong),
                 ("nout", ctypes.c_longlong), ("up", ctypes.c_int), ("Jg", ctypes.c_int),
-                ("edge_len", ctypes.c_longlong), ("H", _dp), ("H_len", ctypes.c_longlong)]
+                ("edge_len", ctypes.c_longlong), ("H", _dp), ("H_len", ctypes.c_longlong),
+                ("in_format", ctypes.c_int)]
 
 
 # Every symbol the C headers declare: (library, name, restype, argtypes)

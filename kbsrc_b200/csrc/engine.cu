@@ -60,12 +60,13 @@ int fail(int code, const std::string& msg) {
 // The staged channel of the reference (resampler.cpp:168-186) is read without being materialised: zeros, the
 // LPC head, the interleaved input, the LPC tail, zeros; frame t of the signal is staged sample t + lead.
 struct Item {
-    const double* in;    // interleaved input, frames x ch
+    const void* in;      // interleaved input, frames x ch, samples in format `fmt` (KBSRC_GPU_IN_*)
     const double* head;  // ch x edge: head[c*edge + i] is frame -1-i
     const double* tail;  // ch x edge: tail[c*edge + i] is frame frames+i
     double* out;         // planar output, ch x nout
     long long frames, edge, lead, nout, o;
     int ch;
+    int fmt;
 };
 
 // Which conversion, channel and block a task is.
@@ -90,8 +91,25 @@ __device__ __forceinline__ TaskRef task_ref(const Work& w, long long task) {
 }
 __device__ __forceinline__ Item item_of(const Work& w, const TaskRef& r) { return w.refs ? w.items[r.item] : w.item0; }
 
+// Input sample i (= frame * ch + channel) as the WAV reader delivers it (src/io/wav.cpp:299-362): float64 as
+// stored, float32 widened, integer PCM times 2^-(8B-1) (8-bit offset by 128), all exact.
+__device__ __forceinline__ double input_at(const Item& s, long long i) {
+    switch (s.fmt) {
+        case KBSRC_GPU_IN_F64: return __ldg(static_cast<const double*>(s.in) + i);
+        case KBSRC_GPU_IN_F32: return (double)__ldg(static_cast<const float*>(s.in) + i);
+        case KBSRC_GPU_IN_S32: return __dmul_rn((double)__ldg(static_cast<const int*>(s.in) + i), 0x1p-31);
+        case KBSRC_GPU_IN_S24: {
+            const unsigned char* p = static_cast<const unsigned char*>(s.in) + 3 * i;
+            const int v = (int)__ldg(p) | (int)__ldg(p + 1) << 8 | (int)(signed char)__ldg(p + 2) << 16;
+            return __dmul_rn((double)v, 0x1p-23);
+        }
+        case KBSRC_GPU_IN_S16: return __dmul_rn((double)__ldg(static_cast<const short*>(s.in) + i), 0x1p-15);
+        default: return __dmul_rn((double)((int)__ldg(static_cast<const unsigned char*>(s.in) + i) - 128), 0x1p-7);
+    }
+}
+
 __device__ __forceinline__ double signal_at(const Item& s, int c, long long t) {
-    if (t >= 0 && t < s.frames) return __ldg(s.in + t * s.ch + c);
+    if (t >= 0 && t < s.frames) return input_at(s, t * s.ch + c);
     if (t < 0 && t >= -s.edge) return __ldg(s.head + c * s.edge + (-1 - t));
     if (t >= s.frames && t < s.frames + s.edge) return __ldg(s.tail + c * s.edge + (t - s.frames));
     return 0.0;
@@ -155,8 +173,8 @@ __device__ __forceinline__ CxR<Ar> load_input(const PassParams<Ar>& P, const Tas
         const long long t = ts.g0 + 2 * i;
         double x0, x1;
         if (ts.interior) {
-            x0 = __ldg(ts.it.in + t * ts.it.ch + ts.c);
-            x1 = __ldg(ts.it.in + (t + 1) * ts.it.ch + ts.c);
+            x0 = input_at(ts.it, t * ts.it.ch + ts.c);
+            x1 = input_at(ts.it, (t + 1) * ts.it.ch + ts.c);
         } else {
             x0 = signal_at(ts.it, ts.c, t);
             x1 = signal_at(ts.it, ts.c, t + 1);
@@ -179,7 +197,10 @@ __device__ __forceinline__ CxR<Ar> czero() {
 }
 
 // Loads per thread issued together before their shared-memory stores (memory-level parallelism)
-constexpr int kLoadBatch = 4;
+#ifndef KB_LOAD_BATCH
+#define KB_LOAD_BATCH 4
+#endif
+constexpr int kLoadBatch = KB_LOAD_BATCH;
 
 // Shared memory of a pass: two plane pairs of n*F values, then (double-double) the sub-FFT's stage twiddles.
 template <class Ar>
@@ -743,6 +764,12 @@ struct DevBuf {
 enum TabFmt { kTabF64 = 0, kTabDD = 1, kTabX80 = 2 };
 
 size_t tab_esize(int tab) { return tab == kTabF64 ? 16 : 32; }
+
+// Bytes of one input sample in a KBSRC_GPU_IN_* format
+size_t in_bytes(int fmt) {
+    static const size_t b[] = {8, 4, 4, 3, 2, 1};
+    return fmt >= 0 && fmt <= 5 ? b[fmt] : 8;
+}
 
 // from_dd<long double> with the host's own x87 arithmetic, stored as the device's x80 (significand, sign and
 // exponent)
@@ -1464,7 +1491,7 @@ int enqueue_any(const PlanCore& pc, const Work& work, long long t_begin, long lo
 Work single_work(const PlanCore& pc, const double* in, const double* head, const double* tail, double* out) {
     const kbsrc_gpu_desc& d = pc.d;
     Work w{};
-    w.item0 = Item{in, head, tail, out, d.frames, d.edge_len, d.lead, d.nout, d.o, d.channels};
+    w.item0 = Item{in, head, tail, out, d.frames, d.edge_len, d.lead, d.nout, d.o, d.channels, d.in_format};
     w.hopQ = (long long)pc.hop * d.Q;
     w.hopP = (long long)pc.hop * d.P;
     w.margP = (long long)d.marg * d.P;
@@ -1510,6 +1537,7 @@ int check_desc(const kbsrc_gpu_desc* d) {
         return fail(KBSRC_GPU_E_ARG, "bad plan shape");
     if (d->frames < 0 || d->nout < 0 || d->nblk < 0 || d->edge_len < 0 || d->lead < 0 || d->Jg < 0)
         return fail(KBSRC_GPU_E_ARG, "bad plan sizes");
+    if (d->in_format < KBSRC_GPU_IN_F64 || d->in_format > KBSRC_GPU_IN_U8) return fail(KBSRC_GPU_E_ARG, "input format");
     if ((long long)d->nb * std::max(d->P, d->Q) > (1LL << 30)) return fail(KBSRC_GPU_E_ARG, "transform too large");
     const long long need = d->Jg ? (long long)d->Jg + 1 : (d->up ? d->nb * d->P / 2 + 1 : d->nb * d->Q / 2 + 1);
     if (!d->H || d->H_len < need) return fail(KBSRC_GPU_E_ARG, "kernel spectrum too short");
@@ -1865,7 +1893,7 @@ int batch_run_device_impl(kbsrc_gpu_batch& b, const double* const* in, const dou
     for (int i = 0; i < count; i++) {
         const kbsrc_gpu_desc& d = b.descs[i];
         b.items_host[i] = Item{in[i], head ? head[i] : nullptr, tail ? tail[i] : nullptr, out[i], d.frames,
-                               d.edge_len, d.lead, d.nout, d.o, d.channels};
+                               d.edge_len, d.lead, d.nout, d.o, d.channels, d.in_format};
     }
     if (!b.graph) {
         // record the run once; it reads every pointer from the item table, so it replays for new buffers
@@ -1994,7 +2022,7 @@ int kbsrc_gpu_engine_run_host(kbsrc_gpu_engine* e, const double* in, const doubl
         int rc;
         const size_t nin = (size_t)d.frames * d.channels, ne = (size_t)d.edge_len * d.channels,
                      no = (size_t)d.nout * d.channels;
-        if (!e->d_in.p && (rc = e->d_in.alloc(nin * 8)) != KBSRC_GPU_OK) return rc;
+        if (!e->d_in.p && (rc = e->d_in.alloc(nin * in_bytes(d.in_format))) != KBSRC_GPU_OK) return rc;
         if (!e->d_head.p && (rc = e->d_head.alloc(ne * 8)) != KBSRC_GPU_OK) return rc;
         if (!e->d_tail.p && (rc = e->d_tail.alloc(ne * 8)) != KBSRC_GPU_OK) return rc;
         if (!e->d_out.p && (rc = e->d_out.alloc(no * 8)) != KBSRC_GPU_OK) return rc;
@@ -2019,6 +2047,7 @@ int kbsrc_gpu_engine_run_host(kbsrc_gpu_engine* e, const double* in, const doubl
             KB_CUDA(cudaMemcpyAsync(e->d_tail.p, tail, ne * 8, cudaMemcpyHostToDevice, hs));
         }
         const long long nblk = d.nblk, ch = d.channels, hopQ = (long long)e->hop * d.Q, hopP = (long long)e->hop * d.P;
+        const long long bps = in_bytes(d.in_format);
         const long long chunks = nout_chunks(e, nblk);
         const Work w = single_work(*e, dinp, (const double*)e->d_head.p, (const double*)e->d_tail.p, dout);
         long long copied = 0;  // frames already sent
@@ -2028,8 +2057,9 @@ int kbsrc_gpu_engine_run_host(kbsrc_gpu_engine* e, const double* in, const doubl
             if (b0 == b1) continue;
             const long long f_hi = std::min(d.frames, std::max(0LL, (b1 - 1) * hopQ + e->Nb - d.lead));
             if (f_hi > copied) {
-                KB_CUDA(cudaMemcpyAsync(e->d_in.p ? (double*)e->d_in.p + copied * ch : nullptr, in + copied * ch,
-                                        (size_t)((f_hi - copied) * ch * 8), cudaMemcpyHostToDevice, hs));
+                KB_CUDA(cudaMemcpyAsync(static_cast<char*>(e->d_in.p) + copied * ch * bps,
+                                        reinterpret_cast<const char*>(in) + copied * ch * bps,
+                                        (size_t)((f_hi - copied) * ch * bps), cudaMemcpyHostToDevice, hs));
                 copied = f_hi;
             }
             KB_CUDA(cudaEventRecord(e->ev_in[k % 2], hs));
@@ -2046,8 +2076,9 @@ int kbsrc_gpu_engine_run_host(kbsrc_gpu_engine* e, const double* in, const doubl
                                           (size_t)(o1 - o0) * 8, (size_t)ch, cudaMemcpyDeviceToHost, ds));
         }
         if (copied < d.frames && nin)  // frames no block reads (none in a valid plan)
-            KB_CUDA(cudaMemcpyAsync((double*)e->d_in.p + copied * ch, in + copied * ch,
-                                    (size_t)((d.frames - copied) * ch * 8), cudaMemcpyHostToDevice, hs));
+            KB_CUDA(cudaMemcpyAsync(static_cast<char*>(e->d_in.p) + copied * ch * bps,
+                                    reinterpret_cast<const char*>(in) + copied * ch * bps,
+                                    (size_t)((d.frames - copied) * ch * bps), cudaMemcpyHostToDevice, hs));
         e->launches = tr.launches;
         KB_CUDA(cudaGetLastError());
         KB_CUDA(cudaStreamSynchronize(hs));
@@ -2071,7 +2102,7 @@ int kbsrc_gpu_engine_run_host_packed(kbsrc_gpu_engine* e, const double* in, cons
         int rc;
         const size_t nin = (size_t)d.frames * d.channels, ne = (size_t)d.edge_len * d.channels,
                      no = (size_t)d.nout * d.channels, nb = no * format_bytes(format);
-        if (!e->d_in.p && (rc = e->d_in.alloc(nin * 8)) != KBSRC_GPU_OK) return rc;
+        if (!e->d_in.p && (rc = e->d_in.alloc(nin * in_bytes(d.in_format))) != KBSRC_GPU_OK) return rc;
         if (!e->d_head.p && (rc = e->d_head.alloc(ne * 8)) != KBSRC_GPU_OK) return rc;
         if (!e->d_tail.p && (rc = e->d_tail.alloc(ne * 8)) != KBSRC_GPU_OK) return rc;
         if (!e->d_out.p && (rc = e->d_out.alloc(no * 8)) != KBSRC_GPU_OK) return rc;
@@ -2082,7 +2113,7 @@ int kbsrc_gpu_engine_run_host_packed(kbsrc_gpu_engine* e, const double* in, cons
         cudaStream_t st = e->stream;
         KB_CUDA(cudaMemsetAsync(cnt.p, 0, 8, st));
         if (use_dither) k_dither<<<1, 320, 0, st>>>(12345ULL, (long long)no, static_cast<double*>(dith.p));
-        if (nin) KB_CUDA(cudaMemcpyAsync(e->d_in.p, in, nin * 8, cudaMemcpyHostToDevice, st));
+        if (nin) KB_CUDA(cudaMemcpyAsync(e->d_in.p, in, nin * in_bytes(d.in_format), cudaMemcpyHostToDevice, st));
         if (ne) {
             KB_CUDA(cudaMemcpyAsync(e->d_head.p, head, ne * 8, cudaMemcpyHostToDevice, st));
             KB_CUDA(cudaMemcpyAsync(e->d_tail.p, tail, ne * 8, cudaMemcpyHostToDevice, st));
@@ -2337,7 +2368,8 @@ int kbsrc_gpu_batch_run_host(kbsrc_gpu_batch* b, const double* const* in, const 
             b->d_in.resize(count); b->d_head.resize(count); b->d_tail.resize(count); b->d_out.resize(count);
             for (int i = 0; i < count; i++) {
                 const kbsrc_gpu_desc& d = b->descs[i];
-                if ((rc = b->d_in[i].alloc((size_t)(d.frames * d.channels * 8))) != KBSRC_GPU_OK) return rc;
+                if ((rc = b->d_in[i].alloc((size_t)(d.frames * d.channels * in_bytes(d.in_format)))) != KBSRC_GPU_OK)
+                    return rc;
                 if ((rc = b->d_head[i].alloc((size_t)(d.edge_len * d.channels * 8))) != KBSRC_GPU_OK) return rc;
                 if ((rc = b->d_tail[i].alloc((size_t)(d.edge_len * d.channels * 8))) != KBSRC_GPU_OK) return rc;
                 if ((rc = b->d_out[i].alloc((size_t)(d.nout * d.channels * 8))) != KBSRC_GPU_OK) return rc;
@@ -2348,7 +2380,8 @@ int kbsrc_gpu_batch_run_host(kbsrc_gpu_batch* b, const double* const* in, const 
         cudaStream_t st = b->stream;
         for (int i = 0; i < count; i++) {
             const kbsrc_gpu_desc& d = b->descs[i];
-            const size_t ni = (size_t)(d.frames * d.channels * 8), ne = (size_t)(d.edge_len * d.channels * 8);
+            const size_t ni = (size_t)(d.frames * d.channels * in_bytes(d.in_format)),
+                         ne = (size_t)(d.edge_len * d.channels * 8);
             if (ni) KB_CUDA(cudaMemcpyAsync(b->d_in[i].p, in[i], ni, cudaMemcpyHostToDevice, st));
             if (ne && head && tail) {
                 KB_CUDA(cudaMemcpyAsync(b->d_head[i].p, head[i], ne, cudaMemcpyHostToDevice, st));

@@ -105,7 +105,7 @@ int run(int argc, char** argv) {
         throw UsageError("format must be f64, f32, s32, s24 or s16");
 
     const double t0 = now();
-    kbsrc::io::Audio a = kbsrc::io::read_wav(in_path.c_str());
+    kbsrc::io::Audio a = kbsrc::io::read_wav_raw(in_path.c_str());  // decoded on the GPU while converting
     if (a.rate > 10000000) throw std::runtime_error("input sample rate above 10000000 Hz");
     kbsrc::io::check_wav_output(a.ch, rate, format);  // fail before converting
     const double t1 = now();
@@ -113,13 +113,14 @@ int run(int argc, char** argv) {
     long long clipped = 0, nout = 0;
     double t2, t3;
     if (a.rate == rate) {  // equal rates: the host copy and the host writer
+        kbsrc::io::decode_wav(a);
         auto y = kbsrc::resample(a.d.data(), a.frames, a.ch, a.rate, rate, opt, &st);
         t2 = now();
         nout = y.empty() ? 0 : (long long)y[0].size();
         kbsrc::io::write_wav(out_path.c_str(), y, a.ch, nout, rate, format, dither, clipped);
-    } else {  // the conversion and the output step (interleave, scale, dither, round, clip) on the GPU
-        const auto data = kbsrc::resample_wav_data(a.d.data(), a.frames, a.ch, a.rate, rate, format.c_str(), dither,
-                                                   clipped, opt, &st);
+    } else {  // the input decode, the conversion and the output step (scale, dither, round, clip) on the GPU
+        const auto data = kbsrc::resample_wav_pcm(a.raw.data(), a.sample_format.c_str(), a.frames, a.ch, a.rate,
+                                                  rate, format.c_str(), dither, clipped, opt, &st);
         t2 = now();
         const long long bps = format == "f64" ? 8 : format == "s24" ? 3 : format == "s16" ? 2 : 4;
         nout = (long long)data.size() / (a.ch * bps);

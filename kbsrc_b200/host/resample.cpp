@@ -10,6 +10,7 @@
 #include <atomic>
 #include <chrono>
 #include <climits>
+#include <cstdint>
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -107,7 +108,7 @@ struct Plan {
     double fml = 0;
 };
 
-Plan make_plan(const double* in, long long frames, int ch, int rate_in, int rate_out, const Options& opt) {
+Plan make_plan(const void* in, long long frames, int ch, int rate_in, int rate_out, const Options& opt) {
     if (ch < 1 || frames < 0 || (frames > 0 && !in)) throw std::invalid_argument("bad input buffer");
     if (rate_in < 1 || rate_out < 1) throw std::invalid_argument("sample rates must be positive");
     if (!(opt.length > 0 && opt.length <= 10) || !(opt.beta > 0 && opt.beta <= 200) || opt.threads < 0 ||
@@ -282,8 +283,29 @@ struct SpectrumCache {
     std::mutex mu;
 };
 
-std::unique_ptr<Conversion> prepare(const double* in, long long frames, int ch, int rate_in, int rate_out,
-                                    const Options& opt, bool make_engine = true, SpectrumCache* cache = nullptr) {
+// Input sample i (= frame * ch + channel) of interleaved data in a KBSRC_GPU_IN_* format, decoded as the WAV
+// reader decodes it (src/io/wav.cpp:299-362); the GPU gather decodes the same way.
+double input_sample(const void* p, int fmt, long long i) {
+    const unsigned char* b = static_cast<const unsigned char*>(p);
+    switch (fmt) {
+        case KBSRC_GPU_IN_F32: { float v; std::memcpy(&v, b + 4 * i, 4); return v; }
+        case KBSRC_GPU_IN_S32: { int32_t v; std::memcpy(&v, b + 4 * i, 4); return v / 2147483648.0; }
+        case KBSRC_GPU_IN_S24: {
+            int32_t v = b[3 * i] | b[3 * i + 1] << 8 | b[3 * i + 2] << 16;
+            if (v & 0x800000) v -= 1 << 24;
+            return v / 8388608.0;
+        }
+        case KBSRC_GPU_IN_S16: { int16_t v; std::memcpy(&v, b + 2 * i, 2); return v / 32768.0; }
+        case KBSRC_GPU_IN_U8: return ((int)b[i] - 128) / 128.0;
+        default: { double v; std::memcpy(&v, b + 8 * i, 8); return v; }
+    }
+}
+
+// Plans a conversion, predicts its LPC edges, designs its kernel and creates its engine. `in`: interleaved
+// input in format in_fmt (KBSRC_GPU_IN_*); only the first and last 4096 frames are read here.
+std::unique_ptr<Conversion> prepare(const void* in, long long frames, int ch, int rate_in, int rate_out,
+                                    const Options& opt, bool make_engine = true, SpectrumCache* cache = nullptr,
+                                    int in_fmt = KBSRC_GPU_IN_F64) {
     auto cv = std::make_unique<Conversion>();
     cv->pl = make_plan(in, frames, ch, rate_in, rate_out, opt);
     cv->opt = opt;
@@ -313,9 +335,9 @@ std::unique_ptr<Conversion> prepare(const double* in, long long frames, int ch, 
             const long long m = std::min<long long>(frames, 4096);
             std::vector<double> seg((size_t)m);
             if (job % 2 == 0)  // tail: the channel's last m samples in order
-                for (long long i = 0; i < m; i++) seg[i] = in[(frames - m + i) * ch + c];
+                for (long long i = 0; i < m; i++) seg[i] = input_sample(in, in_fmt, (frames - m + i) * ch + c);
             else  // head: the first m samples reversed
-                for (long long i = 0; i < m; i++) seg[i] = in[(m - 1 - i) * ch + c];
+                for (long long i = 0; i < m; i++) seg[i] = input_sample(in, in_fmt, (m - 1 - i) * ch + c);
             std::vector<double> pred = burg_predict(seg.data(), m, ext);
             for (int i = 0; i < 32; i++) pred[ext - 32 + i] *= fade[i];
             std::copy(pred.begin(), pred.end(), (job % 2 == 0 ? cv->tail : cv->head).begin() + c * ext);
@@ -387,6 +409,7 @@ std::unique_ptr<Conversion> prepare(const double* in, long long frames, int ch, 
     d.edge_len = ext;
     d.H = cv->H.data();
     d.H_len = (long long)cv->H.size() / 2;
+    d.in_format = in_fmt;
     if (make_engine) gpu_check(kbsrc_gpu_engine_create(&d, &cv->eng.e), "GPU engine");
     cv->design_seconds = now() - t0;
     return cv;
@@ -459,6 +482,33 @@ std::vector<unsigned char> resample_wav_data(const double* in, long long frames,
     std::vector<unsigned char> data((size_t)(cv->pl.nout * channels * bps));
     gpu_check(kbsrc_gpu_engine_run_host_packed(cv->eng.e, in, cv->head.data(), cv->tail.data(), fmt, dither ? 1 : 0,
                                                data.data(), &clipped),
+              "GPU engine");
+    fill_stats(*cv, stats, now() - t1);
+    return data;
+}
+
+std::vector<unsigned char> resample_wav_pcm(const void* pcm, const char* sample_format, long long frames,
+                                            int channels, int rate_in, int rate_out, const char* format, bool dither,
+                                            long long& clipped, const Options& opt, Stats* stats) {
+    const std::string f = format ? format : "", sf = sample_format ? sample_format : "";
+    const int fmt = f == "f64" ? 0 : f == "f32" ? 1 : f == "s32" ? 2 : f == "s24" ? 3 : f == "s16" ? 4 : -1;
+    if (fmt < 0) throw std::invalid_argument("format must be f64, f32, s32, s24 or s16");
+    const int in_fmt = sf == "f64"   ? KBSRC_GPU_IN_F64
+                       : sf == "f32" ? KBSRC_GPU_IN_F32
+                       : sf == "s32" ? KBSRC_GPU_IN_S32
+                       : sf == "s24" ? KBSRC_GPU_IN_S24
+                       : sf == "s16" ? KBSRC_GPU_IN_S16
+                       : sf == "u8"  ? KBSRC_GPU_IN_U8
+                                     : -1;
+    if (in_fmt < 0) throw std::invalid_argument("sample format must be f64, f32, s32, s24, s16 or u8");
+    RoundToNearest rn(opt.precision == Precision::Exact || opt.precision == Precision::SplitTC);
+    auto cv = prepare(pcm, frames, channels, rate_in, rate_out, opt, true, nullptr, in_fmt);
+    if (cv->pl.copy) throw std::invalid_argument("equal rates: nothing to convert");
+    const double t1 = now();
+    const int bps = fmt == 0 ? 8 : fmt == 3 ? 3 : fmt == 4 ? 2 : 4;
+    std::vector<unsigned char> data((size_t)(cv->pl.nout * channels * bps));
+    gpu_check(kbsrc_gpu_engine_run_host_packed(cv->eng.e, static_cast<const double*>(pcm), cv->head.data(),
+                                               cv->tail.data(), fmt, dither ? 1 : 0, data.data(), &clipped),
               "GPU engine");
     fill_stats(*cv, stats, now() - t1);
     return data;

@@ -29,7 +29,39 @@ int bytes_per_sample(const std::string& fmt) { return fmt == "f64" ? 8 : fmt == 
 
 }  // namespace
 
-Audio read_wav(const char* path) {
+namespace {
+// Decodes m samples of `bps` bytes (tag 1 PCM or tag 3 IEEE float) from p into o.
+void decode_samples(const uint8_t* p, size_t m, bool is_float, int bits, int bps, double* o) {
+    if (is_float && bits == 64) {
+        std::memcpy(o, p, 8 * m);
+    } else if (is_float) {
+        for (size_t k = 0; k < m; k++) {
+            float v;
+            std::memcpy(&v, p + 4 * k, 4);
+            o[k] = v;
+        }
+    } else if (bps == 1) {
+        for (size_t k = 0; k < m; k++) o[k] = ((int)p[k] - 128) / 128.0;
+    } else if (bps == 2) {
+        for (size_t k = 0; k < m; k++) o[k] = (int16_t)(p[2 * k] | p[2 * k + 1] << 8) / 32768.0;
+    } else if (bps == 3) {
+        for (size_t k = 0; k < m; k++) {
+            int32_t v = p[3 * k] | p[3 * k + 1] << 8 | p[3 * k + 2] << 16;
+            if (v & 0x800000) v -= 1 << 24;
+            o[k] = v / 8388608.0;
+        }
+    } else {
+        for (size_t k = 0; k < m; k++) {
+            const uint8_t* q = p + 4 * k;
+            o[k] = (int32_t)(q[0] | q[1] << 8 | q[2] << 16 | (uint32_t)q[3] << 24) / 2147483648.0;
+        }
+    }
+}
+
+int sample_bytes(const Audio& a) { return a.fmt_float ? a.fmt_bits / 8 : (a.fmt_bits + 7) / 8; }
+
+// Header checks and the data section; raw: keep the bytes, else decode them.
+Audio read_impl(const char* path, bool raw) {
     FileCloser fc{std::fopen(path, "rb")};
     FILE* f = fc.f;
     if (!f) fail("cannot open input");
@@ -83,42 +115,34 @@ Audio read_wav(const char* path) {
     a.fmt_bits = bits;
     a.fmt_float = tag == 3;
     a.frames = data_len / align;
+    static const char* const pcm[] = {"u8", "s16", "s24", "s32"};
+    a.sample_format = a.fmt_float ? (bits == 64 ? "f64" : "f32") : pcm[bps - 1];
     const size_t n = (size_t)a.frames * ch;
-    a.d.resize(n);
     fseeko(f, data_pos, SEEK_SET);
+    if (raw) {
+        a.raw.resize(n * bps);
+        if (n && std::fread(a.raw.data(), (size_t)bps, n, f) != n) fail("read error");
+        return a;
+    }
+    a.d.resize(n);
     const size_t chunk = (size_t)1 << 20;
     std::vector<uint8_t> buf(chunk * bps);
     for (size_t k0 = 0; k0 < n; k0 += chunk) {
         const size_t m = std::min(chunk, n - k0);
         if (std::fread(buf.data(), (size_t)bps, m, f) != m) fail("read error");
-        const uint8_t* p = buf.data();
-        double* o = a.d.data() + k0;
-        if (tag == 3 && bits == 64) {
-            std::memcpy(o, p, 8 * m);
-        } else if (tag == 3) {
-            for (size_t k = 0; k < m; k++) {
-                float v;
-                std::memcpy(&v, p + 4 * k, 4);
-                o[k] = v;
-            }
-        } else if (bps == 1) {
-            for (size_t k = 0; k < m; k++) o[k] = ((int)p[k] - 128) / 128.0;
-        } else if (bps == 2) {
-            for (size_t k = 0; k < m; k++) o[k] = (int16_t)(p[2 * k] | p[2 * k + 1] << 8) / 32768.0;
-        } else if (bps == 3) {
-            for (size_t k = 0; k < m; k++) {
-                int32_t v = p[3 * k] | p[3 * k + 1] << 8 | p[3 * k + 2] << 16;
-                if (v & 0x800000) v -= 1 << 24;
-                o[k] = v / 8388608.0;
-            }
-        } else {
-            for (size_t k = 0; k < m; k++) {
-                const uint8_t* q = p + 4 * k;
-                o[k] = (int32_t)(q[0] | q[1] << 8 | q[2] << 16 | (uint32_t)q[3] << 24) / 2147483648.0;
-            }
-        }
+        decode_samples(buf.data(), m, a.fmt_float, bits, bps, a.d.data() + k0);
     }
     return a;
+}
+}  // namespace
+
+Audio read_wav(const char* path) { return read_impl(path, false); }
+Audio read_wav_raw(const char* path) { return read_impl(path, true); }
+
+void decode_wav(Audio& a) {
+    const size_t n = (size_t)a.frames * a.ch;
+    a.d.resize(n);
+    if (n) decode_samples(a.raw.data(), n, a.fmt_float, a.fmt_bits, sample_bytes(a), a.d.data());
 }
 
 void check_wav_output(int ch, int rate, const std::string& fmt) {

@@ -11,12 +11,18 @@ namespace kbsrc::io {
 struct Audio {
     int rate = 0, ch = 0;
     long long frames = 0;
-    std::vector<double> d;  // interleaved
+    std::vector<double> d;  // interleaved, decoded (read_wav)
     int fmt_bits = 0;
     bool fmt_float = false;
+    std::vector<unsigned char> raw;  // the data section as stored (read_wav_raw), frames * ch samples
+    std::string sample_format;      // its sample format: "u8", "s16", "s24", "s32", "f32" or "f64"
 };
 
 Audio read_wav(const char* path);
+// The same checks and header parsing as read_wav, but the samples stay as stored in the file (raw,
+// sample_format); decode_wav fills d from them.
+Audio read_wav_raw(const char* path);
+void decode_wav(Audio& a);
 // Fails when a WAV header in `format` cannot describe ch channels at this rate.
 void check_wav_output(int ch, int rate, const std::string& format);
 // y: planar samples. Integer formats are scaled, optionally TPDF-dithered (two uniform draws per sample from

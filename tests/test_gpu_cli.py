@@ -114,3 +114,27 @@ def test_gpu_pack_equals_reference_writer(tmp_path, fmt, dither):
     assert got == want
     m = re.search(r"warning: (\d+) samples clipped", r.stderr)
     assert clipped == (int(m.group(1)) if m else 0)
+
+
+@pytest.mark.skipif(not os.path.exists(oracle.REF_CLI), reason="reference CLI not built (oracle/_ref)")
+@pytest.mark.parametrize("tag,bits,width", [(1, 8, 1), (1, 16, 2), (1, 20, 3), (1, 24, 3), (1, 32, 4), (3, 32, 4),
+                                            (3, 64, 8)])
+def test_cli_input_formats_equal_reference_cli(tmp_path, tag, bits, width):
+    """The GPU decodes the WAV data section itself (the CLI hands it over as stored): every input sample format
+    gives the reference CLI's output bytes."""
+    from test_host import wav
+    rng = np.random.default_rng(bits + width)
+    n, ch = 30000, 3
+    if tag == 3:
+        data = rng.uniform(-0.9, 0.9, n * ch).astype("<f4" if width == 4 else "<f8").tobytes()
+    else:
+        v = rng.integers(0, 256, (n * ch, width), dtype=np.uint8)
+        data = v.tobytes()
+    src = tmp_path / "in.wav"
+    src.write_bytes(wav(tag, ch, 48000, bits, ch * width, data))
+    a, b = tmp_path / "a.wav", tmp_path / "b.wav"
+    args = ["--rate", 44100, "--format", "s24", "--dither"]
+    ra = cli(*args, src, a)
+    rb = cli(*args, src, b, binary=oracle.REF_CLI)
+    assert ra.returncode == rb.returncode == 0, (ra.stderr, rb.stderr)
+    assert a.read_bytes() == b.read_bytes()
