@@ -280,6 +280,7 @@ def product_arm(args, w, world, rank, local, pg):
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
+    tuned = cv.tune(*ptrs, stream=stream) if args.tune else None
     if pg:
         pg.barrier()
     vis = os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",")
@@ -401,6 +402,8 @@ def product_arm(args, w, world, rank, local, pg):
                              "time (Stats::process_seconds), all host threads",
                    "value_t8": round(c_8["engine_msps"], 3), "whole_call_msps": round(c_all["wall_msps"], 3)}
     extra = {}
+    if tuned is not None:
+        extra["tuned_shapes"] = tuned
     if w.get("pcm24") and not args.seconds:  # the tool a user runs, on the 24-bit file, ours and the reference's
         extra["cli_e2e"] = cli_e2e(w)
     if split:  # the comparison the form exists for: accuracy against exact, throughput against plain exact
@@ -586,6 +589,8 @@ def main():
     ap.add_argument("--impl", default="product", choices=["product", "reference"])
     ap.add_argument("--workload", default="c2_exact", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    ap.add_argument("--no-tune", dest="tune", action="store_false",
+                    help="skip the autotuner (launch shapes per pass, chosen after warm-up, before timing)")
     ap.add_argument("--seconds", type=float, default=None,
                     help="shorter input of the same workload (profiling captures of a small case)")
     args = ap.parse_args()

@@ -107,6 +107,16 @@ int kbsrc_gpu_engine_run_host_packed(kbsrc_gpu_engine* e, const double* in, cons
 int kbsrc_gpu_pack(const double* d_planar, int channels, long long frames, long long stride, int format, int dither,
                    unsigned char* d_out, long long* clipped, void* stream);
 
+/* Autotuner: picks the launch shape (sequences per CTA, threads per CTA, hence shared-memory staging) of each
+ * four-step pass (forward column and row, inverse column and row) by timing whole device-resident runs on the
+ * given buffers: every candidate shape is applied to all passes at once, each pass keeps its fastest. The radix
+ * order and the block size are never changed, so the output bytes are the same under every shape. Runs the
+ * conversion many times (d_out holds a valid result afterwards); synchronous. shapes: 8 ints out, F and T of the
+ * four passes (0 for a pass that is not a four-step pass: direct, Bluestein or split-precision transforms).
+ * Not in the reference (its engines have no launch shapes). */
+int kbsrc_gpu_engine_tune(kbsrc_gpu_engine* e, const double* d_in, const double* d_head, const double* d_tail,
+                          double* d_out, void* stream, int* shapes);
+
 /* Number of (channel, block) tasks, kernel launches per run, and the engine's device bytes. */
 int kbsrc_gpu_engine_info(const kbsrc_gpu_engine* e, long long* tasks, long long* launches,
                           long long* device_bytes);

@@ -86,6 +86,8 @@ GPU_SYMBOLS = {
     "kbsrc_gpu_batch_destroy": (None, [ctypes.c_void_p]),
     "kbsrc_gpu_last_error": (ctypes.c_char_p, []),
     "kbsrc_gpu_engine_name": (ctypes.c_char_p, []),
+    "kbsrc_gpu_engine_tune": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                             ctypes.c_void_p, ctypes.c_void_p, _P(ctypes.c_int)]),
 }
 HOST_SYMBOLS = {
     "kbsrc_output_frames": (ctypes.c_longlong, [ctypes.c_longlong, ctypes.c_int, ctypes.c_int]),
@@ -254,6 +256,16 @@ class Conversion:
         if rc:
             raise RuntimeError(f"kbsrc_gpu_engine_run_device_timed: {rc} {gpu_error()}")
         return {k: (ms[i], n[i]) for i, k in enumerate(self.PASSES)}
+
+    def tune(self, d_in, d_head, d_tail, d_out, stream=0):
+        """Autotuner (kbsrc_gpu_engine_tune): times launch shapes on these device buffers and keeps the fastest
+        per four-step pass; returns {pass: (sequences per CTA, threads)} for the passes it tuned."""
+        sh = (ctypes.c_int * 8)()
+        rc = gpu_lib().kbsrc_gpu_engine_tune(self.engine, d_in, d_head, d_tail, d_out, stream or None, sh)
+        if rc:
+            raise RuntimeError(f"kbsrc_gpu_engine_tune: {rc} {gpu_error()}")
+        names = ["fwd_column", "fwd_row", "inv_column", "inv_row"]
+        return {names[i]: (sh[2 * i], sh[2 * i + 1]) for i in range(4) if sh[2 * i]}
 
     def run_host_raw(self, x_ptr, head_ptr, tail_ptr, out_ptr):
         """Engine run on host pointers (ints), e.g. pinned buffers; synchronous."""

@@ -1,0 +1,34 @@
+"""The autotuner (kbsrc_gpu_engine_tune) changes only launch shapes: after tuning, the conversion still writes
+the reference's bytes, and every four-step pass has a shape."""
+import hashlib
+
+import numpy as np
+import pytest
+import torch
+
+import kbsrc_b200
+from cases import CASES, make_input
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("name", ["c1_96k_44k1_exact", "s_96k_44k1_fast_20000", "s_44k1_48k_exact_30000"])
+def test_tuned_engine_keeps_reference_bytes(golden, name):
+    recipe, fi, fo, opts = CASES[name]
+    x = make_input(recipe)
+    cv = kbsrc_b200.Conversion(x, fi, fo, mode=opts.get("mode", "exact"))
+    dev = torch.device("cuda")
+    d_in = torch.from_numpy(x).to(dev)
+    d_h = torch.from_numpy(cv.head if cv.head.size else np.zeros(1)).to(dev)
+    d_t = torch.from_numpy(cv.tail if cv.tail.size else np.zeros(1)).to(dev)
+    d_out = torch.empty(x.shape[1] * cv.nout, dtype=torch.float64, device=dev)
+    p = (d_in.data_ptr(), d_h.data_ptr(), d_t.data_ptr(), d_out.data_ptr())
+    shapes = cv.tune(*p)
+    assert set(shapes) == {"fwd_column", "fwd_row", "inv_column", "inv_row"}
+    assert all(f >= 1 and t >= 64 for f, t in shapes.values())
+    cv.run_device(*p)
+    torch.cuda.synchronize()
+    y = d_out.cpu().numpy().reshape(x.shape[1], cv.nout)
+    assert hashlib.sha256(y.astype("<f8").tobytes()).hexdigest() == golden[name]["sha256"]
+    z = cv.run(x)  # the host path with the tuned shapes
+    assert hashlib.sha256(z.astype("<f8").tobytes()).hexdigest() == golden[name]["sha256"]
