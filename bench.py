@@ -218,9 +218,23 @@ def reference_arm(args, w, world, rank, pg):
         pg.destroy_process_group()
 
 
-def cli_e2e(w):
-    """Wall time of the kbsrc command line on the workload's 24-bit WAV file (read, decode, kernel design, LPC,
-    conversion, output step with dither, write), ours and the reference tool built from source."""
+def write_f64_wav(path, x, rate):
+    """A float64 WAV file (18-byte fmt chunk, fact chunk) of interleaved samples x (frames x channels)."""
+    import struct
+    frames, ch = x.shape
+    n = frames * ch * 8
+    fmt = struct.pack("<HHIIHHH", 3, ch, rate, rate * 8 * ch, 8 * ch, 64, 0)
+    with open(path, "wb") as f:
+        f.write(b"RIFF" + struct.pack("<I", 4 + 8 + len(fmt) + 12 + 8 + n) + b"WAVE" + b"fmt " +
+                struct.pack("<I", len(fmt)) + fmt + b"fact" + struct.pack("<II", 4, frames) + b"data" +
+                struct.pack("<I", n))
+        f.write(np.ascontiguousarray(x, dtype="<f8").tobytes())
+
+
+def cli_e2e(w, x):
+    """Wall time of the kbsrc command line on the workload as a WAV file (read, decode, kernel design, LPC,
+    conversion, output step, write), ours and the reference tool built from source: the 24-bit file with s24
+    dithered output for PCM workloads, else the float64 file with float64 output."""
     import subprocess
     import tempfile
     import kbsrc_b200
@@ -229,9 +243,14 @@ def cli_e2e(w):
     out = {}
     with tempfile.TemporaryDirectory() as d:
         src = os.path.join(d, "in.wav")
-        write_pcm24_wav(src, pcm24_ints(w["seed"], w["seconds"], w["rate_in"], w["channels"]), w["rate_in"])
-        args = ["--rate", str(w["rate_out"]), "--len", str(w["length"]), "--beta", str(w["beta"]), "--format", "s24",
-                "--dither", src]
+        args = ["--rate", str(w["rate_out"]), "--len", str(w.get("length", 0.2)), "--beta", str(w.get("beta", 40.0)),
+                "--mode", w["mode"]]
+        if w.get("pcm24"):
+            write_pcm24_wav(src, pcm24_ints(w["seed"], w["seconds"], w["rate_in"], w["channels"]), w["rate_in"])
+            args += ["--format", "s24", "--dither", src]
+        else:
+            write_f64_wav(src, x, w["rate_in"])
+            args += ["--format", "f64", src]
         tools = [("ours", kbsrc_b200.CLI)] + ([("reference", oracle.REF_CLI)] if os.path.exists(oracle.REF_CLI) else [])
         for name, exe in tools:
             dst = os.path.join(d, name + ".wav")
@@ -241,7 +260,7 @@ def cli_e2e(w):
             out[name + "_ok"] = r.returncode == 0
             if os.path.exists(dst):
                 os.remove(dst)
-    out["input_bytes"] = int(w["seconds"] * w["rate_in"]) * w["channels"] * 3
+        out["input_bytes"] = os.path.getsize(src)
     return out
 
 
@@ -404,8 +423,8 @@ def product_arm(args, w, world, rank, local, pg):
     extra = {}
     if tuned is not None:
         extra["tuned_shapes"] = tuned
-    if w.get("pcm24") and not args.seconds:  # the tool a user runs, on the 24-bit file, ours and the reference's
-        extra["cli_e2e"] = cli_e2e(w)
+    if (w.get("pcm24") or not args.no_cpu) and not args.seconds and world == 1 and not split:
+        extra["cli_e2e"] = cli_e2e(w, x)  # the tool a user runs, on the workload's file, ours and the reference's
     if split:  # the comparison the form exists for: accuracy against exact, throughput against plain exact
         ref = kbsrc_b200.Conversion(x, w["rate_in"], w["rate_out"], mode="exact", **kw)
         fast = kbsrc_b200.Conversion(x, w["rate_in"], w["rate_out"], mode="fast", **kw)
