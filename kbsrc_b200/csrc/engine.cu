@@ -215,6 +215,7 @@ __global__ void __launch_bounds__(Ar::kMaxThreads, Ar::kMinBlocks) k_column(cons
     extern __shared__ __align__(16) unsigned char smem[];
     using C = CxR<Ar>;
     const int F = P.F, N1 = P.N1, N2 = P.N2, total = N1 * F;
+    const FastDiv dF = fast_div(F);
     Planes<Ar> A, B;
     unsigned char* rest = carve<Ar>(smem, total, A, B);
     const long long task = P.task0 + blockIdx.y;
@@ -227,7 +228,7 @@ __global__ void __launch_bounds__(Ar::kMaxThreads, Ar::kMinBlocks) k_column(cons
         C v[kLoadBatch];
 #pragma unroll
         for (int j = 0; j < kLoadBatch; j++) {
-            const int e = e0 + j * blockDim.x, r = e / F, n2 = c0 + (e - r * F);
+            const int e = e0 + j * blockDim.x, r = (int)fdiv(e, dF), n2 = c0 + (e - r * F);
             if (e < total) v[j] = n2 < N2 ? load_input<Ar, SRC>(P, ts, src, (long long)r * N2 + n2) : czero<Ar>();
         }
 #pragma unroll
@@ -241,12 +242,12 @@ __global__ void __launch_bounds__(Ar::kMaxThreads, Ar::kMinBlocks) k_column(cons
         CxW<Ar> w[kLoadBatch];
 #pragma unroll
         for (int j = 0; j < kLoadBatch; j++) {
-            const int e = e0 + j * blockDim.x, k1 = e / F, n2 = c0 + (e - k1 * F);
+            const int e = e0 + j * blockDim.x, k1 = (int)fdiv(e, dF), n2 = c0 + (e - k1 * F);
             if (e < total && n2 < N2 && k1 && (Ar::kLanes || n2)) w[j] = ld_tw(P.tw4 + (long long)k1 * N2 + n2);
         }
 #pragma unroll
         for (int j = 0; j < kLoadBatch; j++) {
-            const int e = e0 + j * blockDim.x, k1 = e / F, n2 = c0 + (e - k1 * F);
+            const int e = e0 + j * blockDim.x, k1 = (int)fdiv(e, dF), n2 = c0 + (e - k1 * F);
             if (e >= total || n2 >= N2) continue;
             C v = res.ld(e);
             if (k1 && (Ar::kLanes || n2)) v = c_mulw<Ar>(v, w[j]);
@@ -263,6 +264,7 @@ __global__ void __launch_bounds__(Ar::kMaxThreads, Ar::kMinBlocks) k_row(const _
     extern __shared__ __align__(16) unsigned char smem[];
     using C = CxR<Ar>;
     const int F = P.F, N1 = P.N1, N2 = P.N2, total = N2 * F;
+    const FastDiv dF = fast_div(F), dN2 = fast_div(N2);
     Planes<Ar> A, B;
     unsigned char* rest = carve<Ar>(smem, total, A, B);
     const long long task = P.task0 + blockIdx.y;
@@ -273,12 +275,12 @@ __global__ void __launch_bounds__(Ar::kMaxThreads, Ar::kMinBlocks) k_row(const _
         C v[kLoadBatch];
 #pragma unroll
         for (int j = 0; j < kLoadBatch; j++) {
-            const int e = e0 + j * blockDim.x, f = e / N2, i = e - f * N2, row = r0 + f;
+            const int e = e0 + j * blockDim.x, f = (int)fdiv(e, dN2), i = e - f * N2, row = r0 + f;
             if (e < total) v[j] = row < N1 ? src[(long long)row * N2 + i] : czero<Ar>();
         }
 #pragma unroll
         for (int j = 0; j < kLoadBatch; j++) {
-            const int e = e0 + j * blockDim.x, f = e / N2, i = e - f * N2;
+            const int e = e0 + j * blockDim.x, f = (int)fdiv(e, dN2), i = e - f * N2;
             if (e < total) A.st(i * F + f, v[j]);
         }
     }
@@ -288,7 +290,7 @@ __global__ void __launch_bounds__(Ar::kMaxThreads, Ar::kMinBlocks) k_row(const _
     const TaskRef tr = DST == kDstOutput ? task_ref(P.work, task) : TaskRef{0, 0, 0};
     const Item it = DST == kDstOutput ? item_of(P.work, tr) : Item{};
     for (int e = threadIdx.x; e < total; e += blockDim.x) {
-        const int k2 = e / F, f = e - k2 * F, row = r0 + f;
+        const int k2 = (int)fdiv(e, dF), f = e - k2 * F, row = r0 + f;
         if (row >= N1) continue;
         C v = res.ld(e);
         if (Ar::kLaneRenorm) v = c_renorm<Ar>(v);
@@ -713,6 +715,9 @@ int build_cfft(int n, HostCfft& c) {
         c.N2 = n / best;
         if (c.N1 < 8) c.four = 0;
     }
+    // the passes divide indices through fast_div, exact while index * divisor < 2^32: sub-FFTs up to 2^15 points
+    if ((c.four ? std::max(c.N1, c.N2) : n) > 32768)
+        return fail(KBSRC_GPU_E_UNSUPPORTED, "FFT length without a four-step split into sub-FFTs of at most 32768");
     if (!c.four) return build_sub(n, c.tw_stage, c.sd);
     int rc = build_sub(c.N1, c.tw_stage, c.s1);
     if (rc) return rc;

@@ -14,6 +14,20 @@ namespace kbsrc::dev {
 
 constexpr int kMaxStages = 16;
 
+// Division by a divisor that is fixed for a loop, through its rounded-up reciprocal m = ceil(2^32 / d) =
+// floor((2^32 - 1) / d) + 1: (n * m) >> 32 is floor(n / d) whenever n * d < 2^32, which every index range of the
+// passes satisfies (n < 2^22, d < 2^12). One division sets it up; each use is one 64-bit multiply.
+struct FastDiv {
+    unsigned d;
+    unsigned long long m;
+};
+__host__ __device__ __forceinline__ FastDiv fast_div(unsigned d) {
+    return FastDiv{d, (unsigned long long)(0xFFFFFFFFu / d) + 1ull};
+}
+__device__ __forceinline__ unsigned fdiv(unsigned n, const FastDiv& f) {
+    return (unsigned)(((unsigned long long)n * f.m) >> 32);
+}
+
 struct Stage {
     int r, m, s;  // radix, butterflies per (p) group count m = n_left/r, output stride s
     int tw;       // offset of this stage's twiddles (complex table entries), laid out [p*(r-1) + u-1]
@@ -174,8 +188,9 @@ __device__ __forceinline__ Planes<Ar> stockham(const SubPlan& sp, Planes<Ar> a, 
         const int r = sp.st[g].r, m = sp.st[g].m, s = sp.st[g].s;
         const CxW<Ar>* twg = tws + (sp.st[g].tw - sp.tw0);
         const int total = m * s * F, sin = s * m * F, sout = s * F;
+        const FastDiv dF = fast_div(F), ds = fast_div(s);
         for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
-            const int f = idx % F, bf = idx / F, q = bf % s, p = bf / s;
+            const int bf = (int)fdiv(idx, dF), f = idx - bf * F, p = (int)fdiv(bf, ds), q = bf - p * s;
             const int ia = (s * p + q) * F + f, ib = (s * r * p + q) * F + f;
             const CxW<Ar>* t = twg + p * (r - 1);
             const bool p0 = p == 0;
