@@ -62,6 +62,11 @@ std::vector<unsigned char> resample_wav_pcm(const void* pcm, const char* sample_
                                             int channels, int rate_in, int rate_out, const char* format, bool dither,
                                             long long& clipped, const Options& options = {}, Stats* stats = nullptr);
 
+// Starts the GPU's initialisation (CUDA context, kernel attributes) on a background thread and returns at once.
+// Optional: the first conversion starts it too, overlapped with its host-side LPC and kernel taps; a caller that
+// knows a conversion is coming (a tool about to read its input file) can start it earlier. Not in the reference.
+void warm_up();
+
 const char* version();
 
 }  // namespace kbsrc

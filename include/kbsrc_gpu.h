@@ -68,6 +68,11 @@ typedef struct {
     int in_format;      /* KBSRC_GPU_IN_*: the input's sample format (0, float64, when zero-initialised) */
 } kbsrc_gpu_desc;
 
+/* Initialises the current CUDA device for the engine (context, kernel attributes). Optional: the first engine
+ * or spectrum call does it otherwise. A caller may run it on another thread while it does host work, since
+ * creating a CUDA context takes a good fraction of a second. Not in the reference (no GPU). */
+int kbsrc_gpu_init(void);
+
 /* Creates an engine on the current CUDA device: FFT plans, twiddle tables and the kernel spectrum on the
  * device. Replaces the set-up half of run_engine (src/resampler.cpp:38-40). */
 int kbsrc_gpu_engine_create(const kbsrc_gpu_desc* desc, kbsrc_gpu_engine** out);

@@ -88,6 +88,7 @@ GPU_SYMBOLS = {
     "kbsrc_gpu_engine_name": (ctypes.c_char_p, []),
     "kbsrc_gpu_engine_tune": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                              ctypes.c_void_p, ctypes.c_void_p, _P(ctypes.c_int)]),
+    "kbsrc_gpu_init": (ctypes.c_int, []),
 }
 HOST_SYMBOLS = {
     "kbsrc_output_frames": (ctypes.c_longlong, [ctypes.c_longlong, ctypes.c_int, ctypes.c_int]),

@@ -1967,6 +1967,17 @@ size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
 
 extern "C" {
 
+int kbsrc_gpu_init(void) {
+    try {
+        int rc;
+        if ((rc = require_device()) != KBSRC_GPU_OK) return rc;
+        KB_CUDA(cudaFree(nullptr));  // creates the context
+        return allow_large_smem();
+    } catch (const std::exception& x) {
+        return fail(KBSRC_GPU_E_CUDA, x.what());
+    }
+}
+
 int kbsrc_gpu_engine_create(const kbsrc_gpu_desc* desc, kbsrc_gpu_engine** out) {
     if (!out) return fail(KBSRC_GPU_E_ARG, "null output pointer");
     *out = nullptr;

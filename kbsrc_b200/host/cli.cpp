@@ -105,6 +105,7 @@ int run(int argc, char** argv) {
         throw UsageError("format must be f64, f32, s32, s24 or s16");
 
     const double t0 = now();
+    kbsrc::warm_up();  // the GPU starts while the file is read
     kbsrc::io::Audio a = kbsrc::io::read_wav_raw(in_path.c_str());  // decoded on the GPU while converting
     if (a.rate > 10000000) throw std::runtime_error("input sample rate above 10000000 Hz");
     kbsrc::io::check_wav_output(a.ch, rate, format);  // fail before converting

@@ -13,6 +13,9 @@
 #include <cstdint>
 #include <cmath>
 #include <cstring>
+#include <future>
+#include <cstdio>
+#include <cstdlib>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -21,6 +24,7 @@
 #include <stdexcept>
 #include <string>
 #include <thread>
+#include <utility>
 #include <vector>
 #if defined(__x86_64__) || defined(__i386__)
 #include <xmmintrin.h>
@@ -283,6 +287,35 @@ struct SpectrumCache {
     std::mutex mu;
 };
 
+// CUDA start-up (context creation and kernel attributes take a good fraction of a second) runs on its own thread
+// from the first conversion (or warm_up()) on, overlapping the host's LPC and kernel taps; gpu_ready() waits.
+// The status travels with its message: kbsrc_gpu_last_error() belongs to the thread that failed.
+std::shared_future<std::pair<int, std::string>>& gpu_init_future() {
+    static std::mutex mu;
+    static std::shared_future<std::pair<int, std::string>> f;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!f.valid())
+        f = std::async(std::launch::async, [] {
+                const int rc = kbsrc_gpu_init();
+                return std::make_pair(rc, std::string(rc ? kbsrc_gpu_last_error() : ""));
+            }).share();
+    return f;
+}
+void gpu_ready() {
+    const auto& r = gpu_init_future().get();
+    if (r.first == KBSRC_GPU_E_NOMEM) throw std::bad_alloc();
+    if (r.first) throw std::runtime_error("GPU initialisation: " + r.second);
+}
+
+// KBSRC_TRACE=1: the host phases of each preparation on stderr
+bool trace_on() {
+    static const bool on = [] {
+        const char* v = std::getenv("KBSRC_TRACE");
+        return v && *v && *v != '0';
+    }();
+    return on;
+}
+
 // Input sample i (= frame * ch + channel) of interleaved data in a KBSRC_GPU_IN_* format, decoded as the WAV
 // reader decodes it (src/io/wav.cpp:299-362); the GPU gather decodes the same way.
 double input_sample(const void* p, int fmt, long long i) {
@@ -314,6 +347,7 @@ std::unique_ptr<Conversion> prepare(const void* in, long long frames, int ch, in
     const Plan& pl = cv->pl;
     if (pl.copy) return cv;
     const double t0 = now();
+    gpu_init_future();  // start CUDA while the host works
     const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
     const int threads = opt.threads ? opt.threads : std::min(hw, 8);
     const long long Q = pl.Q, P = pl.P, Nb = (long long)pl.nb * Q, Mb = (long long)pl.nb * P;
@@ -378,8 +412,12 @@ std::unique_ptr<Conversion> prepare(const void* in, long long frames, int ch, in
             cached = true;
         }
     }
+    const double t_lpc = now();
+    double t_taps = t_lpc;
     if (!cached) {
         const std::vector<dd> taps = kaiser_taps(L, ta, tb, opt.beta, threads);
+        t_taps = now();
+        gpu_ready();
         cv->H.assign((size_t)(nspec / 2 + 1) * 2, 0.0);
         gpu_check(kbsrc_gpu_kernel_spectrum(reinterpret_cast<const double*>(taps.data()), L, nspec, (double)Nb,
                                             cv->H.data()),
@@ -410,8 +448,15 @@ std::unique_ptr<Conversion> prepare(const void* in, long long frames, int ch, in
     d.H = cv->H.data();
     d.H_len = (long long)cv->H.size() / 2;
     d.in_format = in_fmt;
-    if (make_engine) gpu_check(kbsrc_gpu_engine_create(&d, &cv->eng.e), "GPU engine");
+    const double t_spec = now();
+    if (make_engine) {
+        gpu_ready();
+        gpu_check(kbsrc_gpu_engine_create(&d, &cv->eng.e), "GPU engine");
+    }
     cv->design_seconds = now() - t0;
+    if (trace_on())
+        std::fprintf(stderr, "kbsrc trace: lpc %.3fs  taps %.3fs  spectrum (incl. GPU start) %.3fs  engine %.3fs\n",
+                     t_lpc - t0, t_taps - t_lpc, t_spec - t_taps, now() - t_spec);
     return cv;
 }
 
@@ -513,6 +558,8 @@ std::vector<unsigned char> resample_wav_pcm(const void* pcm, const char* sample_
     fill_stats(*cv, stats, now() - t1);
     return data;
 }
+
+void warm_up() { gpu_init_future(); }
 
 const char* version() { return KBSRC_VERSION; }
 
