@@ -138,3 +138,26 @@ def test_cli_input_formats_equal_reference_cli(tmp_path, tag, bits, width):
     rb = cli(*args, src, b, binary=oracle.REF_CLI)
     assert ra.returncode == rb.returncode == 0, (ra.stderr, rb.stderr)
     assert a.read_bytes() == b.read_bytes()
+
+
+@pytest.mark.skipif(not os.path.exists(oracle.REF_CLI), reason="reference CLI not built (oracle/_ref)")
+@pytest.mark.parametrize("frames", [0, 1, 2, 97])
+@pytest.mark.parametrize("tag,bits,width", [(1, 24, 3), (1, 16, 2), (3, 64, 8)])
+def test_cli_tiny_files_equal_reference_cli(tmp_path, frames, tag, bits, width):
+    """Empty and tiny data sections through the raw-input path give the reference CLI's bytes."""
+    from test_host import wav
+    rng = np.random.default_rng(frames + bits)
+    ch = 2
+    if tag == 3:
+        data = rng.uniform(-0.9, 0.9, frames * ch).astype("<f8").tobytes()
+    else:
+        data = rng.integers(0, 256, (frames * ch, width), dtype=np.uint8).tobytes()
+    src = tmp_path / "in.wav"
+    src.write_bytes(wav(tag, ch, 48000, bits, ch * width, data))
+    a, b = tmp_path / "a.wav", tmp_path / "b.wav"
+    args = ["--rate", 44100, "--format", "s16", "--dither"]
+    ra = cli(*args, src, a)
+    rb = cli(*args, src, b, binary=oracle.REF_CLI)
+    assert ra.returncode == rb.returncode, (ra.stderr, rb.stderr)
+    if rb.returncode == 0:
+        assert a.read_bytes() == b.read_bytes()

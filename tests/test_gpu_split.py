@@ -48,3 +48,10 @@ def test_split_runs_twice_the_same():
     cv = kbsrc_b200.Conversion(x, 96000, 44100, mode="split")
     a, b = cv.run(x), cv.run(x)
     assert np.array_equal(a, b)
+
+
+def test_split_rejects_lengths_without_radix_32_factorisation():
+    """22050 -> 48001 needs Bluestein transforms: the split form refuses it with a clear error, no fallback."""
+    x = np.random.default_rng(1).uniform(-0.5, 0.5, (3000, 1))
+    with pytest.raises(RuntimeError, match="split-precision form"):
+        kbsrc_b200.resample(x, 22050, 48001, mode="split")
