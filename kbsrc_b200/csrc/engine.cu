@@ -21,10 +21,13 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <future>
 #include <memory>
 #include <mutex>
 #include <new>
+#include <stdexcept>
 #include <string>
+#include <thread>
 #include <type_traits>
 #include <vector>
 
@@ -1134,6 +1137,20 @@ struct kbsrc_gpu_batch {
     }
 };
 
+// Copies between pageable host memory and the device through two pinned bounce buffers: the host-side copy of
+// one chunk (split over threads) overlaps the DMA of the other. Pinned host memory is copied directly.
+struct Stager {
+    static constexpr size_t kChunk = (size_t)32 << 20;
+    void* pin[2] = {nullptr, nullptr};
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    ~Stager() {
+        for (int i = 0; i < 2; i++) {
+            if (pin[i]) cudaFreeHost(pin[i]);
+            if (ev[i]) cudaEventDestroy(ev[i]);
+        }
+    }
+};
+
 struct kbsrc_gpu_engine : PlanCore {
     int device = 0;
     long long tasks = 0, wave = 0, stride = 0, launches = 0;
@@ -1142,8 +1159,11 @@ struct kbsrc_gpu_engine : PlanCore {
     cudaEvent_t ev_in[2] = {}, ev_done[2] = {};
     DevBuf bufA, bufB;
     DevBuf d_in, d_head, d_tail, d_out;
+    Stager stager;                    // pageable host buffers of run_host / run_host_packed
+    cudaStream_t side = nullptr;      // run_host_packed's dither generator
     std::vector<cudaEvent_t> events;  // per-pass timing trail, created on first use
     ~kbsrc_gpu_engine() {
+        if (side) cudaStreamDestroy(side);
         for (cudaEvent_t x : events) cudaEventDestroy(x);
         for (cudaEvent_t x : {ev_in[0], ev_in[1], ev_done[0], ev_done[1]})
             if (x) cudaEventDestroy(x);
@@ -1661,8 +1681,9 @@ int run_device_impl(kbsrc_gpu_engine* e, const double* in, const double* head, c
 // formats, scales by 2^(8B-1), adds two draws of uniform_real_distribution<double>(-0.5, 0.5) from
 // std::mt19937_64 seeded 12345 per sample (frame-major, channel-minor), rounds to nearest, clips and counts the
 // clipped samples. The packer reproduces it sample for sample; the dither stream is the same generator run on the
-// GPU (MT19937-64, Matsumoto and Nishimura 2000): one CTA updates the 312-word state in parallel in the order the
-// sequential twist would, then tempers 312 outputs, two per sample.
+// GPU (MT19937-64, Matsumoto and Nishimura 2000). The stream is cut into chunks of 2^20 draws; a jump-ahead tree
+// finds each chunk's start state and one CTA per chunk then runs the generator: it updates the 312-word state in
+// parallel in the order the sequential twist would and tempers 312 outputs, two per sample.
 namespace {
 
 constexpr int kMtN = 312, kMtM = 156;
@@ -1684,36 +1705,279 @@ __device__ __forceinline__ double mt_uniform(unsigned long long u) {
     return __dadd_rn(__dmul_rn(r, 1.0), -0.5);
 }
 
-// D[k] = U(draw 2k) + U(draw 2k+1) for k < n: the dither added to sample k (frame-major, channel-minor)
-__global__ void __launch_bounds__(320) k_dither(unsigned long long seed, long long n, double* __restrict__ D) {
-    __shared__ unsigned long long st[kMtN];
-    const int t = threadIdx.x;
-    if (t == 0) {  // seeding is a sequential recurrence
-        st[0] = seed;
-        for (int i = 1; i < kMtN; i++) st[i] = 6364136223846793005ULL * (st[i - 1] ^ (st[i - 1] >> 62)) + i;
+__device__ __forceinline__ unsigned long long mt_twist(unsigned long long a, unsigned long long b) {
+    const unsigned long long x = (a & kMtUpper) | (b & kMtLower);
+    return (x >> 1) ^ ((x & 1) ? kMtA : 0ULL);
+}
+
+// Jump-ahead (Haramoto, Matsumoto, Nishimura, Panneton and L'Ecuyer 2008, "Efficient jump ahead for F2-linear
+// random number generators"). The generator is linear over GF(2). Write x_k for its untempered words (x_0..x_311
+// the seeded state, draw d = temper(x_{312+d})) and W_k = (x_k .. x_{k+311}) for the window at k. For k >= 1 the
+// windows lie in the 19937-dimensional subspace on which the transition A has the primitive characteristic
+// polynomial phi, so A^J W = g(A) W for g = x^J mod phi, and word i of g(A) W_s is the XOR of x_{s+k+i} over the
+// set coefficients k of g. kMtChunk draws make one chunk; W[c] holds the window x_{312+c*kMtChunk} .. .
+constexpr int kMtDeg = 19937;                            // degree of phi; polynomials below it fit kMtN words
+constexpr int kMtSeq = kMtDeg + kMtN;                    // words x_s .. x_{s+20248} the jump reads
+constexpr long long kMtChunk = 1LL << 20;                // draws per chunk (even: a chunk holds whole samples)
+constexpr int kMtJumpParts = 3, kMtJumpThreads = 320 * kMtJumpParts;
+constexpr size_t kMtJumpSmem = (size_t)(kMtSeq + kMtN + kMtJumpParts * kMtN) * 8;
+
+// W[b + half] = g(A) W[b] for b < min(half, G - half): one level of the doubling tree of chunk starts
+__global__ void __launch_bounds__(kMtJumpThreads) k_mt_jump(const unsigned long long* __restrict__ g,
+                                                           unsigned long long* __restrict__ W, int half, int G) {
+    extern __shared__ __align__(16) unsigned long long mt_sh[];
+    unsigned long long* X = mt_sh;             // kMtSeq words of the sequence from W[b]
+    unsigned long long* gs = X + kMtSeq;       // kMtN words of g
+    unsigned long long* part = gs + kMtN;      // kMtJumpParts x kMtN partial sums
+    const int b = blockIdx.x, t = threadIdx.x;
+    if (b + half >= G) return;
+    for (int i = t; i < kMtN; i += blockDim.x) {
+        X[i] = W[(size_t)b * kMtN + i];
+        gs[i] = g[i];
     }
     __syncthreads();
-    for (long long base = 0; base < n; base += kMtN / 2) {
+    // X[j + 312] = X[j + 156] ^ twist(X[j], X[j + 1]); 156 consecutive j only read words written before them
+    for (int base = kMtN; base < kMtSeq; base += kMtN - kMtM) {
+        const int o = base + t;
+        if (t < kMtN - kMtM && o < kMtSeq) X[o] = X[o - kMtM] ^ mt_twist(X[o - kMtN], X[o - kMtN + 1]);
+        __syncthreads();
+    }
+    const int p = t / 320, i = t % 320;
+    if (i < kMtN) {
+        unsigned long long acc = 0;
+        constexpr int per = kMtN / kMtJumpParts;
+        for (int w = p * per; w < (p + 1) * per; w++) {  // g's bits are warp-uniform: no divergence
+            unsigned long long gw = gs[w];
+            while (gw) {
+                const int k = 64 * w + __ffsll((long long)gw) - 1;  // k < kMtDeg, so k + i < kMtSeq
+                gw &= gw - 1;
+                acc ^= X[k + i];
+            }
+        }
+        part[p * kMtN + i] = acc;
+    }
+    __syncthreads();
+    if (t < kMtN) {
+        unsigned long long v = 0;
+#pragma unroll
+        for (int q = 0; q < kMtJumpParts; q++) v ^= part[q * kMtN + t];
+        W[(size_t)(b + half) * kMtN + t] = v;
+    }
+}
+
+// D[k] = U(draw 2k) + U(draw 2k+1) for k < n: the dither added to sample k (frame-major, channel-minor). Block c
+// makes the kMtChunk draws of chunk c from its start window W[c]: 312 draws from the window, then a twist.
+__global__ void __launch_bounds__(320) k_mt_chunks(const unsigned long long* __restrict__ W, long long n,
+                                                   double* __restrict__ D) {
+    __shared__ unsigned long long st[kMtN];
+    const int t = threadIdx.x;
+    const long long k0 = blockIdx.x * (kMtChunk / 2), k1 = min(n, k0 + kMtChunk / 2);
+    if (t < kMtN) st[t] = W[(size_t)blockIdx.x * kMtN + t];
+    __syncthreads();
+    for (long long base = k0; base < k1; base += kMtN / 2) {
+        if (t < kMtN / 2 && base + t < k1)
+            D[base + t] = __dadd_rn(mt_uniform(mt_temper(st[2 * t])), mt_uniform(mt_temper(st[2 * t + 1])));
         unsigned long long a = 0, b = 0;
         if (t < kMtN) {
             a = st[t];
             if (t + 1 < kMtN) b = st[t + 1];
         }
         __syncthreads();
-        if (t < kMtN - kMtM) {  // words 0..155 read only words not yet updated
-            const unsigned long long x = (a & kMtUpper) | (b & kMtLower);
-            st[t] = st[t + kMtM] ^ (x >> 1) ^ ((x & 1) ? kMtA : 0ULL);
-        }
+        if (t < kMtN - kMtM) st[t] = st[t + kMtM] ^ mt_twist(a, b);  // words 0..155 read only old words
         __syncthreads();
-        if (t >= kMtN - kMtM && t < kMtN) {  // words 156..311 read the updated words t-156 (and 0 for the last)
+        if (t >= kMtN - kMtM && t < kMtN) {  // words 156..311 read the new words t-156 (and 0 for the last)
             if (t == kMtN - 1) b = st[0];
-            const unsigned long long x = (a & kMtUpper) | (b & kMtLower);
-            st[t] = st[t - (kMtN - kMtM)] ^ (x >> 1) ^ ((x & 1) ? kMtA : 0ULL);
+            st[t] = st[t - (kMtN - kMtM)] ^ mt_twist(a, b);
         }
         __syncthreads();
-        if (t < kMtN / 2 && base + t < n)
-            D[base + t] = __dadd_rn(mt_uniform(mt_temper(st[2 * t])), mt_uniform(mt_temper(st[2 * t + 1])));
     }
+}
+
+// ---- host side of the jump: phi by Berlekamp-Massey, the jump polynomials by squaring mod phi -------------------
+using Words = std::vector<unsigned long long>;
+
+unsigned long long mt_twist_h(unsigned long long a, unsigned long long b) {
+    const unsigned long long x = (a & kMtUpper) | (b & kMtLower);
+    return (x >> 1) ^ ((x & 1) ? kMtA : 0ULL);
+}
+
+// untempered words x_0 .. x_{n-1} of mt19937_64(seed), n >= 312
+Words mt_words(unsigned long long seed, size_t n) {
+    Words x(n);
+    x[0] = seed;
+    for (int i = 1; i < kMtN; i++) x[i] = 6364136223846793005ULL * (x[i - 1] ^ (x[i - 1] >> 62)) + (unsigned long long)i;
+    for (size_t k = kMtN; k < n; k++) x[k] = x[k - kMtM] ^ mt_twist_h(x[k - kMtN], x[k - kMtN + 1]);
+    return x;
+}
+
+inline unsigned long long bits64(const Words& v, long long pos) {  // bits pos .. pos+63 of v (zero beyond)
+    const size_t w = (size_t)(pos >> 6);
+    const int s = (int)(pos & 63);
+    const unsigned long long lo = w < v.size() ? v[w] : 0, hi = w + 1 < v.size() ? v[w + 1] : 0;
+    return s ? (lo >> s) | (hi << (64 - s)) : lo;
+}
+
+void xor_shifted(Words& c, const Words& b, long long m, size_t bwords) {  // c ^= b * x^m
+    const size_t w = (size_t)(m >> 6);
+    const int s = (int)(m & 63);
+    for (size_t i = 0; i < bwords && i + w < c.size(); i++) {
+        c[i + w] ^= b[i] << s;
+        if (s && i + w + 1 < c.size()) c[i + w + 1] ^= b[i] >> (64 - s);
+    }
+}
+
+// Characteristic polynomial (bit j = coefficient of x^j) of bit 0 of x_312, x_313, ...; degree kMtDeg
+Words mt_phi() {
+    const int N = 2 * kMtDeg + 128;
+    const Words x = mt_words(12345, (size_t)N + kMtN);
+    const size_t nw = (size_t)(2 * N) / 64 + 4;
+    Words rs(nw, 0), C(nw, 0), B(nw, 0), T;
+    for (int n = 0; n < N; n++)  // s_n at bit N-1-n, so s_{n-i}, i = 0.. are consecutive bits from N-1-n
+        if (x[kMtN + n] & 1) rs[(size_t)(N - 1 - n) >> 6] |= 1ULL << ((N - 1 - n) & 63);
+    C[0] = B[0] = 1;
+    int L = 0;
+    long long m = 1;
+    for (int n = 0; n < N; n++) {
+        unsigned long long acc = 0;  // discrepancy: sum_{i<=L} c_i s_{n-i}
+        for (int w = 0; w <= L / 64; w++) acc ^= C[(size_t)w] & bits64(rs, (long long)(N - 1 - n) + 64LL * w);
+        if (!(__builtin_popcountll(acc) & 1)) {
+            m++;
+            continue;
+        }
+        const size_t bw = (size_t)n / 64 + 2;
+        if (2 * L <= n) {
+            T = C;
+            xor_shifted(C, B, m, bw);
+            L = n + 1 - L;
+            B.swap(T);
+            m = 1;
+        } else {
+            xor_shifted(C, B, m, bw);
+            m++;
+        }
+    }
+    if (L != kMtDeg) throw std::runtime_error("dither jump: unexpected linear complexity");
+    Words phi((size_t)kMtN + 1, 0);  // phi = x^L + c_1 x^(L-1) + ... + c_L
+    for (int i = 0; i <= L; i++)
+        if ((C[(size_t)i >> 6] >> (i & 63)) & 1) phi[(size_t)(L - i) >> 6] |= 1ULL << ((L - i) & 63);
+    return phi;
+}
+
+inline unsigned long long spread32(unsigned long long v) {  // bit j -> bit 2j
+    v &= 0xFFFFFFFFULL;
+    v = (v | (v << 16)) & 0x0000FFFF0000FFFFULL;
+    v = (v | (v << 8)) & 0x00FF00FF00FF00FFULL;
+    v = (v | (v << 4)) & 0x0F0F0F0F0F0F0F0FULL;
+    v = (v | (v << 2)) & 0x3333333333333333ULL;
+    v = (v | (v << 1)) & 0x5555555555555555ULL;
+    return v;
+}
+
+struct MtJumpTables {
+    std::vector<Words> phis;  // phi * x^s, s = 0..63
+    std::vector<Words> g;     // g[l] = x^(2^l kMtChunk) mod phi, kMtN words each
+    Words w312;               // x_312 .. x_623 of mt19937_64(12345)
+};
+
+Words sqr_mod(const Words& a, const std::vector<Words>& phis) {  // a^2 mod phi, deg a < kMtDeg
+    Words pr(2 * (size_t)kMtN + 2, 0);
+    for (int w = 0; w < kMtN; w++) {
+        pr[2 * (size_t)w] = spread32(a[(size_t)w]);
+        pr[2 * (size_t)w + 1] = spread32(a[(size_t)w] >> 32);
+    }
+    for (long long p = 2LL * (kMtDeg - 1); p >= kMtDeg; p--) {
+        if (!((pr[(size_t)p >> 6] >> (p & 63)) & 1)) continue;
+        const long long q = p - kMtDeg;  // pr ^= phi * x^q clears bit p
+        const Words& ph = phis[(size_t)(q & 63)];
+        const size_t w0 = (size_t)(q >> 6);
+        for (size_t i = 0; i < ph.size() && w0 + i < pr.size(); i++) pr[w0 + i] ^= ph[i];
+    }
+    pr.resize(kMtN);
+    return pr;
+}
+
+// word i of g(A) W_s from the sequence X = x_s .. x_{s + kMtSeq - 1}
+Words mt_apply_h(const Words& g, const Words& X) {
+    Words out(kMtN, 0);
+    for (int k = 0; k < kMtDeg; k++)
+        if ((g[(size_t)k >> 6] >> (k & 63)) & 1)
+            for (int i = 0; i < kMtN; i++) out[(size_t)i] ^= X[(size_t)(k + i)];
+    return out;
+}
+
+// The tables with at least `levels` jump polynomials, built once per process (and extended on demand). The first
+// polynomial is checked against the directly generated window 2^20 draws ahead.
+const MtJumpTables& mt_tables(int levels) {
+    static MtJumpTables t;
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lock(mu);
+    if (t.phis.empty()) {
+        const Words phi = mt_phi();
+        for (int s = 0; s < 64; s++) {
+            Words v((size_t)kMtN + 2, 0);
+            xor_shifted(v, phi, s, phi.size());
+            t.phis.push_back(std::move(v));
+        }
+        Words g(kMtN, 0);
+        g[0] = 2;  // x
+        for (long long e = 1; e < kMtChunk; e *= 2) g = sqr_mod(g, t.phis);
+        const Words x = mt_words(12345, (size_t)(kMtN + kMtChunk + kMtSeq));
+        t.w312.assign(x.begin() + kMtN, x.begin() + 2 * kMtN);
+        const Words want(x.begin() + kMtN + kMtChunk, x.begin() + 2 * kMtN + kMtChunk);
+        if (mt_apply_h(g, Words(x.begin() + kMtN, x.begin() + kMtN + kMtSeq)) != want)
+            throw std::runtime_error("dither jump: self-check failed");
+        t.g.push_back(std::move(g));
+    }
+    while ((int)t.g.size() < levels) t.g.push_back(sqr_mod(t.g.back(), t.phis));
+    return t;
+}
+
+// Enqueues D[0..n) (the dither of n samples) on `st`; tmp receives chunk windows and jump polynomials.
+int enqueue_dither(long long n, double* D, DevBuf& tmp, cudaStream_t st) {
+    if (n <= 0) return KBSRC_GPU_OK;
+    const long long G = (2 * n + kMtChunk - 1) / kMtChunk;
+    if (G > (1LL << 30)) return fail(KBSRC_GPU_E_ARG, "dither stream too long");
+    int levels = 0;
+    while ((1LL << levels) < G) levels++;
+    static bool smem_done[64] = {};
+    static std::mutex mu;
+    int dev = 0;
+    KB_CUDA(cudaGetDevice(&dev));
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        if (dev >= 64 || !smem_done[dev]) {
+            KB_CUDA(cudaFuncSetAttribute((const void*)k_mt_jump, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kMtJumpSmem));
+            if (dev < 64) smem_done[dev] = true;
+        }
+    }
+    const MtJumpTables& tb = mt_tables(std::max(levels, 1));
+    Words host((size_t)(G + levels) * kMtN, 0);  // W[0], then the level polynomials
+    std::copy(tb.w312.begin(), tb.w312.end(), host.begin());
+    for (int l = 0; l < levels; l++) std::copy(tb.g[(size_t)l].begin(), tb.g[(size_t)l].end(), host.begin() + (size_t)(G + l) * kMtN);
+    int rc;
+    if ((rc = tmp.alloc(host.size() * 8)) != KBSRC_GPU_OK) return rc;
+    unsigned long long* W = static_cast<unsigned long long*>(tmp.p);
+    KB_CUDA(cudaMemcpyAsync(W, host.data(), (size_t)kMtN * 8, cudaMemcpyHostToDevice, st));
+    if (levels)
+        KB_CUDA(cudaMemcpyAsync(W + (size_t)G * kMtN, host.data() + (size_t)G * kMtN, (size_t)levels * kMtN * 8,
+                                cudaMemcpyHostToDevice, st));
+    for (int l = 0; l < levels; l++) {
+        const long long half = 1LL << l;
+        k_mt_jump<<<(unsigned)std::min(half, G - half), kMtJumpThreads, kMtJumpSmem, st>>>(
+            W + (size_t)(G + l) * kMtN, W, (int)half, (int)G);
+    }
+    k_mt_chunks<<<(unsigned)G, 320, 0, st>>>(W, n, D);
+    KB_CUDA(cudaGetLastError());
+    return KBSRC_GPU_OK;  // copies from pageable memory have left `host` when cudaMemcpyAsync returns
+}
+
+// Jump polynomials that enqueue_dither(n, ...) needs, built on a host thread beside other work (0 if none)
+int dither_levels(long long n) {
+    const long long G = (2 * n + kMtChunk - 1) / kMtChunk;
+    int levels = 0;
+    while ((1LL << levels) < G && levels < 40) levels++;
+    return levels;
 }
 
 // Interleaved little-endian WAV data of planar samples y (ch x frames, row stride `stride`)
@@ -1963,6 +2227,93 @@ __global__ void k_place_taps(const double* __restrict__ taps, int L, int n, doub
 
 size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
 
+bool host_pinned(const void* p) {
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
+// memcpy split over up to 8 threads (pieces of at least 4 MB)
+void par_memcpy(void* dst, const void* src, size_t n) {
+    const int nt = (int)std::max<size_t>(1, std::min<size_t>(8, n >> 22));
+    if (nt == 1) {
+        std::memcpy(dst, src, n);
+        return;
+    }
+    std::vector<std::thread> th;
+    const size_t piece = (n + nt - 1) / nt;
+    for (int t = 0; t < nt; t++) {
+        const size_t off = (size_t)t * piece;
+        if (off >= n) break;
+        th.emplace_back([=] {
+            std::memcpy(static_cast<char*>(dst) + off, static_cast<const char*>(src) + off, std::min(piece, n - off));
+        });
+    }
+    for (auto& x : th) x.join();
+}
+
+int stager_ready(Stager& sg) {
+    for (int i = 0; i < 2; i++) {
+        if (!sg.pin[i]) KB_CUDA(cudaMallocHost(&sg.pin[i], Stager::kChunk));
+        if (!sg.ev[i]) KB_CUDA(cudaEventCreateWithFlags(&sg.ev[i], cudaEventDisableTiming));
+    }
+    return KBSRC_GPU_OK;
+}
+
+// Host -> device on `st`; returns once the last chunk is in flight (its bounce buffer is not reused before
+// its DMA completes).
+int copy_h2d(Stager& sg, void* dst, const void* src, size_t n, cudaStream_t st) {
+    if (!n) return KBSRC_GPU_OK;
+    if (host_pinned(src)) {
+        KB_CUDA(cudaMemcpyAsync(dst, src, n, cudaMemcpyHostToDevice, st));
+        return KBSRC_GPU_OK;
+    }
+    int rc;
+    if ((rc = stager_ready(sg)) != KBSRC_GPU_OK) return rc;
+    for (size_t off = 0, k = 0; off < n; off += Stager::kChunk, k++) {
+        const int b = (int)(k & 1);
+        const size_t m = std::min(Stager::kChunk, n - off);
+        KB_CUDA(cudaEventSynchronize(sg.ev[b]));
+        par_memcpy(sg.pin[b], static_cast<const char*>(src) + off, m);
+        KB_CUDA(cudaMemcpyAsync(static_cast<char*>(dst) + off, sg.pin[b], m, cudaMemcpyHostToDevice, st));
+        KB_CUDA(cudaEventRecord(sg.ev[b], st));
+    }
+    return KBSRC_GPU_OK;
+}
+
+// Device -> host after the work already on `st`; synchronous (returns with the data in dst).
+int copy_d2h(Stager& sg, void* dst, const void* src, size_t n, cudaStream_t st) {
+    if (!n) return KBSRC_GPU_OK;
+    if (host_pinned(dst)) {
+        KB_CUDA(cudaMemcpyAsync(dst, src, n, cudaMemcpyDeviceToHost, st));
+        KB_CUDA(cudaStreamSynchronize(st));
+        return KBSRC_GPU_OK;
+    }
+    int rc;
+    if ((rc = stager_ready(sg)) != KBSRC_GPU_OK) return rc;
+    const size_t chunks = (n + Stager::kChunk - 1) / Stager::kChunk;
+    auto issue = [&](size_t k) -> int {
+        const int b = (int)(k & 1);
+        const size_t off = k * Stager::kChunk, m = std::min(Stager::kChunk, n - off);
+        KB_CUDA(cudaEventSynchronize(sg.ev[b]));
+        KB_CUDA(cudaMemcpyAsync(sg.pin[b], static_cast<const char*>(src) + off, m, cudaMemcpyDeviceToHost, st));
+        KB_CUDA(cudaEventRecord(sg.ev[b], st));
+        return KBSRC_GPU_OK;
+    };
+    if ((rc = issue(0)) != KBSRC_GPU_OK) return rc;
+    for (size_t k = 0; k < chunks; k++) {
+        if (k + 1 < chunks && (rc = issue(k + 1)) != KBSRC_GPU_OK) return rc;
+        const int b = (int)(k & 1);
+        const size_t off = k * Stager::kChunk, m = std::min(Stager::kChunk, n - off);
+        KB_CUDA(cudaEventSynchronize(sg.ev[b]));
+        par_memcpy(static_cast<char*>(dst) + off, sg.pin[b], m);
+    }
+    return KBSRC_GPU_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -2150,6 +2501,7 @@ int kbsrc_gpu_engine_run_host(kbsrc_gpu_engine* e, const double* in, const doubl
         const long long nblk = d.nblk, ch = d.channels, hopQ = (long long)e->hop * d.Q, hopP = (long long)e->hop * d.P;
         const long long bps = in_bytes(d.in_format);
         const long long chunks = nout_chunks(e, nblk);
+        const bool out_pinned = host_pinned(out);  // pageable output: one staged copy at the end
         const Work w = single_work(*e, dinp, (const double*)e->d_head.p, (const double*)e->d_tail.p, dout);
         long long copied = 0;  // frames already sent
         Trail tr;
@@ -2158,9 +2510,10 @@ int kbsrc_gpu_engine_run_host(kbsrc_gpu_engine* e, const double* in, const doubl
             if (b0 == b1) continue;
             const long long f_hi = std::min(d.frames, std::max(0LL, (b1 - 1) * hopQ + e->Nb - d.lead));
             if (f_hi > copied) {
-                KB_CUDA(cudaMemcpyAsync(static_cast<char*>(e->d_in.p) + copied * ch * bps,
-                                        reinterpret_cast<const char*>(in) + copied * ch * bps,
-                                        (size_t)((f_hi - copied) * ch * bps), cudaMemcpyHostToDevice, hs));
+                if ((rc = copy_h2d(e->stager, static_cast<char*>(e->d_in.p) + copied * ch * bps,
+                                   reinterpret_cast<const char*>(in) + copied * ch * bps,
+                                   (size_t)((f_hi - copied) * ch * bps), hs)) != KBSRC_GPU_OK)
+                    return rc;
                 copied = f_hi;
             }
             KB_CUDA(cudaEventRecord(e->ev_in[k % 2], hs));
@@ -2172,19 +2525,21 @@ int kbsrc_gpu_engine_run_host(kbsrc_gpu_engine* e, const double* in, const doubl
             KB_CUDA(cudaStreamWaitEvent(ds, e->ev_done[k % 2], 0));
             const long long o0 = std::max(0LL, b0 * hopP - d.o), o1 = k == chunks - 1 ? d.nout
                                                                                     : std::min(d.nout, b1 * hopP - d.o);
-            if (o1 > o0)
+            if (o1 > o0 && out_pinned)
                 KB_CUDA(cudaMemcpy2DAsync(out + o0, (size_t)d.nout * 8, dout + o0, (size_t)d.nout * 8,
                                           (size_t)(o1 - o0) * 8, (size_t)ch, cudaMemcpyDeviceToHost, ds));
         }
-        if (copied < d.frames && nin)  // frames no block reads (none in a valid plan)
-            KB_CUDA(cudaMemcpyAsync(static_cast<char*>(e->d_in.p) + copied * ch * bps,
-                                    reinterpret_cast<const char*>(in) + copied * ch * bps,
-                                    (size_t)((d.frames - copied) * ch * bps), cudaMemcpyHostToDevice, hs));
+        if (copied < d.frames && nin &&  // frames no block reads (none in a valid plan)
+            (rc = copy_h2d(e->stager, static_cast<char*>(e->d_in.p) + copied * ch * bps,
+                           reinterpret_cast<const char*>(in) + copied * ch * bps,
+                           (size_t)((d.frames - copied) * ch * bps), hs)) != KBSRC_GPU_OK)
+            return rc;
         e->launches = tr.launches;
         KB_CUDA(cudaGetLastError());
         KB_CUDA(cudaStreamSynchronize(hs));
         KB_CUDA(cudaStreamSynchronize(cs));
         KB_CUDA(cudaStreamSynchronize(ds));
+        if (!out_pinned && (rc = copy_d2h(e->stager, out, dout, no * 8, cs)) != KBSRC_GPU_OK) return rc;
         return check_tc(*e);
     } catch (const std::exception& x) {
         return fail(KBSRC_GPU_E_CUDA, x.what());
@@ -2207,14 +2562,18 @@ int kbsrc_gpu_engine_run_host_packed(kbsrc_gpu_engine* e, const double* in, cons
         if (!e->d_head.p && (rc = e->d_head.alloc(ne * 8)) != KBSRC_GPU_OK) return rc;
         if (!e->d_tail.p && (rc = e->d_tail.alloc(ne * 8)) != KBSRC_GPU_OK) return rc;
         if (!e->d_out.p && (rc = e->d_out.alloc(no * 8)) != KBSRC_GPU_OK) return rc;
-        DevBuf bytes, dith, cnt;
+        DevBuf bytes, dith, cnt, mtbuf;
         if ((rc = bytes.alloc(nb)) != KBSRC_GPU_OK || (rc = cnt.alloc(8)) != KBSRC_GPU_OK) return rc;
         const bool use_dither = dither && format >= 2 && no > 0;
         if (use_dither && (rc = dith.alloc(no * 8)) != KBSRC_GPU_OK) return rc;
+        // the dither's jump tables (first use in the process) are built while the input is copied
+        const int levels = use_dither ? dither_levels((long long)no) : 0;
+        auto tables = std::async(std::launch::async, [levels] {
+            if (levels) mt_tables(levels);
+        });
         cudaStream_t st = e->stream;
         KB_CUDA(cudaMemsetAsync(cnt.p, 0, 8, st));
-        if (use_dither) k_dither<<<1, 320, 0, st>>>(12345ULL, (long long)no, static_cast<double*>(dith.p));
-        if (nin) KB_CUDA(cudaMemcpyAsync(e->d_in.p, in, nin * in_bytes(d.in_format), cudaMemcpyHostToDevice, st));
+        if ((rc = copy_h2d(e->stager, e->d_in.p, in, nin * in_bytes(d.in_format), st)) != KBSRC_GPU_OK) return rc;
         if (ne) {
             KB_CUDA(cudaMemcpyAsync(e->d_head.p, head, ne * 8, cudaMemcpyHostToDevice, st));
             KB_CUDA(cudaMemcpyAsync(e->d_tail.p, tail, ne * 8, cudaMemcpyHostToDevice, st));
@@ -2222,12 +2581,28 @@ int kbsrc_gpu_engine_run_host_packed(kbsrc_gpu_engine* e, const double* in, cons
         rc = run_device_impl(e, (const double*)e->d_in.p, (const double*)e->d_head.p, (const double*)e->d_tail.p,
                              (double*)e->d_out.p, st);
         if (rc) return rc;
+        tables.get();
+        cudaEvent_t dith_done = nullptr;
+        struct EventGuard {
+            cudaEvent_t& e;
+            ~EventGuard() {
+                if (e) cudaEventDestroy(e);
+            }
+        } guard_ev{dith_done};
+        if (use_dither) {  // the generator on its own stream, beside the conversion
+            if (!e->side) KB_CUDA(cudaStreamCreateWithFlags(&e->side, cudaStreamNonBlocking));
+            KB_CUDA(cudaEventCreateWithFlags(&dith_done, cudaEventDisableTiming));
+            if ((rc = enqueue_dither((long long)no, static_cast<double*>(dith.p), mtbuf, e->side)) != KBSRC_GPU_OK)
+                return rc;
+            KB_CUDA(cudaEventRecord(dith_done, e->side));
+            KB_CUDA(cudaStreamWaitEvent(st, dith_done, 0));
+        }
         if ((rc = enqueue_pack((const double*)e->d_out.p, d.channels, d.nout, d.nout, format,
                                use_dither ? (const double*)dith.p : nullptr, (unsigned char*)bytes.p,
                                (unsigned long long*)cnt.p, st)) != KBSRC_GPU_OK)
             return rc;
         unsigned long long c = 0;
-        if (nb) KB_CUDA(cudaMemcpyAsync(out_bytes, bytes.p, nb, cudaMemcpyDeviceToHost, st));
+        if ((rc = copy_d2h(e->stager, out_bytes, bytes.p, nb, st)) != KBSRC_GPU_OK) return rc;
         KB_CUDA(cudaMemcpyAsync(&c, cnt.p, 8, cudaMemcpyDeviceToHost, st));
         KB_CUDA(cudaStreamSynchronize(st));
         if (clipped) *clipped = (long long)c;
@@ -2246,12 +2621,12 @@ int kbsrc_gpu_pack(const double* d_planar, int channels, long long frames, long 
         const long long n = frames * channels;
         cudaStream_t st = static_cast<cudaStream_t>(stream);
         int rc;
-        DevBuf dith, cnt;
+        DevBuf dith, cnt, mtbuf;
         if ((rc = cnt.alloc(8)) != KBSRC_GPU_OK) return rc;
         const bool use_dither = dither && format >= 2 && n > 0;
         if (use_dither && (rc = dith.alloc((size_t)n * 8)) != KBSRC_GPU_OK) return rc;
         KB_CUDA(cudaMemsetAsync(cnt.p, 0, 8, st));
-        if (use_dither) k_dither<<<1, 320, 0, st>>>(12345ULL, n, static_cast<double*>(dith.p));
+        if (use_dither && (rc = enqueue_dither(n, static_cast<double*>(dith.p), mtbuf, st)) != KBSRC_GPU_OK) return rc;
         if ((rc = enqueue_pack(d_planar, channels, frames, stride, format,
                                use_dither ? (const double*)dith.p : nullptr, d_out, (unsigned long long*)cnt.p, st)) !=
             KBSRC_GPU_OK)

@@ -117,6 +117,40 @@ def test_gpu_pack_equals_reference_writer(tmp_path, fmt, dither):
 
 
 @pytest.mark.skipif(not os.path.exists(oracle.REF_CLI), reason="reference CLI not built (oracle/_ref)")
+@pytest.mark.parametrize("frames,ch", [(524288, 2), (524289, 1), (700001, 3)])
+def test_gpu_dither_across_chunks_equals_reference_writer(tmp_path, frames, ch):
+    """The dither stream is generated in chunks of 2^20 draws (2^19 samples) whose start states come from a
+    jump-ahead tree; samples on both sides of every chunk boundary match the reference's sequential generator.
+    The sizes end exactly on a boundary, one sample past it, and inside a fifth chunk."""
+    x = np.random.default_rng(frames).uniform(-0.99, 0.99, (frames, ch))
+    src = tmp_path / "in.wav"
+    from test_host import wav
+    src.write_bytes(wav(3, ch, 48000, 64, 8 * ch, x.astype("<f8").tobytes()))
+    ref = tmp_path / "ref.wav"
+    r = subprocess.run([oracle.REF_CLI, str(src), str(ref), "--rate", "48000", "--format", "s24", "--dither"],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    _, want = read_wav_samples(ref)
+    got, _ = kbsrc_b200.pack(x.T, "s24", True)
+    assert got == want
+
+
+@pytest.mark.skipif(not os.path.exists(oracle.REF_CLI), reason="reference CLI not built (oracle/_ref)")
+def test_cli_dither_across_chunks_equals_reference_cli(tmp_path):
+    """A conversion whose dithered output spans several generator chunks (2.65 M samples): the CLI's file equals
+    the reference CLI's byte for byte."""
+    x = np.random.default_rng(17).uniform(-0.9, 0.9, (48000 * 30, 2))
+    src = tmp_path / "in.wav"
+    src.write_bytes(refinputs.wav_f64(x.ravel().tolist(), ch=2, rate=48000))
+    a, b = tmp_path / "a.wav", tmp_path / "b.wav"
+    args = ["--rate", 44100, "--format", "s16", "--dither"]
+    ra = cli(*args, src, a)
+    rb = cli(*args, src, b, binary=oracle.REF_CLI)
+    assert ra.returncode == rb.returncode == 0, (ra.stderr, rb.stderr)
+    assert a.read_bytes() == b.read_bytes()
+
+
+@pytest.mark.skipif(not os.path.exists(oracle.REF_CLI), reason="reference CLI not built (oracle/_ref)")
 @pytest.mark.parametrize("tag,bits,width", [(1, 8, 1), (1, 16, 2), (1, 20, 3), (1, 24, 3), (1, 32, 4), (3, 32, 4),
                                             (3, 64, 8)])
 def test_cli_input_formats_equal_reference_cli(tmp_path, tag, bits, width):
