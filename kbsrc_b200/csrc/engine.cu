@@ -18,7 +18,9 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <future>
@@ -2321,9 +2323,19 @@ extern "C" {
 int kbsrc_gpu_init(void) {
     try {
         int rc;
+        const char* tr = std::getenv("KBSRC_TRACE");
+        const bool trace = tr && *tr && *tr != '0';
+        const auto t0 = std::chrono::steady_clock::now();
+        auto since = [&] { return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); };
         if ((rc = require_device()) != KBSRC_GPU_OK) return rc;
+        const double t_dev = since();
         KB_CUDA(cudaFree(nullptr));  // creates the context
-        return allow_large_smem();
+        const double t_ctx = since();
+        rc = allow_large_smem();
+        if (trace)
+            std::fprintf(stderr, "kbsrc trace: GPU start: device %.3fs  context %.3fs  kernel attributes %.3fs\n", t_dev,
+                         t_ctx - t_dev, since() - t_ctx);
+        return rc;
     } catch (const std::exception& x) {
         return fail(KBSRC_GPU_E_CUDA, x.what());
     }
