@@ -120,7 +120,7 @@ int run(int argc, char** argv) {
         nout = y.empty() ? 0 : (long long)y[0].size();
         kbsrc::io::write_wav(out_path.c_str(), y, a.ch, nout, rate, format, dither, clipped);
     } else {  // the input decode, the conversion and the output step (scale, dither, round, clip) on the GPU
-        const auto data = kbsrc::resample_wav_pcm(a.raw.data(), a.sample_format.c_str(), a.frames, a.ch, a.rate,
+        const auto data = kbsrc::resample_wav_pcm(a.bytes(), a.sample_format.c_str(), a.frames, a.ch, a.rate,
                                                   rate, format.c_str(), dither, clipped, opt, &st);
         t2 = now();
         const long long bps = format == "f64" ? 8 : format == "s24" ? 3 : format == "s16" ? 2 : 4;

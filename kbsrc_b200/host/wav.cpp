@@ -10,6 +10,9 @@
 #include <random>
 #include <stdexcept>
 
+#include <sys/mman.h>
+#include <unistd.h>
+
 namespace kbsrc::io {
 namespace {
 
@@ -120,6 +123,17 @@ Audio read_impl(const char* path, bool raw) {
     const size_t n = (size_t)a.frames * ch;
     fseeko(f, data_pos, SEEK_SET);
     if (raw) {
+        if (n) {
+            const long long page = sysconf(_SC_PAGESIZE), off = data_pos / page * page;
+            const size_t len = (size_t)(data_pos - off) + n * bps;
+            void* m = mmap(nullptr, len, PROT_READ, MAP_PRIVATE, fileno(f), (off_t)off);
+            if (m != MAP_FAILED) {
+                madvise(m, len, MADV_SEQUENTIAL);
+                a.map = std::shared_ptr<const void>(m, [len](const void* q) { munmap(const_cast<void*>(q), len); });
+                a.mapped = static_cast<const unsigned char*>(m) + (data_pos - off);
+                return a;
+            }
+        }
         a.raw.resize(n * bps);
         if (n && std::fread(a.raw.data(), (size_t)bps, n, f) != n) fail("read error");
         return a;
@@ -142,7 +156,7 @@ Audio read_wav_raw(const char* path) { return read_impl(path, true); }
 void decode_wav(Audio& a) {
     const size_t n = (size_t)a.frames * a.ch;
     a.d.resize(n);
-    if (n) decode_samples(a.raw.data(), n, a.fmt_float, a.fmt_bits, sample_bytes(a), a.d.data());
+    if (n) decode_samples(a.bytes(), n, a.fmt_float, a.fmt_bits, sample_bytes(a), a.d.data());
 }
 
 void check_wav_output(int ch, int rate, const std::string& fmt) {

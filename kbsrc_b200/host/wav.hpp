@@ -3,6 +3,7 @@
 // since the tool's output file is compared byte for byte.
 #pragma once
 
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -14,13 +15,18 @@ struct Audio {
     std::vector<double> d;  // interleaved, decoded (read_wav)
     int fmt_bits = 0;
     bool fmt_float = false;
-    std::vector<unsigned char> raw;  // the data section as stored (read_wav_raw), frames * ch samples
+    std::vector<unsigned char> raw;  // the data section as stored (read_wav_raw), frames * ch samples,
+    std::shared_ptr<const void> map;  // unless it is read in place from a mapping of the file
+    const unsigned char* mapped = nullptr;
     std::string sample_format;      // its sample format: "u8", "s16", "s24", "s32", "f32" or "f64"
+    const unsigned char* bytes() const { return map ? mapped : raw.data(); }
 };
 
 Audio read_wav(const char* path);
-// The same checks and header parsing as read_wav, but the samples stay as stored in the file (raw,
-// sample_format); decode_wav fills d from them.
+// The same checks and header parsing as read_wav, but the samples stay as stored in the file (bytes(),
+// sample_format); decode_wav fills d from them. The data section is mapped read-only where the file can be
+// mapped (the copies to the GPU then read the page cache directly), else read into raw. A file truncated by
+// another process while it is mapped ends the process with SIGBUS.
 Audio read_wav_raw(const char* path);
 void decode_wav(Audio& a);
 // Fails when a WAV header in `format` cannot describe ch channels at this rate.
