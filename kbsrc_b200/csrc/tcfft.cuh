@@ -23,7 +23,7 @@ namespace kbsrc::dev {
 constexpr int kTcSlices = 8;
 constexpr int kTcAcc = kTcSlices + 1;  // accumulators d = i + j = 0..8: the triangle plus its first diagonal
 constexpr int kTcRows = 128;          // MMA M: row vectors per stage
-constexpr int kTcThreads = 256;       // two threads per row while slicing; two warpgroups while recombining
+constexpr int kTcThreads = 512;       // four threads per row while slicing; four warpgroups while recombining
 constexpr int kTcWaitLimit = 1 << 22; // mbarrier polls before a stage reports a timeout
 
 // One radix of the split form: the sliced real DFT_R matrix (global memory, kTcSlices * 2nh * 2kh bytes).
@@ -46,7 +46,7 @@ struct TcSmem {
     unsigned char* bm_a;    // sliced DFT matrices
     unsigned char* bm_b;
     double2* tw;            // N inner twiddles
-    int* emax;              // row exponents (two per row while slicing)
+    int* emax;              // row exponents (four per row while slicing)
     uint64_t* mbar;
     uint32_t* tmem_slot;
 };
@@ -58,7 +58,7 @@ __host__ __device__ inline size_t tc_align(size_t v) { return (v + 127) & ~(size
 __host__ __device__ inline size_t tc_smem_bytes(const TcSub& s) {
     const int kpad = 2 * (s.a.kh > s.b.kh ? s.a.kh : s.b.kh);
     return tc_align((size_t)kTcSlices * kTcRows * kpad) + tc_align(tc_bm_bytes(s.a)) + tc_align(tc_bm_bytes(s.b)) +
-           tc_align((size_t)s.N * 16) + tc_align(2 * kTcRows * 4) + 128;
+           tc_align((size_t)s.N * 16) + tc_align(4 * kTcRows * 4) + 128;
 }
 
 __device__ inline TcSmem tc_carve(unsigned char* p, const TcSub& s) {
@@ -73,7 +73,7 @@ __device__ inline TcSmem tc_carve(unsigned char* p, const TcSub& s) {
     m.tw = reinterpret_cast<double2*>(p);
     p += tc_align((size_t)s.N * 16);
     m.emax = reinterpret_cast<int*>(p);
-    p += tc_align(2 * kTcRows * 4);
+    p += tc_align(4 * kTcRows * 4);
     m.mbar = reinterpret_cast<uint64_t*>(p);
     m.tmem_slot = reinterpret_cast<uint32_t*>(p + 8);
     return m;
@@ -130,45 +130,42 @@ __device__ inline void tc_stage(const TcRadix& rad, int nrows, const TcSmem& m, 
                                 uint32_t tmem, uint32_t& phase, int* err, Load load, Store store) {
     const int R = rad.R, kh = rad.kh, nh = rad.nh, kpad = 2 * kh, npad = 2 * nh;
     const int t = threadIdx.x;
-    {  // slicing: two threads per row, one per K half (real, imaginary parts); the row exponent through smem
-        const int row = t & (kTcRows - 1), part = t >> 7;
-        double vals[32];
+    {  // slicing: four threads per row, one per 16-column chunk of a K half (real, imaginary parts); the row
+       // exponent through smem
+        const int row = t & (kTcRows - 1), part = (t >> 7) & 1, c = 16 * (t >> 8);
+        double vals[16];
         int e = -1022;
 #pragma unroll
-        for (int j = 0; j < 32; j++) {
-            vals[j] = (row < nrows && j < R) ? load(row, j, part) : 0.0;
-            e = max(e, tc_expo(vals[j]));
+        for (int q = 0; q < 16; q++) {
+            vals[q] = (row < nrows && c + q < R) ? load(row, c + q, part) : 0.0;
+            e = max(e, tc_expo(vals[q]));
         }
-        m.emax[part * kTcRows + row] = e;
+        m.emax[(t >> 7) * kTcRows + row] = e;
         __syncthreads();
-        e = max(m.emax[row], m.emax[kTcRows + row]);
-        if (row < nrows) {
+        e = max(max(m.emax[row], m.emax[kTcRows + row]), max(m.emax[2 * kTcRows + row], m.emax[3 * kTcRows + row]));
+        if (row < nrows && c < kh) {
+            unsigned long long mag[16];
+            unsigned neg = 0;
 #pragma unroll
-            for (int c = 0; c < 32; c += 16) {
-                if (c >= kh) break;
-                unsigned long long mag[16];
-                unsigned neg = 0;
+            for (int q = 0; q < 16; q++) {
+                mag[q] = tc_mag(vals[q], e);
+                if (__double_as_longlong(vals[q]) < 0) neg |= 1u << q;
+            }
+#pragma unroll
+            for (int i = 0; i < kTcSlices; i++) {
+                uint32_t w[4] = {0, 0, 0, 0};
 #pragma unroll
                 for (int q = 0; q < 16; q++) {
-                    mag[q] = tc_mag(vals[c + q], e);
-                    if (__double_as_longlong(vals[c + q]) < 0) neg |= 1u << q;
+                    int sl = (int)((mag[q] >> (49 - 7 * i)) & 127);
+                    if ((neg >> q) & 1) sl = -sl;
+                    w[q >> 2] |= (uint32_t)(sl & 0xff) << (8 * (q & 3));
                 }
-#pragma unroll
-                for (int i = 0; i < kTcSlices; i++) {
-                    uint32_t w[4] = {0, 0, 0, 0};
-#pragma unroll
-                    for (int q = 0; q < 16; q++) {
-                        int sl = (int)((mag[q] >> (49 - 7 * i)) & 127);
-                        if ((neg >> q) & 1) sl = -sl;
-                        w[q >> 2] |= (uint32_t)(sl & 0xff) << (8 * (q & 3));
-                    }
-                    *reinterpret_cast<uint4*>(m.slices + i * kTcRows * kpad + umma_off(row, part * kh + c, kpad)) =
-                        make_uint4(w[0], w[1], w[2], w[3]);
-                }
+                *reinterpret_cast<uint4*>(m.slices + i * kTcRows * kpad + umma_off(row, part * kh + c, kpad)) =
+                    make_uint4(w[0], w[1], w[2], w[3]);
             }
         }
         __syncthreads();
-        if (part == 0) m.emax[row] = e;
+        if (t < kTcRows) m.emax[row] = e;
     }
     fence_async_smem();
     tc_fence_before();
@@ -198,13 +195,13 @@ __device__ inline void tc_stage(const TcRadix& rad, int nrows, const TcSmem& m, 
         tc_fence_after();
         if (!ok) {
             if ((t & 31) == 0) atomicExch(err, 1);
-        } else {  // recombination: warp w reads TMEM lanes 32 (w % 4) .., warpgroup w / 4 one half of the columns
-            const int warp = t >> 5, lane0 = 32 * (warp & 3), row = lane0 + (t & 31), half = nr / 2;
-            const int c_begin = (warp >> 2) * half;
+        } else {  // recombination: warp w reads TMEM lanes 32 (w % 4) ..; warpgroup w / 4 takes every fourth group
+                  // of 8 columns
+            const int warp = t >> 5, lane0 = 32 * (warp & 3), row = lane0 + (t & 31);
             const int e = row < nrows ? m.emax[row] : 0;
             const double s1 = tc_pow2(e - 34), s2 = tc_pow2(e - 69);
             const uint32_t lane_addr = tmem + ((uint32_t)lane0 << 16);
-            for (int c0 = c_begin; c0 < c_begin + half; c0 += 8) {
+            for (int c0 = 8 * (warp >> 2); c0 < nr; c0 += 32) {
                 long long hi[8], lo[8];
                 int32_t v[5][8];
 #pragma unroll
