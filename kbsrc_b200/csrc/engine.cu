@@ -938,7 +938,8 @@ int make_dev_cfft(int n, int tab, int fmax, DevCfft& d, cudaStream_t st) {
 
 // ------------------------------------------------------------------------------------------------------
 // split-precision plans: n = N1 * N2 (four-step, or N2 = 1 for one direct sub-FFT), each sub-FFT N = Ra * Rb
-// with radices <= 32, so that every stage is one tcgen05 contraction with K, N <= 64.
+// (or, where no such pair exists, Ra * Rb * Rc) with radices <= 32, so that every stage is one tcgen05
+// contraction with K, N <= 64.
 // ------------------------------------------------------------------------------------------------------
 // Ra * Rb = N with both <= 32, Ra the largest such divisor <= sqrt(N); false when there is none.
 bool tc_factor(int N, int& Ra, int& Rb) {
@@ -949,6 +950,25 @@ bool tc_factor(int N, int& Ra, int& Rb) {
     Ra = best;
     Rb = N / best;
     return true;
+}
+// Ra * Rb * Rc = N, each <= 32 and >= N / 128 (so that every stage has at most 128 rows), the smallest radix as
+// large as possible; false when there is none.
+bool tc_factor3(int N, int& Ra, int& Rb, int& Rc) {
+    const int lo = std::max(2, (N + kTcRows - 1) / kTcRows);
+    int best = 0;
+    for (int a = lo; a <= 32; a++) {
+        if (N % a) continue;
+        for (int b = a; b <= 32; b++) {
+            if ((N / a) % b) continue;
+            const int c = N / a / b;
+            if (c < b || c > 32 || a <= best) continue;
+            best = a;
+            Ra = a;
+            Rb = b;
+            Rc = c;
+        }
+    }
+    return best > 0;
 }
 int tc_kh(int R) { return R <= 16 ? 16 : 32; }
 int tc_nh(int R) { return R <= 16 ? 16 : R <= 24 ? 24 : 32; }
@@ -992,14 +1012,17 @@ struct TcFftDev {
 
 // Sub-FFT of N points over `count` sequences: radices, sequences per CTA within the shared-memory limit
 int tc_sub_plan(int N, int count, TcSub& sub, size_t& smem) {
-    int Ra, Rb;
-    if (!tc_factor(N, Ra, Rb)) return fail(KBSRC_GPU_E_UNSUPPORTED, "split-precision form: no radix-32 factorisation");
+    int Ra, Rb, Rc = 1;
+    if (!tc_factor(N, Ra, Rb) && !tc_factor3(N, Ra, Rb, Rc))
+        return fail(KBSRC_GPU_E_UNSUPPORTED, "split-precision form: no radix-32 factorisation");
     sub = TcSub{};
     sub.N = N;
     sub.a = TcRadix{Ra, tc_kh(Ra), tc_nh(Ra), nullptr};
     sub.b = TcRadix{Rb, tc_kh(Rb), tc_nh(Rb), nullptr};
+    if (Rc > 1) sub.c = TcRadix{Rc, tc_kh(Rc), tc_nh(Rc), nullptr};
     sub.ncols = 512;  // kTcAcc accumulators of up to 48 columns (or 32 per round): more than 256
-    int F = std::max(1, std::min(kTcRows / std::max(Ra, Rb), count));
+    const int rows1 = N / std::min({Ra, Rb, Rc > 1 ? Rc : Rb});  // rows of the largest stage for one sequence
+    int F = std::max(1, std::min(kTcRows / rows1, count));
     for (;; F--) {
         sub.F = F;
         smem = 2 * (size_t)N * F * 16 + tc_smem_bytes(sub);
@@ -1015,14 +1038,19 @@ int make_tc_fft(int n, TcFftDev& t) {
     KB_CUDA(cudaDeviceGetAttribute(&t.ctas, cudaDevAttrMultiProcessorCount, dev));
     t.n = n;
     t.N1 = t.N2 = 0;
-    if (n <= 1024 && tc_factor(n, a, b)) {
-        t.N1 = n;
-        t.N2 = 1;
-    } else {
+    int c;
+    // two radices per sub-FFT where possible, three where the length needs them
+    for (int three = 0; three < 2 && !t.N1; three++) {
+        auto ok = [&](int N) { return tc_factor(N, a, b) || (three && tc_factor3(N, a, b, c)); };
+        if (n <= 1024 && ok(n)) {
+            t.N1 = n;
+            t.N2 = 1;
+            break;
+        }
         for (int N1 = (int)std::sqrt((double)n) + 1; N1 >= 2; N1--) {
             if ((long long)N1 * N1 > n || n % N1) continue;
             const int N2 = n / N1;
-            if (N2 <= 1024 && tc_factor(N1, a, b) && tc_factor(N2, a, b)) {
+            if (N2 <= 1024 && ok(N1) && ok(N2)) {
                 t.N1 = N1;
                 t.N2 = N2;
                 break;
@@ -1034,29 +1062,38 @@ int make_tc_fft(int n, TcFftDev& t) {
                                                  " has no factorisation into radices <= 32");
     if ((rc = tc_sub_plan(t.N1, t.N2, t.col, t.smem_col)) != KBSRC_GPU_OK) return rc;
     if (t.N2 > 1 && (rc = tc_sub_plan(t.N2, t.N1, t.row, t.smem_row)) != KBSRC_GPU_OK) return rc;
-    // sliced matrices of the (up to four) radices, the inner twiddles of each sub-FFT, and the four-step twiddles
+    // sliced matrices of the (up to six) radices, the inner twiddles of each sub-FFT, and the four-step twiddles
     std::vector<unsigned char> mats;
-    size_t off[4];
-    TcRadix* rads[4] = {&t.col.a, &t.col.b, &t.row.a, &t.row.b};
-    const int nr = t.N2 > 1 ? 4 : 2;
+    size_t off[6];
+    TcRadix* rads[6] = {&t.col.a, &t.col.b, &t.col.c, &t.row.a, &t.row.b, &t.row.c};
+    const int nr = t.N2 > 1 ? 6 : 3;
     for (int i = 0; i < nr; i++) {
         off[i] = mats.size();
-        tc_matrix(rads[i]->R, mats);
+        if (rads[i]->R > 1) tc_matrix(rads[i]->R, mats);
     }
     if ((rc = t.mats.alloc(mats.size())) != KBSRC_GPU_OK) return rc;
     KB_CUDA(cudaMemcpy(t.mats.p, mats.data(), mats.size(), cudaMemcpyHostToDevice));
     for (int i = 0; i < nr; i++)
-        rads[i]->slices = reinterpret_cast<const uint4*>(static_cast<unsigned char*>(t.mats.p) + off[i]);
+        if (rads[i]->R > 1)
+            rads[i]->slices = reinterpret_cast<const uint4*>(static_cast<unsigned char*>(t.mats.p) + off[i]);
     std::vector<double> tw;
-    auto inner = [&](const TcSub& sub) {  // [k1 * Rb + m] = e^{-2 pi i m k1 / N}
-        hd::RootTable rt(sub.N);
-        for (int k1 = 0; k1 < sub.a.R; k1++)
-            for (int m = 0; m < sub.b.R; m++) {
+    auto roots = [&](int N, int A, int B) {  // [k1 * B + m] = e^{-2 pi i m k1 / N}, k1 < A, m < B
+        hd::RootTable rt(N);
+        for (int k1 = 0; k1 < A; k1++)
+            for (int m = 0; m < B; m++) {
                 hd::dd c, sn;
                 rt.get(-(long long)m * k1, c, sn);
                 tw.push_back(c.hi);
                 tw.push_back(sn.hi);
             }
+    };
+    auto inner = [&](const TcSub& sub) {
+        if (sub.c.R > 1) {
+            roots(sub.N, sub.a.R, sub.b.R * sub.c.R);
+            roots(sub.b.R * sub.c.R, sub.b.R, sub.c.R);
+        } else {
+            roots(sub.N, sub.a.R, sub.b.R);
+        }
     };
     inner(t.col);
     const size_t row_off = tw.size();

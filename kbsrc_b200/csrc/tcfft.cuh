@@ -32,46 +32,53 @@ struct TcRadix {
     const uint4* slices;
 };
 
-// A sub-FFT of N = a.R * b.R points on F sequences per CTA (F * max(a.R, b.R) <= 128); tw[k1 * b.R + m] =
-// e^{-2 pi i m k1 / N}; ncols: TMEM columns to allocate.
+// A sub-FFT of N = a.R * b.R * c.R points (c.R == 1: two radices) on F sequences per CTA, every stage at most 128
+// rows (F * N / R <= 128 for each radix R); ncols: TMEM columns to allocate. Inner twiddles, M = b.R * c.R:
+// tw[k1 * M + m] = e^{-2 pi i m k1 / N}, then (three radices) tw[N + c1 * c.R + v] = e^{-2 pi i v c1 / M}.
 struct TcSub {
     int N, F, ncols;
-    TcRadix a, b;
+    TcRadix a, b, c;
     const double2* tw;
 };
+__host__ __device__ inline int tc_tw_count(const TcSub& s) { return s.c.R > 1 ? s.N + s.b.R * s.c.R : s.N; }
 
 // Per-CTA shared memory of the split form after the two data plane pairs.
 struct TcSmem {
     unsigned char* slices;  // kTcSlices * 128 * kpad_max
     unsigned char* bm_a;    // sliced DFT matrices
     unsigned char* bm_b;
-    double2* tw;            // N inner twiddles
+    unsigned char* bm_c;
+    double2* tw;            // tc_tw_count inner twiddles
     int* emax;              // row exponents (four per row while slicing)
     uint64_t* mbar;
     uint32_t* tmem_slot;
 };
 
-__host__ __device__ inline int tc_bm_bytes(const TcRadix& r) { return kTcSlices * (2 * r.nh) * (2 * r.kh); }
+__host__ __device__ inline int tc_bm_bytes(const TcRadix& r) { return r.R > 1 ? kTcSlices * (2 * r.nh) * (2 * r.kh) : 0; }
+__host__ __device__ inline int tc_kpad(const TcSub& s) {
+    const int k = s.a.kh > s.b.kh ? s.a.kh : s.b.kh;
+    return 2 * (s.c.R > 1 && s.c.kh > k ? s.c.kh : k);
+}
 __host__ __device__ inline size_t tc_align(size_t v) { return (v + 127) & ~(size_t)127; }
 
 // Shared bytes the split-form part of a CTA needs after its data planes.
 __host__ __device__ inline size_t tc_smem_bytes(const TcSub& s) {
-    const int kpad = 2 * (s.a.kh > s.b.kh ? s.a.kh : s.b.kh);
-    return tc_align((size_t)kTcSlices * kTcRows * kpad) + tc_align(tc_bm_bytes(s.a)) + tc_align(tc_bm_bytes(s.b)) +
-           tc_align((size_t)s.N * 16) + tc_align(4 * kTcRows * 4) + 128;
+    return tc_align((size_t)kTcSlices * kTcRows * tc_kpad(s)) + tc_align(tc_bm_bytes(s.a)) + tc_align(tc_bm_bytes(s.b)) +
+           tc_align(tc_bm_bytes(s.c)) + tc_align((size_t)tc_tw_count(s) * 16) + tc_align(4 * kTcRows * 4) + 128;
 }
 
 __device__ inline TcSmem tc_carve(unsigned char* p, const TcSub& s) {
     TcSmem m;
-    const int kpad = 2 * (s.a.kh > s.b.kh ? s.a.kh : s.b.kh);
     m.slices = p;
-    p += tc_align((size_t)kTcSlices * kTcRows * kpad);
+    p += tc_align((size_t)kTcSlices * kTcRows * tc_kpad(s));
     m.bm_a = p;
     p += tc_align(tc_bm_bytes(s.a));
     m.bm_b = p;
     p += tc_align(tc_bm_bytes(s.b));
+    m.bm_c = p;
+    p += tc_align(tc_bm_bytes(s.c));
     m.tw = reinterpret_cast<double2*>(p);
-    p += tc_align((size_t)s.N * 16);
+    p += tc_align((size_t)tc_tw_count(s) * 16);
     m.emax = reinterpret_cast<int*>(p);
     p += tc_align(4 * kTcRows * 4);
     m.mbar = reinterpret_cast<uint64_t*>(p);
@@ -84,12 +91,14 @@ __device__ inline TcSmem tc_carve(unsigned char* p, const TcSub& s) {
 __device__ inline uint32_t tc_setup(const TcSmem& m, const TcSub& s) {
     if (threadIdx.x < 32) tmem_alloc(m.tmem_slot, (uint32_t)s.ncols);
     if (threadIdx.x == 0) mbar_init(m.mbar, 1);
-    const int na = tc_bm_bytes(s.a) / 16, nb = tc_bm_bytes(s.b) / 16;
+    const int na = tc_bm_bytes(s.a) / 16, nb = tc_bm_bytes(s.b) / 16, nc = tc_bm_bytes(s.c) / 16, nt = tc_tw_count(s);
 #pragma unroll 4
     for (int i = threadIdx.x; i < na; i += blockDim.x) reinterpret_cast<uint4*>(m.bm_a)[i] = __ldg(s.a.slices + i);
 #pragma unroll 4
     for (int i = threadIdx.x; i < nb; i += blockDim.x) reinterpret_cast<uint4*>(m.bm_b)[i] = __ldg(s.b.slices + i);
-    for (int i = threadIdx.x; i < s.N; i += blockDim.x) m.tw[i] = __ldg(s.tw + i);
+#pragma unroll 4
+    for (int i = threadIdx.x; i < nc; i += blockDim.x) reinterpret_cast<uint4*>(m.bm_c)[i] = __ldg(s.c.slices + i);
+    for (int i = threadIdx.x; i < nt; i += blockDim.x) m.tw[i] = __ldg(s.tw + i);
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
@@ -237,8 +246,15 @@ __device__ inline void tc_stage(const TcRadix& rad, int nrows, const TcSmem& m, 
 // with n = Rb j + m, k = k1 + Ra k2: stage A (DFT_Ra over j for each m), the twiddle w_N^{m k1}, stage B (DFT_Rb
 // over m for each k1). Y is scratch; the result is in X in natural order. `phase`: mbarrier phases completed so
 // far by this CTA.
+__device__ inline void tc_subfft3(const TcSub& s, const Planes<ArF64>& X, const Planes<ArF64>& Y, const TcSmem& m,
+                                  uint32_t tmem, uint32_t& phase, int* err);
+
 __device__ inline void tc_subfft(const TcSub& s, const Planes<ArF64>& X, const Planes<ArF64>& Y, const TcSmem& m,
                                  uint32_t tmem, uint32_t& phase, int* err) {
+    if (s.c.R > 1) {
+        tc_subfft3(s, X, Y, m, tmem, phase, err);
+        return;
+    }
     const int F = s.F, Ra = s.a.R, Rb = s.b.R;
     tc_stage(s.a, Rb * F, m, m.bm_a, tmem, phase, err,
              [&](int r, int j, int part) {
@@ -263,6 +279,55 @@ __device__ inline void tc_subfft(const TcSub& s, const Planes<ArF64>& X, const P
              },
              [&](int r, int k2, int part, double y) {
                  const int k1 = r / F, f = r - k1 * F, i = (k1 + Ra * k2) * F + f;
+                 (part ? X.im : X.re)[i] = y;
+             });
+}
+
+// In-place complex multiply of the N*F values of P by tw[(e / F) % period] (e the plane index)
+__device__ inline void tc_twiddle(const Planes<ArF64>& P, const double2* tw, int n, int F, int period) {
+    for (int e = threadIdx.x; e < n * F; e += blockDim.x) {
+        const double2 w = tw[(e / F) % period];
+        const double re = P.re[e], im = P.im[e];
+        P.re[e] = __dsub_rn(__dmul_rn(re, w.x), __dmul_rn(im, w.y));
+        P.im[e] = __dadd_rn(__dmul_rn(re, w.y), __dmul_rn(im, w.x));
+    }
+    __syncthreads();
+}
+
+// Sub-FFT of N = Ra * M points, M = Rb * Rc: n = M j + m, k = k1 + Ra k2, then within each k1 the M-point
+// transform over m = Rc u + v, k2 = c1 + Rb c2. Stage A (DFT_Ra over j for each m, X -> Y), twiddle w_N^{m k1},
+// stage B (DFT_Rb over u for each (k1, v), Y -> X in the same slots), twiddle w_M^{v c1}, stage C (DFT_Rc over v
+// for each (k1, c1), X -> X in natural order: every value of a stage is read before any is written).
+__device__ inline void tc_subfft3(const TcSub& s, const Planes<ArF64>& X, const Planes<ArF64>& Y, const TcSmem& m,
+                                  uint32_t tmem, uint32_t& phase, int* err) {
+    const int F = s.F, Ra = s.a.R, Rb = s.b.R, Rc = s.c.R, M = Rb * Rc;
+    tc_stage(s.a, M * F, m, m.bm_a, tmem, phase, err,
+             [&](int r, int j, int part) {
+                 const int mm = r / F, f = r - mm * F, i = (M * j + mm) * F + f;
+                 return part ? X.im[i] : X.re[i];
+             },
+             [&](int r, int k1, int part, double y) {
+                 const int mm = r / F, f = r - mm * F, i = (k1 * M + mm) * F + f;
+                 (part ? Y.im : Y.re)[i] = y;
+             });
+    tc_twiddle(Y, m.tw, s.N, F, s.N);
+    tc_stage(s.b, Ra * Rc * F, m, m.bm_b, tmem, phase, err,
+             [&](int r, int u, int part) {
+                 const int q = r / F, f = r - q * F, k1 = q / Rc, v = q - k1 * Rc, i = (k1 * M + Rc * u + v) * F + f;
+                 return part ? Y.im[i] : Y.re[i];
+             },
+             [&](int r, int c1, int part, double y) {
+                 const int q = r / F, f = r - q * F, k1 = q / Rc, v = q - k1 * Rc, i = (k1 * M + Rc * c1 + v) * F + f;
+                 (part ? X.im : X.re)[i] = y;
+             });
+    tc_twiddle(X, m.tw + s.N, s.N, F, M);
+    tc_stage(s.c, Ra * Rb * F, m, m.bm_c, tmem, phase, err,
+             [&](int r, int v, int part) {
+                 const int q = r / F, f = r - q * F, k1 = q / Rb, c1 = q - k1 * Rb, i = (k1 * M + Rc * c1 + v) * F + f;
+                 return part ? X.im[i] : X.re[i];
+             },
+             [&](int r, int c2, int part, double y) {
+                 const int q = r / F, f = r - q * F, k1 = q / Rb, c1 = q - k1 * Rb, i = (k1 + Ra * (c1 + Rb * c2)) * F + f;
                  (part ? X.im : X.re)[i] = y;
              });
 }

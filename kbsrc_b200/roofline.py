@@ -154,15 +154,39 @@ def tc_factor(N):
     return (best, N // best) if best else None
 
 
+def tc_factor3(N):
+    """(Ra, Rb, Rc) with Ra * Rb * Rc = N, each <= 32 and >= N / 128, the smallest radix as large as possible; None
+    if there is none."""
+    lo = max(2, -(-N // TC_ROWS))
+    best = None
+    for a in range(lo, 33):
+        if N % a:
+            continue
+        for b in range(a, 33):
+            if (N // a) % b:
+                continue
+            c = N // a // b
+            if b <= c <= 32 and (best is None or a > best[0]):
+                best = (a, b, c)
+    return best
+
+
+def tc_radices(N):
+    """The radices of a split-form sub-FFT of N points: two where possible, else three."""
+    return tc_factor(N) or tc_factor3(N)
+
+
 def tc_split(n):
-    """(N1, N2): one direct sub-FFT (N2 = 1) up to 1024 points, else the four-step split nearest sqrt(n)."""
-    if n <= 1024 and tc_factor(n):
-        return n, 1
-    N1 = int(math.isqrt(n)) + 1
-    while N1 >= 2:
-        if N1 * N1 <= n and n % N1 == 0 and n // N1 <= 1024 and tc_factor(N1) and tc_factor(n // N1):
-            return N1, n // N1
-        N1 -= 1
+    """(N1, N2): one direct sub-FFT (N2 = 1) up to 1024 points, else the four-step split nearest sqrt(n); sub-FFTs
+    of two radices where any split allows them, else of three."""
+    for ok in (tc_factor, tc_radices):
+        if n <= 1024 and ok(n):
+            return n, 1
+        N1 = int(math.isqrt(n)) + 1
+        while N1 >= 2:
+            if N1 * N1 <= n and n % N1 == 0 and n // N1 <= 1024 and ok(N1) and ok(n // N1):
+                return N1, n // N1
+            N1 -= 1
     return None
 
 
@@ -176,21 +200,22 @@ def _tc_stage_ops(R):
 
 
 def _tc_sub_ops(N, count):
-    Ra, Rb = tc_factor(N)
-    F = max(1, min(TC_ROWS // max(Ra, Rb), count))
-    while F > 1 and 2 * N * F * 16 + _tc_smem(Ra, Rb, N) > 227 * 1024:
+    rads = tc_radices(N)
+    F = max(1, min(TC_ROWS // (N // min(rads)), count))
+    while F > 1 and 2 * N * F * 16 + _tc_smem(rads, N) > 227 * 1024:
         F -= 1
     items = -(-count // F)
-    return items * (_tc_stage_ops(Ra) + _tc_stage_ops(Rb))
+    return items * sum(_tc_stage_ops(R) for R in rads)
 
 
-def _tc_smem(Ra, Rb, N):
+def _tc_smem(rads, N):
     al = lambda v: (v + 127) // 128 * 128
     kh = lambda R: 16 if R <= 16 else 32
     nh = lambda R: 16 if R <= 16 else 24 if R <= 24 else 32
-    kpad = 2 * max(kh(Ra), kh(Rb))
+    kpad = 2 * max(kh(R) for R in rads)
     bm = lambda R: TC_SLICES * 2 * nh(R) * 2 * kh(R)
-    return al(TC_SLICES * TC_ROWS * kpad) + al(bm(Ra)) + al(bm(Rb)) + al(N * 16) + al(2 * TC_ROWS * 4) + 128
+    ntw = N + (rads[1] * rads[2] if len(rads) == 3 else 0)
+    return al(TC_SLICES * TC_ROWS * kpad) + sum(al(bm(R)) for R in rads) + al(ntw * 16) + al(4 * TC_ROWS * 4) + 128
 
 
 def split_work(plan, channels):

@@ -43,6 +43,15 @@ def test_split_full_size_c2():
     assert es <= ef
 
 
+def test_split_three_radix_sub_fft():
+    """192 kHz -> 44.1 kHz with --len 1.0 --beta 60 and block 3024 (the large multichannel plan): the forward
+    transform 967,680 = 960 x 1008 has no sub-FFTs of two radices <= 32, so 1008 runs as 8 x 9 x 14."""
+    x = np.random.default_rng(5).uniform(-0.5, 0.5, (192000 * 3, 1))
+    es, ef, peak = errors(x, 192000, 44100, length=1.0, beta=60.0, block=3024)
+    print(f"split {es:.3e} fast {ef:.3e} peak {peak:.3e}")
+    assert es <= ef
+
+
 def test_split_runs_twice_the_same():
     x = np.random.default_rng(3).uniform(-0.5, 0.5, (30000, 2))
     cv = kbsrc_b200.Conversion(x, 96000, 44100, mode="split")
