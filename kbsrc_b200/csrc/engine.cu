@@ -977,15 +977,16 @@ int tc_nh(int R) { return R <= 16 ? 16 : R <= 24 ? 24 : 32; }
 // imaginary parts from kh), y_re[k1] = sum_j xr_j cos + xi_j sin, y_im[k1] = sum_j xi_j cos - xr_j sin with the
 // angle 2 pi j k1 / R, each entry halved and cut into kTcSlices signed 7-bit slices of floor(|w| 2^55).
 void tc_matrix(int R, std::vector<unsigned char>& out) {
-    const int kh = tc_kh(R), nh = tc_nh(R), kpad = 2 * kh, npad = 2 * nh;
+    const int kh = tc_kh(R), nh = tc_nh(R), kpad = 2 * kh, npad = 2 * nh, nr = npad / tc_rounds(nh);
     const size_t base = out.size();
-    out.resize(base + (size_t)kTcSlices * npad * kpad, 0);
+    out.resize(base + (size_t)kTcMats * npad * kpad, 0);  // slice kTcMats - 1 stays zero
     auto put = [&](int n, int k, double w) {
         const unsigned long long v = (unsigned long long)(std::fabs(w) * 36028797018963968.0);  // |w| 2^55, exact
+        const int rd = n / nr, nn = n - rd * nr;  // [round][slice][nr rows]
         for (int i = 0; i < kTcSlices; i++) {
             int sl = (int)((v >> (49 - 7 * i)) & 127);
             if (w < 0) sl = -sl;
-            out[base + (size_t)i * npad * kpad + umma_off(n, k, kpad)] = (unsigned char)(signed char)sl;
+            out[base + ((size_t)rd * kTcMats + i) * nr * kpad + umma_off(nn, k, kpad)] = (unsigned char)(signed char)sl;
         }
     };
     hd::RootTable rt(R);

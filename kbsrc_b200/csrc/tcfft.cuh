@@ -22,11 +22,14 @@ namespace kbsrc::dev {
 
 constexpr int kTcSlices = 8;
 constexpr int kTcAcc = kTcSlices + 1;  // accumulators d = i + j = 0..8: the triangle plus its first diagonal
+constexpr int kTcMats = kTcSlices + 1; // matrix slices, the last one zero (it initialises accumulator 8)
 constexpr int kTcRows = 128;          // MMA M: row vectors per stage
 constexpr int kTcThreads = 512;       // four threads per row while slicing; four warpgroups while recombining
 constexpr int kTcWaitLimit = 1 << 22; // mbarrier polls before a stage reports a timeout
 
-// One radix of the split form: the sliced real DFT_R matrix (global memory, kTcSlices * 2nh * 2kh bytes).
+// One radix of the split form: the sliced real DFT_R matrix (global memory, kTcMats * 2nh * 2kh bytes), stored per
+// round (the output columns a round covers) with its slices one after the other, so that consecutive slices form
+// one operand of kTcMats times the round's columns.
 struct TcRadix {
     int R, kh, nh;
     const uint4* slices;
@@ -54,7 +57,10 @@ struct TcSmem {
     uint32_t* tmem_slot;
 };
 
-__host__ __device__ inline int tc_bm_bytes(const TcRadix& r) { return r.R > 1 ? kTcSlices * (2 * r.nh) * (2 * r.kh) : 0; }
+__host__ __device__ inline int tc_bm_bytes(const TcRadix& r) { return r.R > 1 ? kTcMats * (2 * r.nh) * (2 * r.kh) : 0; }
+// Rounds of a stage: accumulators of all 2nh output columns at once when they fit TMEM's 512 columns, else the
+// real and the imaginary outputs in turn.
+__host__ __device__ inline int tc_rounds(int nh) { return kTcAcc * 2 * nh <= 512 ? 1 : 2; }
 __host__ __device__ inline int tc_kpad(const TcSub& s) {
     const int k = s.a.kh > s.b.kh ? s.a.kh : s.b.kh;
     return 2 * (s.c.R > 1 && s.c.kh > k ? s.c.kh : k);
@@ -180,22 +186,24 @@ __device__ inline void tc_stage(const TcRadix& rad, int nrows, const TcSmem& m, 
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
-    // Accumulators d = 0..kTcAcc-1 of nr columns each; when they do not fit TMEM at once the real and the
-    // imaginary outputs go in two rounds.
-    const int rounds = kTcAcc * npad <= 512 ? 1 : 2, nr = npad / rounds;
+    // Accumulators d = 0..kTcAcc-1 of nr columns each (tc_rounds).
+    const int rounds = tc_rounds(nh), nr = npad / rounds;
     const uint32_t sbo = 8 * kpad;
     for (int rd = 0; rd < rounds; rd++) {
-        if (t == 0) {  // the product triangle i + j <= kTcAcc - 1, accumulator d collecting every i + j = d
-            const uint32_t idesc = umma_idesc_s8(kTcRows, nr), sa = smem_u32(m.slices),
-                           sb = smem_u32(bmat) + rd * nr * kpad;
-            for (int d = 0; d < kTcAcc; d++) {
-                const int i0 = d < kTcSlices ? 0 : d - kTcSlices + 1, i1 = d < kTcSlices ? d : kTcSlices - 1;
-                for (int i = i0; i <= i1; i++)
+        if (t == 0) {  // the product triangle i + j <= kTcAcc - 1, accumulator d collecting every i + j = d: data
+                       // slice i times matrix slices 0.. side by side lands on accumulators i.., up to 256 columns
+                       // per MMA; i = 0 (with the zero slice) initialises every accumulator
+            const uint32_t sa = smem_u32(m.slices), sb = smem_u32(bmat) + rd * kTcMats * nr * kpad;
+            const int bpc = 256 / nr;
+            for (int i = 0; i < kTcSlices; i++)
+                for (int d0 = i; d0 < kTcAcc; d0 += bpc) {
+                    const int nb = min(bpc, kTcAcc - d0);
+                    const uint32_t idesc = umma_idesc_s8(kTcRows, nb * nr);
                     for (int ks = 0; ks < kpad / 32; ks++)
-                        umma_s8(tmem + d * nr, umma_desc(sa + i * kTcRows * kpad + 256 * ks, 128, sbo),
-                                umma_desc(sb + (d - i) * npad * kpad + 256 * ks, 128, sbo), idesc,
-                                (i > i0 || ks) ? 1u : 0u);
-            }
+                        umma_s8(tmem + d0 * nr, umma_desc(sa + i * kTcRows * kpad + 256 * ks, 128, sbo),
+                                umma_desc(sb + (d0 - i) * nr * kpad + 256 * ks, 128, sbo), idesc,
+                                (i || ks) ? 1u : 0u);
+                }
             umma_commit(m.mbar);
         }
         bool ok = mbar_wait(m.mbar, phase & 1u, kTcWaitLimit);

@@ -141,6 +141,8 @@ def pass_bytes(plan, exact):
 # ---------------------------------------------------------------------------------------------------------------
 TC_SLICES, TC_ACC, TC_ROWS = 8, 9, 128
 TC_PRODUCTS = sum(min(d, TC_SLICES - 1) - max(0, d - TC_SLICES + 1) + 1 for d in range(TC_ACC))  # 43
+# issued accumulator blocks: data slice i against matrix slices 0..8-i (the ninth one zero) in wide MMAs
+TC_ISSUED = sum(TC_ACC - i for i in range(TC_SLICES))  # 44
 
 
 def tc_factor(N):
@@ -196,7 +198,7 @@ def _tc_stage_ops(R):
     kpad, npad = 2 * kh, 2 * nh
     rounds = 1 if TC_ACC * npad <= 512 else 2
     nr = npad // rounds
-    return TC_PRODUCTS * (kpad // 32) * rounds * 2 * TC_ROWS * nr * 32  # issued int8 ops (M x N x K x 2)
+    return TC_ISSUED * (kpad // 32) * rounds * 2 * TC_ROWS * nr * 32  # issued int8 ops (M x N x K x 2)
 
 
 def _tc_sub_ops(N, count):
@@ -213,7 +215,7 @@ def _tc_smem(rads, N):
     kh = lambda R: 16 if R <= 16 else 32
     nh = lambda R: 16 if R <= 16 else 24 if R <= 24 else 32
     kpad = 2 * max(kh(R) for R in rads)
-    bm = lambda R: TC_SLICES * 2 * nh(R) * 2 * kh(R)
+    bm = lambda R: (TC_SLICES + 1) * 2 * nh(R) * 2 * kh(R)
     ntw = N + (rads[1] * rads[2] if len(rads) == 3 else 0)
     return al(TC_SLICES * TC_ROWS * kpad) + sum(al(bm(R)) for R in rads) + al(ntw * 16) + al(4 * TC_ROWS * 4) + 128
 
