@@ -166,14 +166,26 @@ __device__ inline void tc_stage(const TcRadix& rad, int nrows, const TcSmem& m, 
                 mag[q] = tc_mag(vals[q], e);
                 if (__double_as_longlong(vals[q]) < 0) neg |= 1u << q;
             }
+            uint32_t nm[4];  // byte k of nm[g]: 0xff where value 4g + k is negative
+#pragma unroll
+            for (int g = 0; g < 4; g++)
+                nm[g] = ((neg >> (4 * g)) & 1 ? 0xffu : 0u) | ((neg >> (4 * g + 1)) & 1 ? 0xff00u : 0u) |
+                        ((neg >> (4 * g + 2)) & 1 ? 0xff0000u : 0u) | ((neg >> (4 * g + 3)) & 1 ? 0xff000000u : 0u);
 #pragma unroll
             for (int i = 0; i < kTcSlices; i++) {
-                uint32_t w[4] = {0, 0, 0, 0};
+                uint32_t w[4];
 #pragma unroll
-                for (int q = 0; q < 16; q++) {
-                    int sl = (int)((mag[q] >> (49 - 7 * i)) & 127);
-                    if ((neg >> q) & 1) sl = -sl;
-                    w[q >> 2] |= (uint32_t)(sl & 0xff) << (8 * (q & 3));
+                for (int g = 0; g < 4; g++) {
+                    uint32_t v = 0;  // 7-bit field i of value 4g + k, placed in byte k by one constant shift
+#pragma unroll
+                    for (int k = 0; k < 4; k++) {
+                        const int sh = 49 - 7 * i - 8 * k;
+                        const unsigned long long x = sh >= 0 ? mag[4 * g + k] >> sh : mag[4 * g + k] << -sh;
+                        v |= (uint32_t)x & (0x7fu << (8 * k));
+                    }
+                    // the negative values' bytes negated, four at once: -b = (0x80 - b) ^ 0x80 for b in [0, 127]
+                    const uint32_t nv = (0x80808080u - v) ^ 0x80808080u;
+                    w[g] = v ^ ((v ^ nv) & nm[g]);
                 }
                 *reinterpret_cast<uint4*>(m.slices + i * kTcRows * kpad + umma_off(row, part * kh + c, kpad)) =
                     make_uint4(w[0], w[1], w[2], w[3]);
