@@ -589,19 +589,27 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         tc_subfft(T.sub, A, B, m, tmem, phase, T.err);
         const TaskRef tr = DST == kDstOutput ? task_ref(P.work, task) : TaskRef{0, 0, 0};
         const Item it = DST == kDstOutput ? item_of(P.work, tr) : Item{};
-        for (int e = threadIdx.x; e < total; e += blockDim.x) {
-            const int k1 = e / F, n2 = c0 + (e - k1 * F);
-            if (n2 >= N2) continue;
-            C v = A.ld(e);
-            if (DST == kDstComplex) {
-                if (T.tw4) {
-                    const double2 w = __ldg(T.tw4 + (long long)k1 * N2 + n2);
-                    v = c_mulw<ArF64>(v, CxW<ArF64>{w.x, w.y});
+        // four-step twiddle and store; the table loads of a batch are issued before any of its products
+        for (int e0 = threadIdx.x; e0 < total; e0 += kLoadBatch * blockDim.x) {
+            double2 w[kLoadBatch];
+#pragma unroll
+            for (int j = 0; j < kLoadBatch; j++) {
+                const int e = e0 + j * blockDim.x, k1 = e / F, n2 = c0 + (e - k1 * F);
+                w[j] = make_double2(1.0, 0.0);
+                if (DST == kDstComplex && T.tw4 && e < total && n2 < N2) w[j] = __ldg(T.tw4 + (long long)k1 * N2 + n2);
+            }
+#pragma unroll
+            for (int j = 0; j < kLoadBatch; j++) {
+                const int e = e0 + j * blockDim.x, k1 = e / F, n2 = c0 + (e - k1 * F);
+                if (e >= total || n2 >= N2) continue;
+                C v = A.ld(e);
+                if (DST == kDstComplex) {
+                    if (T.tw4) v = c_mulw<ArF64>(v, CxW<ArF64>{w[j].x, w[j].y});
+                    dst[(long long)k1 * N2 + n2] = v;
+                } else {
+                    emit(P.work, it, tr.c, tr.b, 2LL * k1, v.re);
+                    emit(P.work, it, tr.c, tr.b, 2LL * k1 + 1, -v.im);
                 }
-                dst[(long long)k1 * N2 + n2] = v;
-            } else {
-                emit(P.work, it, tr.c, tr.b, 2LL * k1, v.re);
-                emit(P.work, it, tr.c, tr.b, 2LL * k1 + 1, -v.im);
             }
         }
         __syncthreads();
