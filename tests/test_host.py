@@ -208,3 +208,26 @@ def test_two_rank_reference_bench_on_cpu():
     assert len(lines) == 1
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["value"] > 0 and d["n_gpus"] == 2
+
+
+@pytest.mark.parametrize("n,split,radices", [
+    (100800, (315, 320), [(15, 21), (16, 20)]),   # C2 forward: two radices per sub-FFT
+    (46305, (147, 315), [(7, 21), (15, 21)]),     # C2 inverse
+    (222264, (441, 504), [(21, 21), (21, 24)]),   # C5 inverse
+    (967680, (960, 1008), [(30, 32), (8, 9, 14)]),  # C5 forward: no four-radix split, so 1008 takes three
+])
+def test_split_form_plans(n, split, radices):
+    """The split form's transform plans (the Python model of make_tc_fft, which bench.py uses to count the
+    tensor-core work): four radices <= 32 where any split allows them, else a three-radix sub-FFT whose every
+    stage has at most 128 rows."""
+    from kbsrc_b200 import roofline
+    assert roofline.tc_split(n) == split
+    got = [roofline.tc_radices(N) for N in split]
+    assert got == radices
+    for N, rads in zip(split, got):
+        assert all(r <= 32 for r in rads) and N // min(rads) <= 128
+
+
+def test_split_form_rejects_large_prime_factors():
+    from kbsrc_b200 import roofline
+    assert roofline.tc_split(2 * 2087 * 9) is None
