@@ -12,13 +12,21 @@
 
 // Launch shapes the shared-memory passes are compiled for: at most KB_MAXT_* threads per CTA and KB_MINB_*
 // resident CTAs per SM, which caps registers at 64K / (threads * CTAs). Double-double: 192 x 3 (96 registers,
-// 18 warps per SM, measured fastest); f64: 256 x 3 (80 registers); x87 extended: 192 x 2 (170 registers: the
-// integer emulation holds 128-bit intermediates).
+// 18 warps per SM, measured fastest) for the row and direct passes, 320 x 2 for the column passes (their shared
+// memory allows two CTAs: 20 warps per SM; C2 forward column 1.16 -> 1.05 ms, while the row passes lose with
+// it); f64: 256 x 3 (80 registers); x87 extended: 192 x 2 (170 registers: the integer emulation holds 128-bit
+// intermediates).
 #ifndef KB_MINB_DD
 #define KB_MINB_DD 3
 #endif
 #ifndef KB_MAXT_DD
 #define KB_MAXT_DD 192
+#endif
+#ifndef KB_MINB_DD_COL
+#define KB_MINB_DD_COL 2
+#endif
+#ifndef KB_MAXT_DD_COL
+#define KB_MAXT_DD_COL 320
 #endif
 #ifndef KB_MINB_X80
 #define KB_MINB_X80 2
@@ -100,6 +108,7 @@ struct ArF64 {  // Precision::Fast: float64 everywhere (V4 lanes and scalar alik
     using W = double;
     static constexpr bool kLanes = true, kLaneRenorm = false, kWide = false;
     static constexpr int kMinBlocks = KB_MINB_F64, kMaxThreads = KB_MAXT_F64;
+    static constexpr int kColMinBlocks = KB_MINB_F64, kColMaxThreads = KB_MAXT_F64;
     static __device__ __forceinline__ R add(R a, R b) { return __dadd_rn(a, b); }
     static __device__ __forceinline__ R sub(R a, R b) { return __dsub_rn(a, b); }
     static __device__ __forceinline__ R mul(R a, R b) { return __dmul_rn(a, b); }
@@ -115,6 +124,7 @@ struct ArDDShort {  // four-step sub-FFTs of Precision::Exact (DD4 lanes)
     using W = dd;
     static constexpr bool kLanes = true, kLaneRenorm = true, kWide = true;
     static constexpr int kMinBlocks = KB_MINB_DD, kMaxThreads = KB_MAXT_DD;
+    static constexpr int kColMinBlocks = KB_MINB_DD_COL, kColMaxThreads = KB_MAXT_DD_COL;
     static __device__ __forceinline__ R add(R a, R b) { return add_short(a, b); }
     static __device__ __forceinline__ R sub(R a, R b) { return add_short(a, dd_neg(b)); }
     static __device__ __forceinline__ R mul(R a, R b) { return mul_dd(a, b); }
@@ -131,6 +141,7 @@ struct ArDDAccurate {  // scalar dd: direct SFFT, Bluestein, RFFT split/merge, s
     using W = dd;
     static constexpr bool kLanes = false, kLaneRenorm = false, kWide = true;
     static constexpr int kMinBlocks = KB_MINB_DD, kMaxThreads = KB_MAXT_DD;
+    static constexpr int kColMinBlocks = KB_MINB_DD_COL, kColMaxThreads = KB_MAXT_DD_COL;
     static __device__ __forceinline__ R add(R a, R b) { return add_accurate(a, b); }
     static __device__ __forceinline__ R sub(R a, R b) { return add_accurate(a, dd_neg(b)); }
     static __device__ __forceinline__ R mul(R a, R b) { return mul_dd(a, b); }
@@ -147,6 +158,7 @@ struct ArX80 {  // Precision::LongDouble: x87 extended everywhere, one lane (CFF
     using W = x80;
     static constexpr bool kLanes = false, kLaneRenorm = false, kWide = true;
     static constexpr int kMinBlocks = KB_MINB_X80, kMaxThreads = KB_MAXT_X80;
+    static constexpr int kColMinBlocks = KB_MINB_X80, kColMaxThreads = KB_MAXT_X80;
     static __device__ __forceinline__ R add(R a, R b) { return x80_add(a, b); }
     static __device__ __forceinline__ R sub(R a, R b) { return x80_sub(a, b); }
     static __device__ __forceinline__ R mul(R a, R b) { return x80_mul(a, b); }

@@ -216,7 +216,7 @@ __device__ __forceinline__ CxW<Ar>* twiddle_smem(unsigned char* after_planes) {
 // Column pass: sequences n2 in [c0, c0+F) of length N1 (stride N2), twiddle, store in place
 // (fft.hpp:283-299). blockIdx.x: column group; blockIdx.y: task slot.
 template <class Ar, int SRC>
-__global__ void __launch_bounds__(Ar::kMaxThreads, Ar::kMinBlocks) k_column(const __grid_constant__ PassParams<Ar> P) {
+__global__ void __launch_bounds__(Ar::kColMaxThreads, Ar::kColMinBlocks) k_column(const __grid_constant__ PassParams<Ar> P) {
     extern __shared__ __align__(16) unsigned char smem[];
     using C = CxR<Ar>;
     const int F = P.F, N1 = P.N1, N2 = P.N2, total = N1 * F;
@@ -782,6 +782,12 @@ struct DevBuf {
 enum TabFmt { kTabF64 = 0, kTabDD = 1, kTabX80 = 2 };
 
 size_t tab_esize(int tab) { return tab == kTabF64 ? 16 : 32; }
+// Most threads per CTA the column (or row) pass kernels of a table format are compiled for
+int tab_max_threads(int tab, bool column) {
+    if (tab == kTabF64) return KB_MAXT_F64;
+    if (tab == kTabX80) return KB_MAXT_X80;
+    return column ? KB_MAXT_DD_COL : KB_MAXT_DD;
+}
 
 // Bytes of one input sample in a KBSRC_GPU_IN_* format
 size_t in_bytes(int fmt) {
@@ -872,7 +878,7 @@ int env_int(const char* name, int dflt);
 
 // F sequences per CTA (a divisor of `count` when one fits) and T threads, within a shared-memory budget; the
 // block also holds the sub-FFT's twiddles in double-double.
-Shape pick_shape(const SubPlan& sp, int count, size_t esize, int fmax) {
+Shape pick_shape(const SubPlan& sp, int count, size_t esize, int fmax, int maxT) {
     const size_t budget = (size_t)env_int("KBSRC_GPU_SMEM_KB", 100) * 1024;
     const size_t tw = esize == 32 ? (size_t)sp.twn * esize : 0;
     int F = 1;
@@ -882,7 +888,7 @@ Shape pick_shape(const SubPlan& sp, int count, size_t esize, int fmax) {
         if (count % f == 0) { F = f; break; }
     }
     int T = ((max_bfly(sp) * F + 31) / 32) * 32;
-    T = std::max(64, std::min(env_int("KBSRC_GPU_THREADS", esize == 32 ? KB_MAXT_DD : kThreadsF64), T));
+    T = std::max(64, std::min(std::min(env_int("KBSRC_GPU_THREADS", maxT), maxT), T));
     return Shape{F, T, 2 * (size_t)sp.n * F * esize + tw};
 }
 
@@ -936,8 +942,9 @@ int make_dev_cfft(int n, int tab, int fmax, DevCfft& d, cudaStream_t st) {
     std::vector<HostCx>().swap(d.host.tw_stage);
     std::vector<HostCx>().swap(d.host.tw4);
     if (d.host.four) {
-        d.col = pick_shape(d.host.s1, d.host.N2, esize, fmax);
-        d.row = pick_shape(d.host.s2, d.host.N1, esize, fmax);
+        // default thread caps: float64 kThreadsF64 (the autotuner tries up to the compiled maximum)
+        d.col = pick_shape(d.host.s1, d.host.N2, esize, fmax, tab == kTabF64 ? kThreadsF64 : tab_max_threads(tab, true));
+        d.row = pick_shape(d.host.s2, d.host.N1, esize, fmax, tab == kTabF64 ? kThreadsF64 : tab_max_threads(tab, false));
     } else {
         d.dir = direct_shape(d.host.sd, esize);
     }
@@ -2462,7 +2469,8 @@ int kbsrc_gpu_engine_tune(kbsrc_gpu_engine* e, const double* d_in, const double*
             pass[3] = &e->iv.row; sub[3] = &e->iv.host.s2; count[3] = e->iv.host.N1;
         }
         const size_t esize = e->esize();
-        const int maxT = e->tab == kTabF64 ? KB_MAXT_F64 : e->tab == kTabX80 ? KB_MAXT_X80 : KB_MAXT_DD;
+        const int maxT[4] = {tab_max_threads(e->tab, true), tab_max_threads(e->tab, false),
+                             tab_max_threads(e->tab, true), tab_max_threads(e->tab, false)};  // col, row, col, row
         int dev = 0, smem_max = 0;
         KB_CUDA(cudaGetDevice(&dev));
         KB_CUDA(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
@@ -2473,7 +2481,7 @@ int kbsrc_gpu_engine_tune(kbsrc_gpu_engine* e, const double* d_in, const double*
             for (int F : {1, 2, 3, 4, 5, 6, 8, 10, 12, 16}) {
                 const size_t sm = 2 * (size_t)sub[p]->n * F * esize + tw;
                 if (F > count[p] || sm > (size_t)smem_max) continue;
-                for (int T = 64; T <= maxT; T += 32) cand[p].push_back(Shape{F, T, sm});
+                for (int T = 64; T <= maxT[p]; T += 32) cand[p].push_back(Shape{F, T, sm});
             }
             cand[p].push_back(*pass[p]);  // the default stays a candidate
         }
@@ -2843,7 +2851,7 @@ int kbsrc_gpu_kernel_spectrum_static(const double* d_taps, int L, int n, double 
         p.ddreal = r;
         p.stride = 0;
         if (c.four) {
-            const Shape sc = pick_shape(c.s1, c.N2, esize, 4), sr = pick_shape(c.s2, c.N1, esize, 4);
+            const Shape sc = pick_shape(c.s1, c.N2, esize, 4, KB_MAXT_DD_COL), sr = pick_shape(c.s2, c.N1, esize, 4, KB_MAXT_DD);
             p.sp = c.s1; p.N1 = c.N1; p.N2 = c.N2; p.F = sc.F;
             p.tw4 = reinterpret_cast<const CxW<ArDDAccurate>*>(base + off_t4);
             p.src = A; p.dst = A;
