@@ -214,7 +214,9 @@ __device__ __forceinline__ CxW<Ar>* twiddle_smem(unsigned char* after_planes) {
 }
 
 // Column pass: sequences n2 in [c0, c0+F) of length N1 (stride N2), twiddle, store in place
-// (fft.hpp:283-299). blockIdx.x: column group; blockIdx.y: task slot.
+// (fft.hpp:283-299). blockIdx.x: column group; blockIdx.y: task slot. Reading the staged signal, the two are
+// swapped (task slot fastest): the channels of a block are consecutive tasks, and their CTAs for one column group
+// then run side by side and share the interleaved input's sectors in L2.
 template <class Ar, int SRC>
 __global__ void __launch_bounds__(Ar::kColMaxThreads, Ar::kColMinBlocks) k_column(const __grid_constant__ PassParams<Ar> P) {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -223,10 +225,11 @@ __global__ void __launch_bounds__(Ar::kColMaxThreads, Ar::kColMinBlocks) k_colum
     const FastDiv dF = fast_div(F);
     Planes<Ar> A, B;
     unsigned char* rest = carve<Ar>(smem, total, A, B);
-    const long long task = P.task0 + blockIdx.y;
-    const int c0 = blockIdx.x * F;
-    const C* src = P.src + blockIdx.y * P.stride;
-    C* dst = P.dst + blockIdx.y * P.stride;
+    const unsigned slot = SRC == kSrcSignal ? blockIdx.x : blockIdx.y, group = SRC == kSrcSignal ? blockIdx.y : blockIdx.x;
+    const long long task = P.task0 + slot;
+    const int c0 = group * F;
+    const C* src = P.src + slot * P.stride;
+    C* dst = P.dst + slot * P.stride;
     const TaskSource ts = SRC == kSrcSignal ? task_source(P.work, task, 2LL * N1 * N2) : TaskSource{};
     const CxW<Ar>* tws = stage_twiddles<Ar>(P.sp, P.tw_stage, twiddle_smem<Ar>(rest));
     for (int e0 = threadIdx.x; e0 < total; e0 += kLoadBatch * blockDim.x) {
@@ -1357,7 +1360,9 @@ int launch_smooth(const DevCfft& c, const Slots& sl, void* x, void* y, cudaStrea
     if (h.four) {
         PassParams<ArL> p = pass_params<ArL>(sl, c, x, x);
         p.sp = h.s1; p.N1 = h.N1; p.N2 = h.N2; p.F = c.col.F;
-        k_column<ArL, SRC><<<dim3((h.N2 + p.F - 1) / p.F, sl.nt), c.col.T, c.col.smem, st>>>(p);
+        const unsigned groups = (unsigned)((h.N2 + p.F - 1) / p.F);
+        k_column<ArL, SRC><<<SRC == kSrcSignal ? dim3((unsigned)sl.nt, groups) : dim3(groups, (unsigned)sl.nt), c.col.T,
+                             c.col.smem, st>>>(p);
         if ((rc = tr.mark(st, kA)) != KBSRC_GPU_OK) return rc;
         p.sp = h.s2; p.F = c.row.F; p.src = static_cast<CxR<ArL>*>(x); p.dst = static_cast<CxR<ArL>*>(y);
         k_row<ArL, DST><<<dim3((h.N1 + p.F - 1) / p.F, sl.nt), c.row.T, c.row.smem, st>>>(p);
