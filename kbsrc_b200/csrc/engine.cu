@@ -557,9 +557,9 @@ struct TcParams {
 };
 
 // Column pass, persistent: each CTA sets up its tensor memory and tables once, then takes items (column group
-// g, task slot y) in turn, item = y * groups + g. An item: sequences n2 in [c0, c0+F) of length N1 (stride N2),
-// the sub-FFT, the four-step twiddle, stored in place; with N2 == 1 the single column is the whole transform and
-// DST may write it as output samples.
+// g, task slot y) in turn, item = y * groups + g (reading the signal: item = g * slots + y). An item: sequences
+// n2 in [c0, c0+F) of length N1 (stride N2), the sub-FFT, the four-step twiddle, stored in place; with N2 == 1
+// the single column is the whole transform and DST may write it as output samples.
 template <int SRC, int DST>
 __global__ void __launch_bounds__(kTcThreads, 1)
     k_tc_column(const __grid_constant__ PassParams<ArF64> P, const __grid_constant__ TcParams T) {
@@ -571,7 +571,9 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     const uint32_t tmem = tc_setup(m, T.sub);
     uint32_t phase = 0;
     for (long long item = blockIdx.x; item < (long long)groups * T.slots; item += gridDim.x) {
-        const int slot = (int)(item / groups), c0 = (int)(item - (long long)slot * groups) * F;
+        // reading the signal, the task slot varies fastest: the channels of a block share input sectors in L2
+        const int slot = SRC == kSrcSignal ? (int)(item % T.slots) : (int)(item / groups);
+        const int c0 = (SRC == kSrcSignal ? (int)(item / T.slots) : (int)(item - (long long)slot * groups)) * F;
         const long long task = P.task0 + slot;
         const C* src = P.src + slot * P.stride;
         C* dst = P.dst + slot * P.stride;
