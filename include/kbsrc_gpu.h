@@ -150,18 +150,23 @@ void kbsrc_gpu_batch_destroy(kbsrc_gpu_batch* b);
  * taps: (L+1) (hi, lo) pairs; H: (n/2+1) (hi, lo) pairs out. n must be even. */
 int kbsrc_gpu_kernel_spectrum(const double* taps, int L, int n, double scale, double* H);
 
-/* The same kernel spectrum for callers that cannot allocate device memory (a fixed memory pool, a real-time
- * thread that must not enter the allocator, a region being captured into a CUDA graph by a framework that
- * forbids allocation). No counterpart in the reference: it exists for such callers only.
+/* The same kernel spectrum for callers that cannot let a library allocate GPU memory. No counterpart in the
+ * reference: it exists for such callers only. Examples: an application that reserves the device's memory up front
+ * for its own pool (a framework's caching allocator, an audio host that budgets the GPU at start-up) and has nothing
+ * left for cudaMalloc, or one whose other streams must not stall, which they would at the device-wide wait inside
+ * cudaFree.
  *   d_taps  (L+1) (hi, lo) pairs in device memory; d_H  (n/2+1) (hi, lo) pairs out, device memory
- *   stream  cudaStream_t to run on (NULL: the CUDA default stream); the call returns once the work is queued
- * It calls no cudaMalloc, cudaFree or other allocator: its scratch is one 24 MiB device array inside the library
- * (present on every GPU that loads it, until exit), so n is limited to about 300,000 points (80 bytes per point);
- * larger n returns KBSRC_GPU_E_ARG with the sizes in the message, and n/2 must be 7-smooth (otherwise
- * KBSRC_GPU_E_UNSUPPORTED: the Bluestein tables would need more scratch). The first call on each device looks up the
- * array's device address (cudaGetSymbolAddress) and sets kernel attributes; make that first call before any
- * stream capture. All calls share the one array and it keeps the previous call's contents (each call rewrites
- * what it reads), so calls that can overlap on the GPU (other streams, other threads) race: serialise them. */
+ *   stream  cudaStream_t to run on (NULL: the CUDA default stream); the call returns once its kernels are queued
+ * It calls no cudaMalloc, cudaFree or other allocating routine, and builds and copies no host table: its scratch
+ * (work buffers and every twiddle table, computed on the GPU) is one 24 MiB device array inside the library, present
+ * on every GPU that loads the library until the process exits. So n is limited to about 300,000 points (80 bytes
+ * per point); a larger n returns KBSRC_GPU_E_ARG with the sizes in the message. The n/2-point transform must also
+ * have a plan without Bluestein's chirp-z (n/2 7-smooth) whose four-step sub-FFTs have at most 32768 points;
+ * otherwise the call returns KBSRC_GPU_E_UNSUPPORTED (use kbsrc_gpu_kernel_spectrum for such n). The array's device
+ * address is looked up on every call (cudaGetSymbolAddress, in the current device's context); the first call on a
+ * device also sets kernel attributes, so make it before any stream capture. All calls share the one array and it
+ * keeps the previous call's contents (each call rewrites all it reads), so calls that can overlap on the GPU (other
+ * streams, other threads) race: serialise them. */
 int kbsrc_gpu_kernel_spectrum_static(const double* d_taps, int L, int n, double scale, double* d_H, void* stream);
 
 /* Text of the last error on this thread ("" if none). */

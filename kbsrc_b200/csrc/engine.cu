@@ -680,9 +680,10 @@ struct HostCx {
     hd::dd re, im;
 };
 
-// Stockham plan of n points: radices 4,..,4,2,..,2,3,..,5,..,7,.. (fft.hpp:93-97); stage twiddles
-// w_n^{s p u} appended to `tw` (fft.hpp:98-107).
-int build_sub(int n, std::vector<HostCx>& tw, SubPlan& sp) {
+// Stockham plan of n points: radices 4,..,4,2,..,2,3,..,5,..,7,.. (fft.hpp:93-97), its stage twiddles to start
+// at table entry tw0, m * (r - 1) entries per stage (one entry when there are none, keeping the table pointer
+// valid for n = 1). Builds nothing but the plan.
+int plan_sub(int n, int tw0, SubPlan& sp) {
     int rs[64], ns = 0, t = n;
     while (t % 4 == 0) { rs[ns++] = 4; t /= 4; }
     while (t % 2 == 0) { rs[ns++] = 2; t /= 2; }
@@ -693,23 +694,34 @@ int build_sub(int n, std::vector<HostCx>& tw, SubPlan& sp) {
     std::memset(&sp, 0, sizeof sp);
     sp.n = n;
     sp.nst = ns;
-    sp.tw0 = (int)tw.size();
-    hd::RootTable rt(n);
-    int rem = n, s = 1;
+    sp.tw0 = tw0;
+    int rem = n, s = 1, at = tw0;
     for (int g = 0; g < ns; g++) {
         const int r = rs[g], m = rem / r;
-        sp.st[g] = Stage{r, m, s, (int)tw.size()};
-        for (int p = 0; p < m; p++)
-            for (int u = 1; u < r; u++) {
-                HostCx w;
-                rt.get(-(long long)s * p * u, w.re, w.im);
-                tw.push_back(w);
-            }
+        sp.st[g] = Stage{r, m, s, at};
+        at += m * (r - 1);
         rem /= r;
         s *= r;
     }
-    if (tw.empty()) tw.push_back(HostCx{});  // keep the table pointer valid for n = 1
-    sp.twn = (int)tw.size() - sp.tw0;
+    sp.twn = std::max(1, at - tw0);
+    return KBSRC_GPU_OK;
+}
+
+// The plan of n points with its stage twiddles w_n^{s p u} appended to `tw` (fft.hpp:98-107).
+int build_sub(int n, std::vector<HostCx>& tw, SubPlan& sp) {
+    const int rc = plan_sub(n, (int)tw.size(), sp);
+    if (rc) return rc;
+    hd::RootTable rt(n);
+    for (int g = 0; g < sp.nst; g++) {
+        const Stage& st = sp.st[g];
+        for (int p = 0; p < st.m; p++)
+            for (int u = 1; u < st.r; u++) {
+                HostCx w;
+                rt.get(-(long long)st.s * p * u, w.re, w.im);
+                tw.push_back(w);
+            }
+    }
+    if ((int)tw.size() == sp.tw0) tw.push_back(HostCx{});
     return KBSRC_GPU_OK;
 }
 
@@ -720,8 +732,9 @@ struct HostCfft {
 };
 
 // Complex FFT of n points (fft.hpp:226-265): direct up to 2048 points, else four-step with N1 the largest
-// divisor <= sqrt(n) (falling back to direct when N1 < 8).
-int build_cfft(int n, HostCfft& c) {
+// divisor <= sqrt(n) (falling back to direct when N1 < 8). The plan only: sub-plans with their stage twiddles laid
+// out in one table (s1's, then s2's), no tables built.
+int plan_cfft(int n, HostCfft& c) {
     c.n = n;
     if (!hd::smooth7(n)) return fail(KBSRC_GPU_E_UNSUPPORTED, "FFT length not 7-smooth (Bluestein)");
     c.four = n > 2048;
@@ -736,9 +749,17 @@ int build_cfft(int n, HostCfft& c) {
     // the passes divide indices through fast_div, exact while index * divisor < 2^32: sub-FFTs up to 2^15 points
     if ((c.four ? std::max(c.N1, c.N2) : n) > 32768)
         return fail(KBSRC_GPU_E_UNSUPPORTED, "FFT length without a four-step split into sub-FFTs of at most 32768");
-    if (!c.four) return build_sub(n, c.tw_stage, c.sd);
-    int rc = build_sub(c.N1, c.tw_stage, c.s1);
+    if (!c.four) return plan_sub(n, 0, c.sd);
+    const int rc = plan_sub(c.N1, 0, c.s1);
+    return rc ? rc : plan_sub(c.N2, c.s1.twn, c.s2);
+}
+
+// The plan with its host tables: stage twiddles and the four-step twiddles w_n^{-k1 n2}.
+int build_cfft(int n, HostCfft& c) {
+    int rc = plan_cfft(n, c);
     if (rc) return rc;
+    if (!c.four) return build_sub(n, c.tw_stage, c.sd);
+    if ((rc = build_sub(c.N1, c.tw_stage, c.s1)) != KBSRC_GPU_OK) return rc;
     if ((rc = build_sub(c.N2, c.tw_stage, c.s2)) != KBSRC_GPU_OK) return rc;
     c.tw4.resize((size_t)n);
     hd::RootTable rt(n);
@@ -1242,16 +1263,18 @@ const OddRoots<W>& odd_table() {
     return t;
 }
 
-// Lets every pass kernel use up to the device's shared memory per block (once per device).
+// Lets every pass kernel use up to the device's shared memory per block. The attribute belongs to the current
+// context, so whether it is set is read back from the context (the last kernel set below) rather than remembered.
 int allow_large_smem() {
-    static bool done[64] = {};
     static std::mutex mu;
     std::lock_guard<std::mutex> lock(mu);
     int dev = 0;
     KB_CUDA(cudaGetDevice(&dev));
-    if (dev < 64 && done[dev]) return KBSRC_GPU_OK;
     int mx = 0;
     KB_CUDA(cudaDeviceGetAttribute(&mx, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    cudaFuncAttributes fa{};
+    KB_CUDA(cudaFuncGetAttributes(&fa, (const void*)k_tc_row<kDstOutput>));
+    if (fa.maxDynamicSharedSizeBytes >= mx) return KBSRC_GPU_OK;
 #define KB_SMEM(k) KB_CUDA(cudaFuncSetAttribute((const void*)(k), cudaFuncAttributeMaxDynamicSharedMemorySize, mx))
     KB_SMEM((k_column<ArF64, kSrcSignal>));
     KB_SMEM((k_column<ArF64, kSrcComplex>));
@@ -1282,9 +1305,8 @@ int allow_large_smem() {
     KB_SMEM((k_tc_column<kSrcComplex, kDstComplex>));
     KB_SMEM((k_tc_column<kSrcComplex, kDstOutput>));
     KB_SMEM((k_tc_row<kDstComplex>));
-    KB_SMEM((k_tc_row<kDstOutput>));
+    KB_SMEM((k_tc_row<kDstOutput>));  // last: the marker read above
 #undef KB_SMEM
-    if (dev < 64) done[dev] = true;
     return KBSRC_GPU_OK;
 }
 
@@ -2260,12 +2282,14 @@ int batch_run_device_impl(kbsrc_gpu_batch& b, const double* const* in, const dou
 
 // ---- kernel spectrum for callers that cannot allocate device memory ----------------------------------------
 //
-// Some callers own every device allocation themselves and may not call cudaMalloc from a library: a host that
-// runs on a fixed, pre-reserved memory pool, a real-time audio thread that must not block in the allocator, or
-// code being captured into a CUDA graph by a framework that forbids allocation inside the region. For them,
-// kbsrc_gpu_kernel_spectrum_static takes its inputs and outputs in device memory and keeps all of its scratch
-// (the placed taps, two FFT work buffers, the twiddle tables) in one file-scope device array below. The array
-// is part of the library image: every GPU that loads the library holds it until the process exits.
+// Some callers may not let a library allocate GPU memory. An application that reserves the device's memory up
+// front for its own pool (a framework's caching allocator, an audio host that budgets the GPU at start-up) can
+// have nothing left for cudaMalloc, and cudaFree waits for the whole device, stalling the caller's other streams.
+// For them kbsrc_gpu_kernel_spectrum_static takes its taps and its output in device memory and keeps all of its
+// scratch (the placed taps, two FFT work buffers, the twiddle tables and the root tables they are built from) in
+// one file-scope device array below. The array is part of the library image: every GPU that loads the library
+// holds it until the process exits. The tables are computed on the GPU as well, so the call builds nothing on
+// the host and copies nothing from host memory: it only launches kernels on the caller's stream.
 
 // Capacity of the shared scratch: transforms up to about 300,000 points (80 bytes per point), which covers the
 // automatic plans of the common rates (for example 201,600 points for 96 kHz -> 44.1 kHz at --len 0.2).
@@ -2274,8 +2298,114 @@ static __device__ __align__(256) unsigned char g_spectrum_scratch[kSpectrumScrat
 
 namespace {
 
-std::mutex g_scratch_mu;
-void* g_scratch_ptr[64] = {};  // device address of g_spectrum_scratch, per device, looked up on first use
+// Roots of unity on the device, bit-identical to the host's tables: kbsrc::host::unit_root and RootTable
+// (host/ddh.hpp), which build the reference's CisTable (src/dsp/fft.hpp:29-43) from dd Taylor series after an
+// exact octant reduction. Each function below runs the host function's IEEE operations in the same order: the
+// accurate dd add, the dd product with one fma, the dd-by-double product and the three-digit division.
+constexpr double kPiHi = 3.141592653589793116e+00, kPiLo = 1.224646799147353207e-16;
+
+__device__ __forceinline__ dd dvr_mul_f(dd a, double b) {  // dd * double
+    const double p = __dmul_rn(a.hi, b);
+    double e = __fma_rn(a.hi, b, -p);
+    e = __dadd_rn(e, __dmul_rn(a.lo, b));
+    return qts(p, e);
+}
+
+// cos and sin of x in [0, pi/4] by their Taylor series in dd
+__device__ void dvr_sincos(dd x, dd& c, dd& s) {
+    const dd x2 = mul_dd(x, x);
+    dd ts = x, ss = x, tc{1.0, 0.0}, cc{1.0, 0.0};
+    for (int k = 1; k < 40; k++) {
+        tc = div_dd_f64(dd_neg(mul_dd(tc, x2)), (double)((2 * k - 1) * (2 * k)));
+        cc = add_accurate(cc, tc);
+        ts = div_dd_f64(dd_neg(mul_dd(ts, x2)), (double)((2 * k) * (2 * k + 1)));
+        ss = add_accurate(ss, ts);
+        if (fabs(ts.hi) < 1e-40 && fabs(tc.hi) < 1e-40) break;
+    }
+    c = cc;
+    s = ss;
+}
+
+// e^{+2 pi i k / n} = c + i s
+__device__ void dvr_unit_root(long long k, long long n, dd& c, dd& s) {
+    k %= n;
+    if (k < 0) k += n;
+    const long long eighths = 8 * k, oct = eighths / n, rem = eighths - oct * n;
+    const bool mirrored = oct & 1;
+    long long quadrant = oct / 2;
+    const dd phi = div_dd_f64(dvr_mul_f(dd{kPiHi / 4, kPiLo / 4}, (double)(mirrored ? n - rem : rem)), (double)n);
+    dd cr, sr;
+    dvr_sincos(phi, cr, sr);
+    if (mirrored) {
+        sr = dd_neg(sr);
+        quadrant += 1;
+    }
+    switch (quadrant & 3) {
+        case 0: c = cr; s = sr; break;
+        case 1: c = dd_neg(sr); s = cr; break;
+        case 2: c = dd_neg(cr); s = dd_neg(sr); break;
+        default: c = sr; s = dd_neg(cr); break;
+    }
+}
+
+// A root table of n on the device: `coarse` entries w^(j step) followed by `step` entries w^l, as cx<dd> (c, s).
+struct DevRoots {
+    const cx<dd>* t;
+    long long n, step, coarse;
+};
+DevRoots dev_roots_shape(long long n) {
+    DevRoots r{};
+    r.n = n;
+    r.step = (long long)std::ceil(std::sqrt((double)n));  // as RootTable's constructor
+    r.coarse = n / r.step + 1;
+    return r;
+}
+
+__global__ void k_roots_build(DevRoots r, cx<dd>* out) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < r.coarse + r.step;
+         i += (long long)gridDim.x * blockDim.x) {
+        dd c, s;
+        dvr_unit_root(i < r.coarse ? i * r.step : i - r.coarse, r.n, c, s);
+        out[i] = cx<dd>{c, s};
+    }
+}
+
+// e^{2 pi i k/n} from the table: the dd product of a coarse and a fine entry (RootTable::get)
+__device__ cx<dd> dvr_get(const DevRoots& r, long long k) {
+    k %= r.n;
+    if (k < 0) k += r.n;
+    const long long j = k / r.step, l = k % r.step;
+    const cx<dd> a = r.t[j], b = r.t[r.coarse + l];
+    if (l == 0) return a;
+    if (j == 0) return b;
+    return cx<dd>{add_accurate(mul_dd(a.re, b.re), dd_neg(mul_dd(a.im, b.im))),
+                  add_accurate(mul_dd(a.re, b.im), mul_dd(a.im, b.re))};
+}
+
+// out[k] = w^(-k) for k < count (the real-FFT split roots), or out[k1 * N2 + n2] = w^(-k1 n2) (four-step twiddles;
+// N2 > 0)
+__global__ void k_roots_table(DevRoots r, long long count, int N2, cx<dd>* out) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < count;
+         i += (long long)gridDim.x * blockDim.x)
+        out[i] = dvr_get(r, N2 ? -(i / N2) * (i % N2) : -i);
+}
+
+// The stage twiddles of a sub-plan, w^(-s p u) at sp.st[g].tw + p (r - 1) + u - 1 (build_sub's layout); `out` is
+// entry sp.tw0
+__global__ void k_roots_stages(DevRoots r, SubPlan sp, cx<dd>* out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < sp.twn; i += gridDim.x * blockDim.x) {
+        const int e = sp.tw0 + i;
+        int g = 0;
+        while (g + 1 < sp.nst && e >= sp.st[g + 1].tw) g++;
+        const Stage& st = sp.st[g];
+        if (sp.nst == 0 || e - st.tw >= st.m * (st.r - 1)) {  // the placeholder entry of a plan without twiddles
+            out[i] = cx<dd>{dd{0.0, 0.0}, dd{0.0, 0.0}};
+            continue;
+        }
+        const int p = (e - st.tw) / (st.r - 1), u = (e - st.tw) % (st.r - 1) + 1;
+        out[i] = dvr_get(r, -(long long)st.s * p * u);
+    }
+}
 
 // r[i] = h[i] for i <= L, h[n - i] for i >= n - L, else 0 (the circular placement of design.cpp:42-43);
 // every entry is written, so nothing left by an earlier call survives.
@@ -2806,55 +2936,67 @@ int kbsrc_gpu_kernel_spectrum_static(const double* d_taps, int L, int n, double 
         if (rc) return rc;
         rc = allow_large_smem();
         if (rc) return rc;
-        int dev = 0;
-        KB_CUDA(cudaGetDevice(&dev));
-        if (dev < 0 || dev >= 64) return fail(KBSRC_GPU_E_ARG, "device index out of range");
-        unsigned char* base = nullptr;
-        {
-            std::lock_guard<std::mutex> lock(g_scratch_mu);
-            if (!g_scratch_ptr[dev]) {
-                void* p = nullptr;
-                const cudaError_t e = cudaGetSymbolAddress(&p, g_spectrum_scratch);
-                if (e != cudaSuccess || !p)
-                    return fail(KBSRC_GPU_E_CUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
-                g_scratch_ptr[dev] = p;
-            }
-            base = static_cast<unsigned char*>(g_scratch_ptr[dev]);
-        }
-        // plan and tables on the host (dd, exactly as the allocating entry builds them)
+        // the device address of the scratch array in the current device's context, looked up on every call (it
+        // allocates nothing and stays right if the context is ever recreated)
+        void* sym = nullptr;
+        const cudaError_t se = cudaGetSymbolAddress(&sym, g_spectrum_scratch);
+        if (se != cudaSuccess || !sym)
+            return fail(KBSRC_GPU_E_CUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(se));
+        unsigned char* base = static_cast<unsigned char*>(sym);
+        // the plan only (fixed-size structures); every table is computed on the device below
         const int h = n / 2;
         HostCfft c;
-        if ((rc = build_cfft(h, c)) != KBSRC_GPU_OK) return rc;
-        const std::vector<HostCx> w = split_roots(n);
+        if ((rc = plan_cfft(h, c)) != KBSRC_GPU_OK) return rc;
         const size_t esize = 32;
-        const size_t off_r = 0, off_A = align256(off_r + (size_t)n * 16), off_B = align256(off_A + (size_t)(h + 1) * esize),
-                     off_w = align256(off_B + (size_t)(h + 1) * esize), off_ts = align256(off_w + w.size() * esize),
-                     off_t4 = align256(off_ts + c.tw_stage.size() * esize),
-                     end = align256(off_t4 + c.tw4.size() * esize);
-        if (end > kSpectrumScratchBytes)
+        const long long n_stage = c.four ? (long long)c.s1.twn + c.s2.twn : c.sd.twn;
+        DevRoots rt_w = dev_roots_shape(n), rt_h = dev_roots_shape(h), rt_1 = dev_roots_shape(c.four ? c.N1 : h),
+                 rt_2 = dev_roots_shape(c.four ? c.N2 : 1);
+        size_t at = 0;
+        auto take = [&](size_t bytes) {
+            const size_t o = at;
+            at = align256(at + bytes);
+            return o;
+        };
+        const size_t off_r = take((size_t)n * 16), off_A = take((size_t)(h + 1) * esize),
+                     off_B = take((size_t)(h + 1) * esize), off_w = take((size_t)(h + 1) * esize),
+                     off_ts = take((size_t)n_stage * esize), off_t4 = take(c.four ? (size_t)h * esize : 0),
+                     off_rw = take((size_t)(rt_w.coarse + rt_w.step) * esize),
+                     off_rh = take(c.four ? (size_t)(rt_h.coarse + rt_h.step) * esize : 0),
+                     off_r1 = take((size_t)(rt_1.coarse + rt_1.step) * esize),
+                     off_r2 = take(c.four ? (size_t)(rt_2.coarse + rt_2.step) * esize : 0);
+        if (at > kSpectrumScratchBytes)
             return fail(KBSRC_GPU_E_ARG, "kernel spectrum of " + std::to_string(n) + " points needs " +
-                                             std::to_string(end) + " bytes of scratch; the static scratch holds " +
+                                             std::to_string(at) + " bytes of scratch; the static scratch holds " +
                                              std::to_string(kSpectrumScratchBytes) + " (about 300,000 points)");
         cudaStream_t st = static_cast<cudaStream_t>(stream);
-        auto put = [&](size_t off, const std::vector<HostCx>& v) -> int {
-            if (v.empty()) return KBSRC_GPU_OK;
-            std::vector<double> flat(v.size() * 4);
-            for (size_t i = 0; i < v.size(); i++) {
-                flat[4 * i] = v[i].re.hi; flat[4 * i + 1] = v[i].re.lo;
-                flat[4 * i + 2] = v[i].im.hi; flat[4 * i + 3] = v[i].im.lo;
-            }
-            KB_CUDA(cudaMemcpyAsync(base + off, flat.data(), flat.size() * 8, cudaMemcpyHostToDevice, st));
-            return KBSRC_GPU_OK;
-        };
-        if ((rc = put(off_w, w)) || (rc = put(off_ts, c.tw_stage)) || (rc = put(off_t4, c.tw4))) return rc;
         using C = CxR<ArDDAccurate>;
+        auto tab = [&](size_t off) { return reinterpret_cast<cx<dd>*>(base + off); };
+        // root tables, then the real-FFT split roots w_n^-k (k <= n/2), the stage and the four-step twiddles
+        auto roots = [&](DevRoots& r, size_t off) {
+            r.t = tab(off);
+            k_roots_build<<<grid_for(r.coarse + r.step, 128), 128, 0, st>>>(r, tab(off));
+        };
+        roots(rt_w, off_rw);
+        roots(rt_1, off_r1);
+        if (c.four) {
+            roots(rt_h, off_rh);
+            roots(rt_2, off_r2);
+        }
+        k_roots_table<<<grid_for(h + 1, 128), 128, 0, st>>>(rt_w, h + 1, 0, tab(off_w));
+        if (c.four) {
+            k_roots_stages<<<grid_for(c.s1.twn, 128), 128, 0, st>>>(rt_1, c.s1, tab(off_ts));
+            k_roots_stages<<<grid_for(c.s2.twn, 128), 128, 0, st>>>(rt_2, c.s2, tab(off_ts) + c.s1.twn);
+            k_roots_table<<<grid_for(h, 128), 128, 0, st>>>(rt_h, h, c.N2, tab(off_t4));
+        } else {
+            k_roots_stages<<<grid_for(c.sd.twn, 128), 128, 0, st>>>(rt_1, c.sd, tab(off_ts));
+        }
         double* r = reinterpret_cast<double*>(base + off_r);
         C* A = reinterpret_cast<C*>(base + off_A);
         C* B = reinterpret_cast<C*>(base + off_B);
         k_place_taps<<<grid_for(n, 256), 256, 0, st>>>(d_taps, L, n, r);
         PassParams<ArDDAccurate> p{};
         p.tw_stage = reinterpret_cast<const CxW<ArDDAccurate>*>(base + off_ts);
-        p.odd = odd_roots<dd>();
+        p.odd = odd_table<dd>();
         p.ddreal = r;
         p.stride = 0;
         if (c.four) {

@@ -1,10 +1,16 @@
 // kbsrc command-line tool on the GPU engine. Options, messages, exit codes (0 ok, 1 runtime error, 2 usage)
 // and the -v plan line are those of HongYue1/KBSRC app/main.cpp:84-165, so scripts and the reference's own
 // test suites drive it unchanged.
+#include <algorithm>
+#include <cerrno>
 #include <chrono>
+#include <climits>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <exception>
+#include <iterator>
+#include <type_traits>
 #include <new>
 #include <stdexcept>
 #include <string>
@@ -16,32 +22,45 @@
 
 namespace {
 
-struct UsageError : std::exception {
-    std::string msg;
-    explicit UsageError(std::string m) : msg(std::move(m)) {}
-    const char* what() const noexcept override { return msg.c_str(); }
+// A command line the tool cannot act on: reported as "kbsrc: <text> (see --help)" with exit status 2.
+struct BadCommandLine {
+    std::string text;
 };
 
-double now() { return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count(); }
-
-int parse_int(const std::string& v, const char* name) {
-    try {
-        size_t used;
-        const int r = std::stoi(v, &used);
-        if (used == v.size()) return r;
-    } catch (...) {
-    }
-    throw UsageError(std::string("invalid value for ") + name + ": " + v);
+double seconds_now() {
+    using clock = std::chrono::steady_clock;
+    return std::chrono::duration_cast<std::chrono::duration<double>>(clock::now().time_since_epoch()).count();
 }
 
-double parse_double(const std::string& v, const char* name) {
-    try {
-        size_t used;
-        const double r = std::stod(v, &used);
-        if (used == v.size() && std::isfinite(r)) return r;
-    } catch (...) {
-    }
-    throw UsageError(std::string("invalid value for ") + name + ": " + v);
+// Whole-string decimal numbers: leading blanks and a sign are accepted, trailing characters are not; an integer
+// must fit an int and a real number must be finite.
+bool whole_int(const std::string& text, int& out) {
+    const char* s = text.c_str();
+    char* end = nullptr;
+    errno = 0;
+    const long v = std::strtol(s, &end, 10);
+    if (end == s || *end != '\0' || errno == ERANGE || v < INT_MIN || v > INT_MAX) return false;
+    out = (int)v;
+    return true;
+}
+bool whole_real(const std::string& text, double& out) {
+    const char* s = text.c_str();
+    char* end = nullptr;
+    errno = 0;
+    const double v = std::strtod(s, &end);
+    if (end == s || *end != '\0' || errno == ERANGE || !std::isfinite(v)) return false;
+    out = v;
+    return true;
+}
+
+template <class T>
+T option_value(const std::string& text, const char* option) {
+    T v{};
+    bool ok;
+    if constexpr (std::is_same_v<T, int>) ok = whole_int(text, v);
+    else ok = whole_real(text, v);
+    if (!ok) throw BadCommandLine{std::string("invalid value for ") + option + ": " + text};
+    return v;
 }
 
 void help() {
@@ -73,61 +92,62 @@ int run(int argc, char** argv) {
     for (int i = 1; i < argc; i++) {
         const std::string a = argv[i];
         auto value = [&]() -> std::string {
-            if (i + 1 >= argc) throw UsageError("missing value for " + a);
+            if (i + 1 >= argc) throw BadCommandLine{"missing value for " + a};
             return argv[++i];
         };
-        if (a == "-r" || a == "--rate") rate = parse_int(value(), "--rate");
+        if (a == "-r" || a == "--rate") rate = option_value<int>(value(), "--rate");
         else if (a == "-m" || a == "--mode") {
             const std::string m = value();
             if (m == "exact") opt.precision = kbsrc::Precision::Exact;
             else if (m == "fast") opt.precision = kbsrc::Precision::Fast;
             else if (m == "ld") opt.precision = kbsrc::Precision::LongDouble;
             else if (m == "split") opt.precision = kbsrc::Precision::SplitTC;
-            else throw UsageError("mode must be exact, fast or ld");
+            else throw BadCommandLine{"mode must be exact, fast or ld"};
         } else if (a == "-f" || a == "--format") format = value();
-        else if (a == "-t" || a == "--threads") opt.threads = parse_int(value(), "--threads");
-        else if (a == "--block") opt.block = parse_int(value(), "--block");
-        else if (a == "--len") opt.length = parse_double(value(), "--len");
-        else if (a == "--beta") opt.beta = parse_double(value(), "--beta");
+        else if (a == "-t" || a == "--threads") opt.threads = option_value<int>(value(), "--threads");
+        else if (a == "--block") opt.block = option_value<int>(value(), "--block");
+        else if (a == "--len") opt.length = option_value<double>(value(), "--len");
+        else if (a == "--beta") opt.beta = option_value<double>(value(), "--beta");
         else if (a == "--dither") dither = true;
         else if (a == "--no-lpc") opt.lpc_edges = false;
         else if (a == "-v" || a == "--verbose") verbose = true;
         else if (a == "-h" || a == "--help") { help(); return 0; }
         else if (a == "--version") { std::printf("kbsrc %s\n", kbsrc::version()); return 0; }
-        else if (a.size() > 1 && a[0] == '-') throw UsageError("unknown option " + a);
+        else if (a.size() > 1 && a[0] == '-') throw BadCommandLine{"unknown option " + a};
         else if (in_path.empty()) in_path = a;
         else if (out_path.empty()) out_path = a;
-        else throw UsageError("too many arguments");
+        else throw BadCommandLine{"too many arguments"};
     }
-    if (in_path.empty() || out_path.empty()) throw UsageError("expected input and output paths");
-    if (rate < 1 || rate > 10000000) throw UsageError("--rate must be between 1 and 10000000");
-    if (format != "f64" && format != "f32" && format != "s32" && format != "s24" && format != "s16")
-        throw UsageError("format must be f64, f32, s32, s24 or s16");
+    if (in_path.empty() || out_path.empty()) throw BadCommandLine{"expected input and output paths"};
+    if (rate < 1 || rate > 10000000) throw BadCommandLine{"--rate must be between 1 and 10000000"};
+    static const char* const kFormats[] = {"f64", "f32", "s32", "s24", "s16"};
+    if (std::find(std::begin(kFormats), std::end(kFormats), format) == std::end(kFormats))
+        throw BadCommandLine{"format must be f64, f32, s32, s24 or s16"};
 
-    const double t0 = now();
+    const double t0 = seconds_now();
     kbsrc::warm_up();  // the GPU starts while the file is read
     kbsrc::io::Audio a = kbsrc::io::read_wav_raw(in_path.c_str());  // decoded on the GPU while converting
     if (a.rate > 10000000) throw std::runtime_error("input sample rate above 10000000 Hz");
     kbsrc::io::check_wav_output(a.ch, rate, format);  // fail before converting
-    const double t1 = now();
+    const double t1 = seconds_now();
     kbsrc::Stats st;
     long long clipped = 0, nout = 0;
     double t2, t3;
     if (a.rate == rate) {  // equal rates: the host copy and the host writer
         kbsrc::io::decode_wav(a);
         auto y = kbsrc::resample(a.d.data(), a.frames, a.ch, a.rate, rate, opt, &st);
-        t2 = now();
+        t2 = seconds_now();
         nout = y.empty() ? 0 : (long long)y[0].size();
         kbsrc::io::write_wav(out_path.c_str(), y, a.ch, nout, rate, format, dither, clipped);
     } else {  // the input decode, the conversion and the output step (scale, dither, round, clip) on the GPU
         const auto data = kbsrc::resample_wav_pcm(a.bytes(), a.sample_format.c_str(), a.frames, a.ch, a.rate,
                                                   rate, format.c_str(), dither, clipped, opt, &st);
-        t2 = now();
+        t2 = seconds_now();
         const long long bps = format == "f64" ? 8 : format == "s24" ? 3 : format == "s16" ? 2 : 4;
         nout = (long long)data.size() / (a.ch * bps);
         kbsrc::io::write_wav_data(out_path.c_str(), a.ch, nout, rate, format, data.data(), data.size());
     }
-    t3 = now();
+    t3 = seconds_now();
     if (clipped) std::fprintf(stderr, "kbsrc: warning: %lld samples clipped\n", clipped);
     if (verbose) {
         std::fprintf(stderr, "%d Hz -> %d Hz, %d ch, %lld -> %lld frames\n", a.rate, rate, a.ch, a.frames, nout);
@@ -142,17 +162,21 @@ int run(int argc, char** argv) {
 
 }  // namespace
 
+// Exit status 0 on success, 2 for a command line the tool cannot act on, 1 for any failure while converting; the
+// reason goes to stderr after "kbsrc: " and no output file is left behind.
 int main(int argc, char** argv) {
+    std::string reason;
+    int status = 1;
     try {
         return run(argc, argv);
-    } catch (const UsageError& e) {
-        std::fprintf(stderr, "kbsrc: %s (see --help)\n", e.what());
-        return 2;
+    } catch (const BadCommandLine& e) {
+        reason = e.text + " (see --help)";
+        status = 2;
     } catch (const std::bad_alloc&) {
-        std::fprintf(stderr, "kbsrc: out of memory\n");
-        return 1;
+        reason = "out of memory";
     } catch (const std::exception& e) {
-        std::fprintf(stderr, "kbsrc: %s\n", e.what());
-        return 1;
+        reason = e.what();
     }
+    std::fprintf(stderr, "kbsrc: %s\n", reason.c_str());
+    return status;
 }
