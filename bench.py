@@ -12,8 +12,9 @@ block loop of that conversion (every (channel, block) task), output byte-identic
   --impl reference: the reference's own engine (HongYue1/KBSRC built from source, oracle/_ref) on the host
          cores, its Stats::process_seconds (the block loop run_engine) per conversion
 
-Multi-GPU (torchrun): every rank converts its own file of the workload (independent conversions, no
-collective on the data path; weak scaling). Timing is the max over ranks.
+Multi-GPU (torchrun, N ranks): one conversion of N times the workload's length, split into N contiguous block
+ranges (kbsrc_gpu_shard_plan); rank k holds only share k's input span (its blocks' inputs, halo included) and output
+range on its GPU. No collective on the data path (the only one is the timing max); weak scaling.
 """
 import argparse
 import json
@@ -37,6 +38,8 @@ WORKLOADS = {
     "c2_split": dict(seed=2, seconds=180, rate_in=96000, rate_out=44100, channels=2, mode="split"),
     "c1_exact": dict(seed=1, seconds=10, rate_in=96000, rate_out=44100, channels=2, mode="exact"),
     "c3_exact": dict(sweep=True, seconds=60, rate_in=44100, rate_out=48000, channels=2, mode="exact"),
+    # the split-precision form on the 60 s stereo 44.1k -> 48k log sweep (upsampling: periodic spectrum extension)
+    "c3_split": dict(sweep=True, seconds=60, rate_in=44100, rate_out=48000, channels=2, mode="split"),
     # large multichannel, long kernel: 600 s 8 ch 192k -> 44.1k from 24-bit PCM, --len 1.0 --beta 60
     "c5_exact": dict(pcm24=True, seed=4, seconds=600, rate_in=192000, rate_out=44100, channels=8, mode="exact",
                      length=1.0, beta=60.0),
@@ -50,24 +53,14 @@ METRIC = "out Msamples/s 96k->44.1k exact (180 s stereo f64, byte-identical to t
 METRIC_SPLIT = ("out Msamples/s 96k->44.1k split-precision tensor-core form (180 s stereo f64; error against the "
                 "exact output and throughput against the plain exact GPU engine stated)")
 METRIC_OF = {
+    "c3_split": "out Msamples/s 44.1k->48k split-precision tensor-core form (60 s stereo log sweep 20 Hz-20 kHz at "
+                "0.5; error against the exact output and throughput against the plain exact GPU engine stated)",
     "c5_exact": "out Msamples/s 192k->44.1k exact (600 s 8-channel 24-bit PCM, --len 1.0 --beta 60, byte-identical "
                 "to the reference)",
     "c5_split": "out Msamples/s 192k->44.1k split-precision tensor-core form (600 s 8-channel 24-bit PCM, --len 1.0 "
                 "--beta 60; error against the exact output and throughput against the plain exact GPU engine stated)",
 }
 TENSOR_INT8_PEAK_TOPS = 4500.0  # nominal dense int8 of B200; no measured int8 figure exists for this pool
-
-
-def error_stats(y, ref):
-    """Max and RMS of |y - ref|: absolute (and in dB of full scale 1.0), and in float64 ULPs of each ref sample
-    (samples below 2^-10 of the peak left out of the ULP figures)."""
-    d = np.abs(y - ref)
-    mx, rms = float(d.max(initial=0.0)), float(np.sqrt(np.mean(d * d))) if d.size else 0.0
-    big = np.abs(ref) >= np.abs(ref).max(initial=0.0) * 2.0 ** -10
-    u = d[big] / np.spacing(np.abs(ref[big]))
-    db = lambda v: round(20 * np.log10(v), 2) if v > 0 else None
-    return {"max_abs": mx, "rms_abs": rms, "max_db": db(mx), "rms_db": db(rms),
-            "max_ulps": float(u.max(initial=0.0)), "rms_ulps": float(np.sqrt(np.mean(u * u))) if u.size else 0.0}
 
 
 def make_input(w):
@@ -273,6 +266,59 @@ def cli_e2e(w, x):
     return out
 
 
+def companion_form(mode, x, w, kw, dev, stream, args, ref_out, tune):
+    """Another precision of the same conversion, measured in the same process on the same resident input: device
+    ms per step over args.steps block loops, its output's error against the exact output `ref_out` (the reference's
+    bytes), and its roofline. Used to put the split-precision form and the fast engine beside plain exact."""
+    import torch
+    import kbsrc_b200
+    from kbsrc_b200 import roofline
+    frames, ch = x.shape
+    cv = kbsrc_b200.Conversion(x, w["rate_in"], w["rate_out"], mode=mode, **kw)
+    plan = kbsrc_b200.plan(frames, ch, w["rate_in"], w["rate_out"], mode, **kw)
+    d_in = torch.from_numpy(x).to(dev)
+    d_head = torch.from_numpy(cv.head).to(dev) if cv.head.size else torch.zeros(1, dtype=torch.float64, device=dev)
+    d_tail = torch.from_numpy(cv.tail).to(dev) if cv.tail.size else torch.zeros(1, dtype=torch.float64, device=dev)
+    d_out = torch.empty(ch * max(cv.nout, 1), dtype=torch.float64, device=dev)
+    ptrs = (d_in.data_ptr(), d_head.data_ptr(), d_tail.data_ptr(), d_out.data_ptr())
+    for _ in range(args.warmup):
+        cv.run_device(*ptrs, stream=stream)
+    torch.cuda.synchronize()
+    shapes = cv.tune(*ptrs, stream=stream) if tune and mode != "split" else None
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        cv.run_device(*ptrs, stream=stream)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    y = d_out[:ch * cv.nout].cpu().numpy().reshape(ch, cv.nout)
+    out = {"ms_per_step": round(ms, 4), "value": round(ch * cv.nout / (ms * 1e-3) / 1e6, 3), "unit": "Msamples/s",
+           "error_vs_exact": roofline.error_stats(y, ref_out), "gpu_launches_per_step": cv.engine_info()["launches"]}
+    if shapes is not None:
+        out["tuned_shapes"] = shapes
+    if mode == "fast":
+        work = roofline.conversion_work(plan, ch, False)
+        peaks = fp64_peak()
+        hbm, how = measured_hbm_gbs()
+        t_fp64 = work["ops_total"] / max(peaks.values()) if peaks else None
+        t_hbm = work["compulsory_bytes"] / (hbm * 1e9)
+        roof_ms = max(t_fp64 or 0.0, t_hbm) * 1e3
+        out["roofline"] = {"bound": "max(fp64, hbm)", "roofline_ms_per_step": round(roof_ms, 4),
+                           "fp64_ms": round(t_fp64 * 1e3, 4) if t_fp64 else None, "hbm_ms": round(t_hbm * 1e3, 4),
+                           "frac": round(roof_ms / ms, 4), "fp64_ops_per_step": work["ops_total"],
+                           "compulsory_bytes_per_step": work["compulsory_bytes"],
+                           "note": "roofline time = max(FP64 instructions / measured FP64 issue rate, compulsory "
+                                   "bytes (each block's input span and kept output) / HBM peak (" + how + ")); "
+                                   "frac = roofline time / measured time"}
+    else:
+        tw = roofline.split_work(plan, ch)
+        out["int8_ops_per_step"] = tw["int8_ops_total"]
+        out["tensor_frac_of_nominal"] = round(tw["int8_ops_total"] / (ms * 1e-3) / 1e12 / TENSOR_INT8_PEAK_TOPS, 4)
+    cv.close()
+    return out
+
+
 def product_arm(args, w, world, rank, local, pg):
     import torch
     import kbsrc_b200
@@ -282,15 +328,19 @@ def product_arm(args, w, world, rank, local, pg):
     dev = torch.device("cuda", local)
     exact = w["mode"] == "exact"
     split = w["mode"] == "split"
-    x = make_input(w)
-    frames, ch = x.shape
+    # N ranks: one conversion of N times the workload's length, split into N contiguous block ranges (shares); each
+    # rank holds only its share's input span and output range on its GPU, and no data moves between GPUs
+    x_all = make_input(w if world == 1 else dict(w, seconds=w["seconds"] * world))
+    frames, ch = x_all.shape
     kw = dict(length=w.get("length", 0.2), beta=w.get("beta", 40.0))
-    cv = kbsrc_b200.Conversion(x, w["rate_in"], w["rate_out"], mode=w["mode"], **kw)
+    cv = kbsrc_b200.Conversion(x_all, w["rate_in"], w["rate_out"], mode=w["mode"], share=(rank, world) if world > 1
+                               else None, **kw)
     plan = kbsrc_b200.plan(frames, ch, w["rate_in"], w["rate_out"], w["mode"], **kw)
     work = roofline.conversion_work(plan, ch, exact or split)
     twork = roofline.split_work(plan, ch) if split else None
     info = cv.engine_info()
-    nout = cv.nout
+    nout_all, nout = cv.nout, cv.out_len  # output samples per channel: the whole conversion's, this rank's
+    x = x_all[cv.share["frame0"]:cv.share["frame0"] + cv.share["frames"]] if cv.share else x_all
     d_in = torch.from_numpy(x).to(dev)
     d_head = torch.from_numpy(cv.head).to(dev) if cv.head.size else torch.zeros(1, dtype=torch.float64, device=dev)
     d_tail = torch.from_numpy(cv.tail).to(dev) if cv.tail.size else torch.zeros(1, dtype=torch.float64, device=dev)
@@ -305,6 +355,10 @@ def product_arm(args, w, world, rank, local, pg):
     def step():
         cv.run_device(*ptrs, stream=stream)
 
+    L2_BYTES = 126 << 20
+    resident = x.nbytes + 8 * ch * nout
+    flush = torch.empty((256 << 20) // 8, dtype=torch.float64, device=dev) if resident < 2 * L2_BYTES else None
+
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
@@ -315,15 +369,26 @@ def product_arm(args, w, world, rank, local, pg):
     phys = vis[local] if local < len(vis) and vis[local].strip().isdigit() else str(local)
     sampler = ClockSampler(int(phys))
     with sampler:
-        # value: K back-to-back block loops on resident data (inputs 276 MB > L2, so no flush is needed)
+        # value: K block loops on resident data. Inputs larger than L2 run back to back; a smaller input is timed
+        # step by step with a 256 MB write between steps (untimed), so no step starts with its data in L2.
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
-        e0.record()
-        for _ in range(args.steps):
-            step()
-        e1.record()
-        torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1)
+        if flush is None:
+            e0.record()
+            for _ in range(args.steps):
+                step()
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+        else:
+            ms = 0.0
+            for _ in range(args.steps):
+                flush.fill_(1.0)
+                e0.record()
+                step()
+                e1.record()
+                torch.cuda.synchronize()
+                ms += e0.elapsed_time(e1)
         # per-pass device time over K more steps (an event after every launch, same stream)
         pass_ms = {}
         for _ in range(args.steps):
@@ -358,11 +423,16 @@ def product_arm(args, w, world, rank, local, pg):
             torch.cuda.synchronize()
         copy_s = time.perf_counter() - t
         del d_x2
+    h2d_all = int(8 * (x.size + cv.head.size + cv.tail.size))  # this rank's copies per step, summed below
+    d2h_all = int(8 * ch * nout)
     if pg:
         import torch.distributed as dist
         tt = torch.tensor([ms, e2e_s, copy_s], dtype=torch.float64, device=dev)
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         ms, e2e_s, copy_s = tt.tolist()
+        bb = torch.tensor([h2d_all, d2h_all], dtype=torch.float64, device=dev)
+        dist.all_reduce(bb, op=dist.ReduceOp.SUM)
+        h2d_all, d2h_all = (int(v) for v in bb.tolist())
     # byte-identity of what was timed, against the reference's hash for this workload
     got = ho[:ch * nout].numpy().reshape(ch, nout)
     import hashlib
@@ -372,9 +442,9 @@ def product_arm(args, w, world, rank, local, pg):
         with open(os.path.join(ROOT, "tests", "golden", "golden.json")) as f:
             gold = json.load(f)["cases"]
         key = {"c2_exact": "c2_96k_44k1_exact", "c2_fast": "c2_96k_44k1_fast", "c1_exact": "c1_96k_44k1_exact",
-               "c3_exact": "c3_sweep_44k1_48k_exact"}.get(args.workload) if not args.seconds else None
+               "c3_exact": "c3_sweep_44k1_48k_exact"}.get(args.workload) if not args.seconds and world == 1 else None
         golden_sha = gold.get(key, {}).get("sha256")
-        if args.workload == "c5_exact" and not args.seconds:
+        if args.workload == "c5_exact" and not args.seconds and world == 1:
             with open(os.path.join(ROOT, "tests", "golden", "golden_c5.json")) as f:
                 golden_sha = json.load(f)["planar_sha256"]
     except Exception:
@@ -384,7 +454,7 @@ def product_arm(args, w, world, rank, local, pg):
             pg.barrier()
             pg.destroy_process_group()
         return
-    samples = ch * nout * world
+    samples = ch * nout_all  # the whole job's output, summed over the ranks' shares
     value = samples * args.steps / (ms * 1e-3) / 1e6
     e2e = samples * e2e_steps / e2e_s / 1e6
     # roofline of the dominant kernel
@@ -393,7 +463,7 @@ def product_arm(args, w, world, rank, local, pg):
     share = {k: v[0] / sum(a[0] for a in pass_ms.values()) for k, v in pass_ms.items() if v[1]}
     top = max(avg_ms, key=lambda k: pass_ms[k][0])
     waves = max(1, int(round(launches_per_step[top])))
-    tasks_per_launch = work["tasks"] / waves
+    tasks_per_launch = info["tasks"] / waves
     traffic = load_traffic().get(args.workload, {}).get(top)
     if split:
         achieved = twork["int8_ops_per_task"][top] * tasks_per_launch / (avg_ms[top] * 1e-3)
@@ -434,11 +504,20 @@ def product_arm(args, w, world, rank, local, pg):
         extra["tuned_shapes"] = tuned
     if (w.get("pcm24") or not args.no_cpu) and not args.seconds and world == 1 and not split:
         extra["cli_e2e"] = cli_e2e(w, x)  # the tool a user runs, on the workload's file, ours and the reference's
+    if args.workload in ("c2_exact", "c5_exact") and world == 1 and not args.seconds and not args.no_forms:
+        # the metric's other half: the split-precision form (and the fast engine) beside plain exact, same process,
+        # same resident input, errors against the exact output just timed
+        ref_y = got.copy()
+        for mode in ("split", "fast"):
+            f = companion_form(mode, x, w, kw, dev, stream, args, ref_y, args.tune)
+            f["vs_plain_exact"] = round((ms / args.steps) / f["ms_per_step"], 4)
+            extra[mode] = f
     if split:  # the comparison the form exists for: accuracy against exact, throughput against plain exact
         ref = kbsrc_b200.Conversion(x, w["rate_in"], w["rate_out"], mode="exact", **kw)
         fast = kbsrc_b200.Conversion(x, w["rate_in"], w["rate_out"], mode="fast", **kw)
         y_exact, y_fast = ref.run(x), fast.run(x)
-        extra["error_vs_exact"] = {"split": error_stats(got, y_exact), "fast": error_stats(y_fast, y_exact)}
+        extra["error_vs_exact"] = {"split": roofline.error_stats(got, y_exact),
+                                   "fast": roofline.error_stats(y_fast, y_exact)}
         d_out2 = torch.empty_like(d_out)
         p2 = (d_in.data_ptr(), d_head.data_ptr(), d_tail.data_ptr(), d_out2.data_ptr())
         for _ in range(args.warmup):
@@ -461,11 +540,15 @@ def product_arm(args, w, world, rank, local, pg):
         "dtype": "dd (double-double f64 pairs)" if exact else ("int8 tensor-core slices, f64" if split else "f64"),
         "data": "synthetic",
         "config": {"workload": args.workload, **w, "tasks": work["tasks"], "block": plan["nb"],
-                   "fft_points": [plan["Nb"], plan["Mb"]], "l2": f"inputs larger than L2 ({x.nbytes / 1e6:.0f} MB)",
-                   "parallelism": f"independent conversions x{world}"},
-        "e2e": {"value": round(e2e, 3), "unit": "Msamples/s", "h2d_bytes_per_step": int(8 * (x.size + cv.head.size
-                                                                                                 + cv.tail.size)),
-                "d2h_bytes_per_step": int(8 * ch * nout), "path": "kbsrc_gpu_engine_run_host (C ABI), pinned",
+                   "fft_points": [plan["Nb"], plan["Mb"]],
+                   "l2": (f"inputs larger than L2 ({x.nbytes / 1e6:.0f} MB)" if flush is None else
+                          f"input {x.nbytes / 1e6:.0f} MB: L2 flushed (256 MB write) before each step, steps timed "
+                          "one by one"),
+                   "parallelism": ("one GPU" if world == 1 else
+                                   f"{world} block-range shares of one {w['seconds'] * world:g} s conversion, one per "
+                                   "GPU, no inter-GPU data")},
+        "e2e": {"value": round(e2e, 3), "unit": "Msamples/s", "h2d_bytes_per_step": h2d_all,
+                "d2h_bytes_per_step": d2h_all, "path": "kbsrc_gpu_engine_run_host (C ABI), pinned",
                 "copy_floor_ms_per_step": round(copy_s / e2e_steps * 1e3, 3),
                 "frac_of_copy_floor": round(copy_s / e2e_s, 4)},
         "gpu_launches": int(info["launches"] * args.steps),
@@ -617,6 +700,8 @@ def main():
     ap.add_argument("--impl", default="product", choices=["product", "reference"])
     ap.add_argument("--workload", default="c2_exact", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    ap.add_argument("--no-forms", action="store_true",
+                    help="skip the split-precision and fast companions of the exact workloads")
     ap.add_argument("--no-tune", dest="tune", action="store_false",
                     help="skip the autotuner (launch shapes per pass, chosen after warm-up, before timing)")
     ap.add_argument("--seconds", type=float, default=None,

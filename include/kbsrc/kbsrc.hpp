@@ -62,6 +62,14 @@ std::vector<unsigned char> resample_wav_pcm(const void* pcm, const char* sample_
                                             int channels, int rate_in, int rate_out, const char* format, bool dither,
                                             long long& clipped, const Options& options = {}, Stats* stats = nullptr);
 
+// Not in the reference: the same conversion with its block loop split across CUDA devices in contiguous block
+// ranges, one engine and one host thread per device; each device receives only its input span (its blocks' inputs,
+// halo included) and returns its output range, and nothing moves between devices. `devices` lists CUDA device
+// indices (one may appear more than once). Output, exceptions and rounding-mode handling as resample().
+std::vector<std::vector<double>> resample_devices(const double* interleaved, long long frames, int channels,
+                                                  int rate_in, int rate_out, const int* devices, int ndevices,
+                                                  const Options& options = {}, Stats* stats = nullptr);
+
 // Starts the GPU's initialisation (CUDA context, kernel attributes) on a background thread and returns at once.
 // Optional: the first conversion starts it too, overlapped with its host-side LPC and kernel taps; a caller that
 // knows a conversion is coming (a tool about to read its input file) can start it earlier. Not in the reference.

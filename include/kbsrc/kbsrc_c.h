@@ -52,6 +52,23 @@ int kbsrc_conversion_info_c(const kbsrc_conversion* cv, long long* nout, long lo
                             const double** tail, struct kbsrc_gpu_engine** engine, kbsrc_stats_c* stats);
 void kbsrc_conversion_free_c(kbsrc_conversion* cv);
 
+/* Multi-GPU (not in the reference): the block loop split into contiguous block ranges, one per device
+ * (kbsrc_gpu_shard_plan in include/kbsrc_gpu.h); each device receives only its input span and returns its output
+ * range, nothing moves between devices, and the output equals kbsrc_resample_c's.
+ * kbsrc_resample_devices_c: the whole conversion over devices[0..ndevices) (a device may appear more than once),
+ *   one host thread per share; arguments and return values as kbsrc_resample_c.
+ * kbsrc_prepare_share_c: a conversion whose engine runs share `index` of `count` on the calling thread's current
+ *   device (one process per GPU). kbsrc_conversion_run_c then takes the whole interleaved input and writes that
+ *   share's output, channels * share.nout doubles; kbsrc_conversion_share_c returns the share (blocks, input
+ *   frames, output samples) as six long longs: blk0 blk1 frame0 frames out0 nout (all zero for equal rates). */
+long long kbsrc_resample_devices_c(const double* in, long long frames, int channels, int rate_in, int rate_out,
+                                   const int* devices, int ndevices, const kbsrc_options_c* opt, double* out,
+                                   long long out_cap, kbsrc_stats_c* stats, char* err, int err_len);
+int kbsrc_prepare_share_c(const double* in, long long frames, int channels, int rate_in, int rate_out,
+                          const kbsrc_options_c* opt, int index, int count, kbsrc_conversion** out, char* err,
+                          int err_len);
+int kbsrc_conversion_share_c(const kbsrc_conversion* cv, long long* share6);
+
 /* Batches: many conversions (files) of any lengths, channel counts and rate pairs, planned together and run
  * on the GPU as one recorded launch sequence (kbsrc_gpu_batch in include/kbsrc_gpu.h); conversions with equal
  * plans share their kernel design and launches. Each output equals that of kbsrc_resample_c for the item. */

@@ -45,6 +45,18 @@ extern "C" {
 
 typedef struct kbsrc_gpu_engine kbsrc_gpu_engine;
 
+/* One device's share of a conversion split across GPUs by contiguous block ranges (the reference's tasks are
+ * independent: each reads its own input span and writes a disjoint output range, src/resampler.cpp:48-50,80-84).
+ * All zero: the whole conversion. Otherwise the engine runs blocks [blk0, blk1) of every channel; its input buffer
+ * holds frames [frame0, frame0 + frames) (the blocks' spans, their 2*marg*Q halo included, clipped to the signal;
+ * the LPC edge buffers stay whole) and its output buffer holds output samples [out0, out0 + nout) of each channel,
+ * channel after channel (out[c*nout + i]). kbsrc_gpu_shard_plan computes the shares. */
+typedef struct {
+    long long blk0, blk1;
+    long long frame0, frames;
+    long long out0, nout;
+} kbsrc_gpu_shard;
+
 /* One conversion plan, as computed by the host planner (reference src/resampler.cpp:98-209).
  * Block b of channel c reads staged samples [b*hop*Q, b*hop*Q + nb*Q) where the staged channel holds
  * `lead` zeros/edge samples before input frame 0 (lead = marg*Q + pre), and writes output samples
@@ -66,12 +78,27 @@ typedef struct {
     const double* H;    /* kernel spectrum, H_len (hi, lo) pairs, host memory; copied at create */
     long long H_len;
     int in_format;      /* KBSRC_GPU_IN_*: the input's sample format (0, float64, when zero-initialised) */
+    kbsrc_gpu_shard shard; /* this engine's share of a multi-GPU conversion (zero-initialised: all of it) */
 } kbsrc_gpu_desc;
+
+/* Splits the conversion `d` (its shard ignored) into `count` shares of contiguous block ranges, as even as the
+ * block count allows: share k gets blocks [nblk*k/count, nblk*(k+1)/count), the input frames those blocks read and
+ * the output samples they write; the output ranges partition [0, nout) in order (the last share also owns samples
+ * past the last block, which are zero). Host arithmetic only, no device needed. Run share k with
+ * kbsrc_gpu_engine_create on a descriptor whose `shard` is shards[k], passing that share's input span (interleaved
+ * frames from frame0) and an output buffer of channels * shards[k].nout samples. No data crosses between devices.
+ * Not in the reference (its block loop runs on one host). */
+int kbsrc_gpu_shard_plan(const kbsrc_gpu_desc* d, int count, kbsrc_gpu_shard* shards);
 
 /* Initialises the current CUDA device for the engine (context, kernel attributes). Optional: the first engine
  * or spectrum call does it otherwise. A caller may run it on another thread while it does host work, since
  * creating a CUDA context takes a good fraction of a second. Not in the reference (no GPU). */
 int kbsrc_gpu_init(void);
+
+/* Makes `device` (a CUDA device index) the calling thread's current device: engines, batches and spectra the
+ * thread creates afterwards live there. For multi-GPU callers that run one host thread per device. Not in the
+ * reference (no GPU). */
+int kbsrc_gpu_use_device(int device);
 
 /* Creates an engine on the current CUDA device: FFT plans, twiddle tables and the kernel spectrum on the
  * device. Replaces the set-up half of run_engine (src/resampler.cpp:38-40). */
@@ -82,12 +109,15 @@ int kbsrc_gpu_engine_create(const kbsrc_gpu_desc* desc, kbsrc_gpu_engine** out);
  *   head  channels * edge_len doubles: head[c*edge_len + i] is the sample i+1 frames before frame 0
  *   tail  channels * edge_len doubles: tail[c*edge_len + i] is the sample i frames after the last frame
  *   out   planar output, channels * nout doubles (out[c*nout + i])
- * head/tail may be NULL when edge_len is 0. Replaces the block loop of run_engine (src/resampler.cpp:41-87). */
+ * head/tail may be NULL when edge_len is 0. An engine created for a share (desc.shard) reads `in` as that share's
+ * span, shard.frames * channels doubles from frame shard.frame0, and writes channels * shard.nout samples to `out`
+ * (out[c*shard.nout + i] is output sample shard.out0 + i). Replaces the block loop of run_engine
+ * (src/resampler.cpp:41-87). */
 int kbsrc_gpu_engine_run_host(kbsrc_gpu_engine* e, const double* in, const double* head, const double* tail,
                               double* out);
 
-/* Same with device buffers, asynchronous on `stream` (a cudaStream_t; NULL = the engine's own stream).
- * The caller keeps the buffers alive until the stream reaches this point. */
+/* Same with device buffers (a share's span and output range as above), asynchronous on `stream` (a cudaStream_t;
+ * NULL = the engine's own stream). The caller keeps the buffers alive until the stream reaches this point. */
 int kbsrc_gpu_engine_run_device(kbsrc_gpu_engine* e, const double* d_in, const double* d_head,
                                 const double* d_tail, double* d_out, void* stream);
 
@@ -103,7 +133,8 @@ int kbsrc_gpu_engine_run_device_timed(kbsrc_gpu_engine* e, const double* d_in, c
  * when `dither` (two uniform(-0.5, 0.5) draws per sample from std::mt19937_64 seeded 12345, frame-major order,
  * generated on the GPU), rounded to nearest, clipped; *clipped receives the number of clipped samples.
  * kbsrc_gpu_engine_run_host_packed: the block loop on host input followed by the packing; out_bytes is
- *   host memory of channels * nout * bytes-per-sample.
+ *   host memory of channels * nout * bytes-per-sample (whole conversions only: a share returns
+ *   KBSRC_GPU_E_UNSUPPORTED, since the dither stream runs from the file's first sample).
  * kbsrc_gpu_pack: packs planar device samples (ch x frames, row stride `stride`) into device memory d_out on
  *   `stream`, synchronous. */
 int kbsrc_gpu_engine_run_host_packed(kbsrc_gpu_engine* e, const double* in, const double* head,

@@ -49,6 +49,15 @@ class BatchItem(ctypes.Structure):
                 ("rate_out", ctypes.c_int)]
 
 
+class GpuShard(ctypes.Structure):
+    """kbsrc_gpu_shard (include/kbsrc_gpu.h): one device's share of a conversion."""
+    _fields_ = [("blk0", ctypes.c_longlong), ("blk1", ctypes.c_longlong), ("frame0", ctypes.c_longlong),
+                ("frames", ctypes.c_longlong), ("out0", ctypes.c_longlong), ("nout", ctypes.c_longlong)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class GpuDesc(ctypes.Structure):
     """kbsrc_gpu_desc (include/kbsrc_gpu.h)."""
     _fields_ = [("precision", ctypes.c_int), ("channels", ctypes.c_int), ("P", ctypes.c_longlong),
@@ -56,7 +65,7 @@ class GpuDesc(ctypes.Structure):
                 ("lead", ctypes.c_longlong), ("o", ctypes.c_longlong), ("frames", ctypes.c_longlong),
                 ("nout", ctypes.c_longlong), ("up", ctypes.c_int), ("Jg", ctypes.c_int),
                 ("edge_len", ctypes.c_longlong), ("H", _dp), ("H_len", ctypes.c_longlong),
-                ("in_format", ctypes.c_int)]
+                ("in_format", ctypes.c_int), ("shard", GpuShard)]
 
 
 # Every symbol the C headers declare: (library, name, restype, argtypes)
@@ -89,6 +98,8 @@ GPU_SYMBOLS = {
     "kbsrc_gpu_engine_tune": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                              ctypes.c_void_p, ctypes.c_void_p, _P(ctypes.c_int)]),
     "kbsrc_gpu_init": (ctypes.c_int, []),
+    "kbsrc_gpu_shard_plan": (ctypes.c_int, [_P(GpuDesc), ctypes.c_int, _P(GpuShard)]),
+    "kbsrc_gpu_use_device": (ctypes.c_int, [ctypes.c_int]),
 }
 HOST_SYMBOLS = {
     "kbsrc_output_frames": (ctypes.c_longlong, [ctypes.c_longlong, ctypes.c_int, ctypes.c_int]),
@@ -115,6 +126,13 @@ HOST_SYMBOLS = {
     "kbsrc_kernel_taps_c": (ctypes.c_int, [ctypes.c_int, ctypes.c_longlong, ctypes.c_longlong, ctypes.c_double,
                                            ctypes.c_int, _dp]),
     "kbsrc_burg_c": (ctypes.c_int, [_dp, ctypes.c_longlong, ctypes.c_longlong, _dp]),
+    "kbsrc_resample_devices_c": (ctypes.c_longlong, [_dp, ctypes.c_longlong, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                     _P(ctypes.c_int), ctypes.c_int, _P(Options), _dp,
+                                                     ctypes.c_longlong, _P(Stats), ctypes.c_char_p, ctypes.c_int]),
+    "kbsrc_prepare_share_c": (ctypes.c_int, [_dp, ctypes.c_longlong, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                             _P(Options), ctypes.c_int, ctypes.c_int, _P(ctypes.c_void_p),
+                                             ctypes.c_char_p, ctypes.c_int]),
+    "kbsrc_conversion_share_c": (ctypes.c_int, [ctypes.c_void_p, _lp]),
 }
 PLAN_KEYS = ["P", "Q", "taps", "nb", "marg", "hop", "nblk", "Nb", "Mb", "pre", "o", "E", "lead", "general", "up",
              "nout"]
@@ -197,9 +215,15 @@ def resample(x, rate_in, rate_out, mode="exact", length=0.2, beta=40.0, block=0,
 
 class Conversion:
     """A planned conversion (kbsrc_prepare_c): plan, LPC edges, kernel spectrum and GPU engine, built once for
-    input of one shape and run many times."""
+    input of one shape and run many times.
 
-    def __init__(self, x, rate_in, rate_out, mode="exact", length=0.2, beta=40.0, block=0, lpc=True, threads=0):
+    share=(index, count): the engine runs only share `index` of the conversion split into `count` contiguous block
+    ranges (kbsrc_prepare_share_c, one process per GPU); `self.share` then describes it (blocks, input frames
+    [frame0, frame0 + frames) and output samples [out0, out0 + nout)), run() returns that share's output, and the
+    device buffers of run_device() hold the share's input span and output range only."""
+
+    def __init__(self, x, rate_in, rate_out, mode="exact", length=0.2, beta=40.0, block=0, lpc=True, threads=0,
+                 share=None):
         x = np.ascontiguousarray(x, dtype=np.float64)
         if x.ndim == 1:
             x = x[:, None]
@@ -207,8 +231,13 @@ class Conversion:
         self._h = ctypes.c_void_p()
         err = ctypes.create_string_buffer(512)
         opt = _options(mode, length, beta, block, lpc, threads)
-        r = host_lib().kbsrc_prepare_c(_ptr(x), self.frames, self.channels, rate_in, rate_out, ctypes.byref(opt),
-                                       ctypes.byref(self._h), err, 512)
+        if share is None:
+            r = host_lib().kbsrc_prepare_c(_ptr(x), self.frames, self.channels, rate_in, rate_out, ctypes.byref(opt),
+                                           ctypes.byref(self._h), err, 512)
+        else:
+            r = host_lib().kbsrc_prepare_share_c(_ptr(x), self.frames, self.channels, rate_in, rate_out,
+                                                 ctypes.byref(opt), int(share[0]), int(share[1]),
+                                                 ctypes.byref(self._h), err, 512)
         if r == -1:
             raise ValueError(err.value.decode())
         if r < 0:
@@ -224,16 +253,28 @@ class Conversion:
         self.head = np.ctypeslib.as_array(head, (n,)).copy() if n else np.zeros(0)
         self.tail = np.ctypeslib.as_array(tail, (n,)).copy() if n else np.zeros(0)
         self.stats = st.as_dict()
+        self.share = None
+        if share is not None:
+            v = np.zeros(6, dtype=np.int64)
+            host_lib().kbsrc_conversion_share_c(self._h, v.ctypes.data_as(_lp))
+            self.share = dict(zip(["blk0", "blk1", "frame0", "frames", "out0", "nout"], v.tolist()))
+
+    @property
+    def out_len(self):
+        """Output samples per channel that run() returns: nout, or the share's."""
+        return self.share["nout"] if self.share and self.share["blk1"] else self.nout
 
     def run(self, x, out=None):
-        """Runs on interleaved input x (frames, channels) host memory; returns planar (channels, nout)."""
+        """Runs on interleaved input x (frames, channels) host memory (the whole input, also for a share); returns
+        planar (channels, out_len)."""
         x = np.ascontiguousarray(x, dtype=np.float64)
+        n = self.out_len
         if out is None:
-            out = np.zeros((self.channels, max(self.nout, 1)))
+            out = np.zeros((self.channels, max(n, 1)))
         err = ctypes.create_string_buffer(512)
         if host_lib().kbsrc_conversion_run_c(self._h, _ptr(x), _ptr(out), err, 512):
             raise RuntimeError(err.value.decode())
-        return out[:, :self.nout]
+        return out[:, :n]
 
     def engine_info(self):
         t, l, b = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_longlong()
@@ -354,6 +395,57 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+def resample_devices(x, rate_in, rate_out, devices, mode="exact", length=0.2, beta=40.0, block=0, lpc=True, threads=0,
+                     stats=None):
+    """resample() with the block loop split across CUDA devices (kbsrc_resample_devices_c): contiguous block ranges,
+    one engine per device, nothing exchanged between devices; the same output as resample()."""
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    if x.ndim == 1:
+        x = x[:, None]
+    frames, ch = x.shape
+    n = output_frames(frames, rate_in, rate_out)
+    if n < 0:
+        raise ValueError("sample rates must be positive" if rate_in < 1 or rate_out < 1 else "input too long")
+    out = np.zeros((ch, max(n, 1)))
+    devs = (ctypes.c_int * len(devices))(*devices)
+    st = Stats()
+    err = ctypes.create_string_buffer(512)
+    opt = _options(mode, length, beta, block, lpc, threads)
+    r = host_lib().kbsrc_resample_devices_c(_ptr(x), frames, ch, rate_in, rate_out, devs, len(devices),
+                                            ctypes.byref(opt), _ptr(out), out.shape[1], ctypes.byref(st), err, 512)
+    if r == -1:
+        raise ValueError(err.value.decode())
+    if r < 0:
+        raise RuntimeError(err.value.decode())
+    if stats is not None:
+        stats.update(st.as_dict())
+    return out[:, :r]
+
+
+def shard_plan(frames, channels, rate_in, rate_out, count, mode="exact", length=0.2, beta=40.0, block=0):
+    """The shares of a conversion split into `count` contiguous block ranges (kbsrc_gpu_shard_plan), from the host
+    plan alone: a list of dicts blk0, blk1, frame0, frames, out0, nout. No GPU needed."""
+    p = plan(frames, channels, rate_in, rate_out, mode, length, beta, block)
+    if p["copy"]:
+        raise ValueError("equal rates: no block loop to split")
+    d = GpuDesc()
+    d.precision = {"fast": 0, "exact": 1, "ld": 2, "split": 3}[mode]
+    d.channels, d.P, d.Q, d.nb, d.marg, d.nblk = channels, p["P"], p["Q"], p["nb"], p["marg"], p["nblk"]
+    d.lead, d.o, d.frames, d.nout, d.up = p["lead"], p["o"], frames, p["nout"], p["up"]
+    n_spec = (p["Mb"] if p["up"] else p["Nb"]) // 2 + 1
+    H = np.zeros((n_spec, 2))  # the shares do not depend on the spectrum's values
+    d.H, d.H_len = _ptr(H), n_spec
+    if p["general"]:
+        d.Jg = 1
+        H = np.zeros((max(p["Nb"], p["Mb"]) * 2, 2))
+        d.H, d.H_len = _ptr(H), H.shape[0]
+    out = (GpuShard * count)()
+    rc = gpu_lib().kbsrc_gpu_shard_plan(ctypes.byref(d), count, out)
+    if rc:
+        raise ValueError(gpu_error())
+    return [s.as_dict() for s in out]
 
 
 def plan(frames, channels, rate_in, rate_out, mode="exact", length=0.2, beta=40.0, block=0):

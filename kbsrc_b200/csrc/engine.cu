@@ -64,14 +64,17 @@ int fail(int code, const std::string& msg) {
 // One conversion's buffers and placement; a single engine runs one, a batch many.
 // The staged channel of the reference (resampler.cpp:168-186) is read without being materialised: zeros, the
 // LPC head, the interleaved input, the LPC tail, zeros; frame t of the signal is staged sample t + lead.
+// A multi-GPU share holds only part of the input and of the output: `in` starts at frame f0, and `out` holds
+// output samples [d0, d0 + ostride) of each channel (a whole conversion: f0 = d0 = 0, ostride = nout).
 struct Item {
-    const void* in;      // interleaved input, frames x ch, samples in format `fmt` (KBSRC_GPU_IN_*)
+    const void* in;      // interleaved input, frames [f0, ...) x ch, samples in format `fmt` (KBSRC_GPU_IN_*)
     const double* head;  // ch x edge: head[c*edge + i] is frame -1-i
     const double* tail;  // ch x edge: tail[c*edge + i] is frame frames+i
-    double* out;         // planar output, ch x nout
+    double* out;         // planar output, ch x ostride: out[c*ostride + (d - d0)] is output sample d
     long long frames, edge, lead, nout, o;
     int ch;
     int fmt;
+    long long f0, d0, ostride;
 };
 
 // Which conversion, channel and block a task is.
@@ -114,7 +117,7 @@ __device__ __forceinline__ double input_at(const Item& s, long long i) {
 }
 
 __device__ __forceinline__ double signal_at(const Item& s, int c, long long t) {
-    if (t >= 0 && t < s.frames) return input_at(s, t * s.ch + c);
+    if (t >= 0 && t < s.frames) return input_at(s, (t - s.f0) * s.ch + c);
     if (t < 0 && t >= -s.edge) return __ldg(s.head + c * s.edge + (-1 - t));
     if (t >= s.frames && t < s.frames + s.edge) return __ldg(s.tail + c * s.edge + (t - s.frames));
     return 0.0;
@@ -124,8 +127,8 @@ __device__ __forceinline__ double signal_at(const Item& s, int c, long long t) {
 __device__ __forceinline__ void emit(const Work& w, const Item& it, int c, long long b, long long e, double v) {
     const long long k = e - w.margP;
     if (k < 0 || k >= w.hopP) return;
-    const long long d = b * w.hopP + k - it.o;
-    if (d >= 0 && d < it.nout) it.out[c * it.nout + d] = v;
+    const long long d = b * w.hopP + k - it.o, j = d - it.d0;
+    if (d >= 0 && d < it.nout && j >= 0 && j < it.ostride) it.out[c * it.ostride + j] = v;
 }
 
 enum Src { kSrcSignal = 0, kSrcComplex = 1, kSrcDDReal = 2 };
@@ -178,8 +181,8 @@ __device__ __forceinline__ CxR<Ar> load_input(const PassParams<Ar>& P, const Tas
         const long long t = ts.g0 + 2 * i;
         double x0, x1;
         if (ts.interior) {
-            x0 = input_at(ts.it, t * ts.it.ch + ts.c);
-            x1 = input_at(ts.it, (t + 1) * ts.it.ch + ts.c);
+            x0 = input_at(ts.it, (t - ts.it.f0) * ts.it.ch + ts.c);
+            x1 = input_at(ts.it, (t + 1 - ts.it.f0) * ts.it.ch + ts.c);
         } else {
             x0 = signal_at(ts.it, ts.c, t);
             x1 = signal_at(ts.it, ts.c, t + 1);
@@ -1235,6 +1238,7 @@ struct Stager {
 struct kbsrc_gpu_engine : PlanCore {
     int device = 0;
     long long tasks = 0, wave = 0, stride = 0, launches = 0;
+    long long t_begin = 0, t_end = 0;  // the share's tasks: blocks [blk0, blk1) x channels, task = b*ch + c
     cudaStream_t stream = nullptr;
     cudaStream_t copy_in = nullptr, copy_out = nullptr;  // run_host's copy pipeline
     cudaEvent_t ev_in[2] = {}, ev_done[2] = {};
@@ -1601,10 +1605,18 @@ int enqueue_any(const PlanCore& pc, const Work& work, long long t_begin, long lo
     return enqueue_plan<ArF64, ArF64>(pc, work, t_begin, t_end, a, b, stride, wave, st, tr);
 }
 
+// The share of a descriptor that an engine runs: its own shard, or the whole conversion when the shard is zero.
+kbsrc_gpu_shard effective_shard(const kbsrc_gpu_desc& d) {
+    if (d.shard.blk1 > 0) return d.shard;
+    return kbsrc_gpu_shard{0, d.nblk, 0, d.frames, 0, d.nout};
+}
+
 Work single_work(const PlanCore& pc, const double* in, const double* head, const double* tail, double* out) {
     const kbsrc_gpu_desc& d = pc.d;
+    const kbsrc_gpu_shard sh = effective_shard(d);
     Work w{};
-    w.item0 = Item{in, head, tail, out, d.frames, d.edge_len, d.lead, d.nout, d.o, d.channels, d.in_format};
+    w.item0 = Item{in, head, tail, out, d.frames, d.edge_len, d.lead, d.nout, d.o, d.channels, d.in_format,
+                   sh.frame0, sh.out0, sh.nout};
     w.hopQ = (long long)pc.hop * d.Q;
     w.hopP = (long long)pc.hop * d.P;
     w.margP = (long long)d.marg * d.P;
@@ -1641,6 +1653,23 @@ int check_tc(const PlanCore& pc) {
     return fail(KBSRC_GPU_E_CUDA, "split-precision form: a tensor-core stage did not complete");
 }
 
+// The input frames blocks [b0, b1) read (staged samples [b*hop*Q, b*hop*Q + nb*Q) of each block, frame = staged
+// sample - lead, clipped to the signal) and the output samples they write ([b*hop*P - o, (b+1)*hop*P - o) clipped
+// to [0, nout)).
+int shard_span(const kbsrc_gpu_desc& d, long long b0, long long b1, kbsrc_gpu_shard& s) {
+    const long long hop = d.nb - 2LL * d.marg, hopQ = hop * d.Q, hopP = hop * d.P, Nb = (long long)d.nb * d.Q;
+    s.blk0 = b0;
+    s.blk1 = b1;
+    const long long f0 = std::max(0LL, b0 * hopQ - d.lead), f1 = std::min(d.frames, (b1 - 1) * hopQ + Nb - d.lead);
+    s.frame0 = std::min(f0, d.frames);
+    s.frames = std::max(0LL, f1 - s.frame0);
+    const long long o0 = std::min(d.nout, std::max(0LL, b0 * hopP - d.o)),
+                    o1 = std::min(d.nout, std::max(0LL, b1 * hopP - d.o));
+    s.out0 = o0;
+    s.nout = std::max(0LL, o1 - o0);
+    return KBSRC_GPU_OK;
+}
+
 int check_desc(const kbsrc_gpu_desc* d) {
     if (!d) return fail(KBSRC_GPU_E_ARG, "null descriptor");
     if (d->precision != KBSRC_GPU_FAST && d->precision != KBSRC_GPU_EXACT && d->precision != KBSRC_GPU_LD &&
@@ -1654,6 +1683,18 @@ int check_desc(const kbsrc_gpu_desc* d) {
     if ((long long)d->nb * std::max(d->P, d->Q) > (1LL << 30)) return fail(KBSRC_GPU_E_ARG, "transform too large");
     const long long need = d->Jg ? (long long)d->Jg + 1 : (d->up ? d->nb * d->P / 2 + 1 : d->nb * d->Q / 2 + 1);
     if (!d->H || d->H_len < need) return fail(KBSRC_GPU_E_ARG, "kernel spectrum too short");
+    const kbsrc_gpu_shard& s = d->shard;
+    if (s.blk0 || s.blk1 || s.frame0 || s.frames || s.out0 || s.nout) {
+        // a share must hold every input frame its blocks read and every output sample they write: the kernels
+        // index its buffers relative to frame0 and out0 without further checks on the input side
+        kbsrc_gpu_shard want;
+        if (s.blk0 < 0 || s.blk1 <= s.blk0 || s.blk1 > d->nblk || s.frame0 < 0 || s.frames < 0 ||
+            s.frame0 + s.frames > d->frames || s.out0 < 0 || s.nout < 0 || s.out0 + s.nout > d->nout ||
+            shard_span(*d, s.blk0, s.blk1, want) != KBSRC_GPU_OK ||
+            (want.frames > 0 && (want.frame0 < s.frame0 || want.frame0 + want.frames > s.frame0 + s.frames)) ||
+            (want.nout > 0 && (want.out0 < s.out0 || want.out0 + want.nout > s.out0 + s.nout)))
+            return fail(KBSRC_GPU_E_ARG, "shard does not hold the input span or output range of its blocks");
+    }
     return KBSRC_GPU_OK;
 }
 
@@ -1721,7 +1762,10 @@ int create_impl(const kbsrc_gpu_desc* desc, kbsrc_gpu_engine** out) {
     KB_CUDA(cudaGetDevice(&e->device));
     KB_CUDA(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
     if ((rc = make_core(desc, *e, e->stream)) != KBSRC_GPU_OK) return rc;
-    e->tasks = (long long)desc->channels * desc->nblk;
+    const kbsrc_gpu_shard sh = effective_shard(*desc);
+    e->t_begin = sh.blk0 * desc->channels;
+    e->t_end = sh.blk1 * desc->channels;
+    e->tasks = e->t_end - e->t_begin;
     e->stride = e->slot();
     const long long budget = (long long)env_int("KBSRC_GPU_WAVE_MB", 4096) << 20;
     const long long per_task = 2 * e->stride * (long long)e->esize();
@@ -1738,15 +1782,16 @@ int create_impl(const kbsrc_gpu_desc* desc, kbsrc_gpu_engine** out) {
 int run_device_impl(kbsrc_gpu_engine* e, const double* in, const double* head, const double* tail, double* out,
                     cudaStream_t st, Trail* trail = nullptr) {
     const kbsrc_gpu_desc& d = e->d;
-    if (d.nout > 0) KB_CUDA(cudaMemsetAsync(out, 0, (size_t)d.nout * d.channels * sizeof(double), st));
-    if (e->tasks == 0 || d.nout == 0) return KBSRC_GPU_OK;
+    const kbsrc_gpu_shard sh = effective_shard(d);
+    if (sh.nout > 0) KB_CUDA(cudaMemsetAsync(out, 0, (size_t)sh.nout * d.channels * sizeof(double), st));
+    if (e->tasks == 0 || sh.nout == 0) return KBSRC_GPU_OK;
     if (d.frames > 0 && !in) return fail(KBSRC_GPU_E_ARG, "null input");
     if (d.edge_len > 0 && (!head || !tail)) return fail(KBSRC_GPU_E_ARG, "null edge buffers");
     Trail none;
     Trail& tr = trail ? *trail : none;
     int rc;
     if ((rc = tr.mark(st, -1)) != KBSRC_GPU_OK) return rc;
-    rc = enqueue_any(*e, single_work(*e, in, head, tail, out), 0, e->tasks, e->bufA.p, e->bufB.p, e->stride,
+    rc = enqueue_any(*e, single_work(*e, in, head, tail, out), e->t_begin, e->t_end, e->bufA.p, e->bufB.p, e->stride,
                      e->wave, st, tr);
     if (rc) return rc;
     e->launches = tr.launches;
@@ -2159,8 +2204,10 @@ bool same_plan(const kbsrc_gpu_desc& a, const kbsrc_gpu_desc& b) {
 int batch_create_impl(const kbsrc_gpu_desc* descs, int count, kbsrc_gpu_batch** out) {
     if (!descs || count < 1) return fail(KBSRC_GPU_E_ARG, "empty batch");
     int rc;
-    for (int i = 0; i < count; i++)
+    for (int i = 0; i < count; i++) {
         if ((rc = check_desc(descs + i)) != KBSRC_GPU_OK) return fail(rc, "conversion " + std::to_string(i) + ": " + g_error);
+        if (descs[i].shard.blk1 > 0) return fail(KBSRC_GPU_E_ARG, "batches run whole conversions (no shards)");
+    }
     if ((rc = require_device()) != KBSRC_GPU_OK) return rc;
     if ((rc = allow_large_smem()) != KBSRC_GPU_OK) return rc;
     auto bp = std::make_unique<kbsrc_gpu_batch>();
@@ -2251,7 +2298,7 @@ int batch_run_device_impl(kbsrc_gpu_batch& b, const double* const* in, const dou
     for (int i = 0; i < count; i++) {
         const kbsrc_gpu_desc& d = b.descs[i];
         b.items_host[i] = Item{in[i], head ? head[i] : nullptr, tail ? tail[i] : nullptr, out[i], d.frames,
-                               d.edge_len, d.lead, d.nout, d.o, d.channels, d.in_format};
+                               d.edge_len, d.lead, d.nout, d.o, d.channels, d.in_format, 0, 0, d.nout};
     }
     if (!b.graph) {
         // record the run once; it reads every pointer from the item table, so it replays for new buffers
@@ -2531,6 +2578,38 @@ int kbsrc_gpu_init(void) {
     }
 }
 
+int kbsrc_gpu_use_device(int device) {
+    int rc = require_device();
+    if (rc) return rc;
+    int n = 0;
+    KB_CUDA(cudaGetDeviceCount(&n));
+    if (device < 0 || device >= n)
+        return fail(KBSRC_GPU_E_ARG, "no CUDA device " + std::to_string(device) + " (" + std::to_string(n) + " present)");
+    KB_CUDA(cudaSetDevice(device));
+    return KBSRC_GPU_OK;
+}
+
+int kbsrc_gpu_shard_plan(const kbsrc_gpu_desc* d, int count, kbsrc_gpu_shard* shards) {
+    if (!d || !shards || count < 1) return fail(KBSRC_GPU_E_ARG, "bad shard plan arguments");
+    kbsrc_gpu_desc whole = *d;
+    whole.shard = kbsrc_gpu_shard{};
+    int rc = check_desc(&whole);
+    if (rc) return rc;
+    if (count > whole.nblk) return fail(KBSRC_GPU_E_ARG, "more shares than blocks");
+    long long next_out = 0;
+    for (int k = 0; k < count; k++) {
+        const long long b0 = whole.nblk * k / count, b1 = whole.nblk * (k + 1) / count;
+        kbsrc_gpu_shard& s = shards[k];
+        shard_span(whole, b0, b1, s);
+        // output ranges partition [0, nout): each share starts where the previous one ended, the last runs to nout
+        const long long end = k == count - 1 ? whole.nout : s.out0 + s.nout;
+        s.out0 = next_out;
+        s.nout = std::max(0LL, end - next_out);
+        next_out = s.out0 + s.nout;
+    }
+    return KBSRC_GPU_OK;
+}
+
 int kbsrc_gpu_engine_create(const kbsrc_gpu_desc* desc, kbsrc_gpu_engine** out) {
     if (!out) return fail(KBSRC_GPU_E_ARG, "null output pointer");
     *out = nullptr;
@@ -2671,12 +2750,13 @@ int kbsrc_gpu_engine_run_host(kbsrc_gpu_engine* e, const double* in, const doubl
                               double* out) {
     if (!e) return fail(KBSRC_GPU_E_ARG, "null engine");
     const kbsrc_gpu_desc& d = e->d;
-    if ((d.frames > 0 && !in) || (d.nout > 0 && !out) || (d.edge_len > 0 && (!head || !tail)))
+    const kbsrc_gpu_shard sh = effective_shard(d);
+    if ((sh.frames > 0 && !in) || (sh.nout > 0 && !out) || (d.edge_len > 0 && (!head || !tail)))
         return fail(KBSRC_GPU_E_ARG, "null buffer");
     try {
         int rc;
-        const size_t nin = (size_t)d.frames * d.channels, ne = (size_t)d.edge_len * d.channels,
-                     no = (size_t)d.nout * d.channels;
+        const size_t nin = (size_t)sh.frames * d.channels, ne = (size_t)d.edge_len * d.channels,
+                     no = (size_t)sh.nout * d.channels;
         if (!e->d_in.p && (rc = e->d_in.alloc(nin * in_bytes(d.in_format))) != KBSRC_GPU_OK) return rc;
         if (!e->d_head.p && (rc = e->d_head.alloc(ne * 8)) != KBSRC_GPU_OK) return rc;
         if (!e->d_tail.p && (rc = e->d_tail.alloc(ne * 8)) != KBSRC_GPU_OK) return rc;
@@ -2691,8 +2771,9 @@ int kbsrc_gpu_engine_run_host(kbsrc_gpu_engine* e, const double* in, const doubl
         }
         // Pipeline by chunks of blocks: the input frames a chunk reads go up while the previous chunk computes,
         // and its output goes down while the next one computes. Tasks are block-major, so a chunk of blocks is a
-        // contiguous task range; every frame is copied once, in order.
-        if (e->tasks == 0 || d.nout == 0) return KBSRC_GPU_OK;
+        // contiguous task range; every frame is copied once, in order. A share's buffers start at its first held
+        // frame (frame0) and output sample (out0).
+        if (e->tasks == 0 || sh.nout == 0) return KBSRC_GPU_OK;
         cudaStream_t cs = e->stream, hs = e->copy_in, ds = e->copy_out;
         const double* dinp = (const double*)e->d_in.p;
         double* dout = (double*)e->d_out.p;
@@ -2701,22 +2782,26 @@ int kbsrc_gpu_engine_run_host(kbsrc_gpu_engine* e, const double* in, const doubl
             KB_CUDA(cudaMemcpyAsync(e->d_head.p, head, ne * 8, cudaMemcpyHostToDevice, hs));
             KB_CUDA(cudaMemcpyAsync(e->d_tail.p, tail, ne * 8, cudaMemcpyHostToDevice, hs));
         }
-        const long long nblk = d.nblk, ch = d.channels, hopQ = (long long)e->hop * d.Q, hopP = (long long)e->hop * d.P;
+        const long long ch = d.channels, hopQ = (long long)e->hop * d.Q, hopP = (long long)e->hop * d.P;
+        const long long nblk = sh.blk1 - sh.blk0, F0 = sh.frame0, F1 = sh.frame0 + sh.frames;
+        const long long O0 = sh.out0, O1 = sh.out0 + sh.nout;
         const long long bps = in_bytes(d.in_format);
         const long long chunks = nout_chunks(e, nblk);
         const bool out_pinned = host_pinned(out);  // pageable output: one staged copy at the end
         const Work w = single_work(*e, dinp, (const double*)e->d_head.p, (const double*)e->d_tail.p, dout);
-        long long copied = 0;  // frames already sent
+        long long copied = F0;  // frames already sent
+        auto send = [&](long long upto) -> int {
+            return copy_h2d(e->stager, static_cast<char*>(e->d_in.p) + (copied - F0) * ch * bps,
+                            reinterpret_cast<const char*>(in) + (copied - F0) * ch * bps,
+                            (size_t)((upto - copied) * ch * bps), hs);
+        };
         Trail tr;
         for (long long k = 0; k < chunks; k++) {
-            const long long b0 = nblk * k / chunks, b1 = nblk * (k + 1) / chunks;
+            const long long b0 = sh.blk0 + nblk * k / chunks, b1 = sh.blk0 + nblk * (k + 1) / chunks;
             if (b0 == b1) continue;
-            const long long f_hi = std::min(d.frames, std::max(0LL, (b1 - 1) * hopQ + e->Nb - d.lead));
+            const long long f_hi = std::min(F1, std::max(F0, (b1 - 1) * hopQ + e->Nb - d.lead));
             if (f_hi > copied) {
-                if ((rc = copy_h2d(e->stager, static_cast<char*>(e->d_in.p) + copied * ch * bps,
-                                   reinterpret_cast<const char*>(in) + copied * ch * bps,
-                                   (size_t)((f_hi - copied) * ch * bps), hs)) != KBSRC_GPU_OK)
-                    return rc;
+                if ((rc = send(f_hi)) != KBSRC_GPU_OK) return rc;
                 copied = f_hi;
             }
             KB_CUDA(cudaEventRecord(e->ev_in[k % 2], hs));
@@ -2726,16 +2811,12 @@ int kbsrc_gpu_engine_run_host(kbsrc_gpu_engine* e, const double* in, const doubl
                 return rc;
             KB_CUDA(cudaEventRecord(e->ev_done[k % 2], cs));
             KB_CUDA(cudaStreamWaitEvent(ds, e->ev_done[k % 2], 0));
-            const long long o0 = std::max(0LL, b0 * hopP - d.o), o1 = k == chunks - 1 ? d.nout
-                                                                                    : std::min(d.nout, b1 * hopP - d.o);
+            const long long o0 = std::max(O0, b0 * hopP - d.o), o1 = k == chunks - 1 ? O1 : std::min(O1, b1 * hopP - d.o);
             if (o1 > o0 && out_pinned)
-                KB_CUDA(cudaMemcpy2DAsync(out + o0, (size_t)d.nout * 8, dout + o0, (size_t)d.nout * 8,
+                KB_CUDA(cudaMemcpy2DAsync(out + (o0 - O0), (size_t)sh.nout * 8, dout + (o0 - O0), (size_t)sh.nout * 8,
                                           (size_t)(o1 - o0) * 8, (size_t)ch, cudaMemcpyDeviceToHost, ds));
         }
-        if (copied < d.frames && nin &&  // frames no block reads (none in a valid plan)
-            (rc = copy_h2d(e->stager, static_cast<char*>(e->d_in.p) + copied * ch * bps,
-                           reinterpret_cast<const char*>(in) + copied * ch * bps,
-                           (size_t)((d.frames - copied) * ch * bps), hs)) != KBSRC_GPU_OK)
+        if (copied < F1 && nin && (rc = send(F1)) != KBSRC_GPU_OK)  // frames no block reads (none in a valid plan)
             return rc;
         e->launches = tr.launches;
         KB_CUDA(cudaGetLastError());
@@ -2755,6 +2836,8 @@ int kbsrc_gpu_engine_run_host_packed(kbsrc_gpu_engine* e, const double* in, cons
     if (!e) return fail(KBSRC_GPU_E_ARG, "null engine");
     const kbsrc_gpu_desc& d = e->d;
     if (format < 0 || format > 4) return fail(KBSRC_GPU_E_ARG, "unknown sample format");
+    if (d.shard.blk1 > 0)  // the dither stream runs from the file's first sample
+        return fail(KBSRC_GPU_E_UNSUPPORTED, "packed output of a multi-GPU share");
     if ((d.frames > 0 && !in) || (d.nout > 0 && !out_bytes) || (d.edge_len > 0 && (!head || !tail)))
         return fail(KBSRC_GPU_E_ARG, "null buffer");
     try {

@@ -276,7 +276,7 @@ struct Conversion {
     std::vector<double> head, tail;  // LPC edges, ch * ext each
     long long ext = 0;
     std::vector<double> H;           // kernel spectrum (hi, lo) pairs
-    kbsrc_gpu_desc desc{};           // the engine's plan (desc.H points into H)
+    kbsrc_gpu_desc desc{};           // the engine's plan (desc.H points into H); desc.shard: its share, if any
     EngineHandle eng;
     double design_seconds = 0;
 };
@@ -481,7 +481,8 @@ void fill_stats(const Conversion& cv, Stats* stats, double process_seconds) {
     stats->stopband = (double)pl.c2 / 2 + pl.fml;
 }
 
-// Runs a prepared conversion on input of its shape; out: planar ch * nout.
+// Runs a prepared conversion on input of its shape (the whole interleaved input); out: planar ch * nout, or for a
+// share ch * shard.nout (its output samples from shard.out0).
 void run_conversion(Conversion& cv, const double* in, double* out) {
     const Plan& pl = cv.pl;
     if (pl.copy) {
@@ -489,7 +490,30 @@ void run_conversion(Conversion& cv, const double* in, double* out) {
             for (long long i = 0; i < cv.frames; i++) out[c * pl.nout + i] = in[i * cv.ch + c];
         return;
     }
-    gpu_check(kbsrc_gpu_engine_run_host(cv.eng.e, in, cv.head.data(), cv.tail.data(), out), "GPU engine");
+    const double* span = in ? in + cv.desc.shard.frame0 * cv.ch : in;
+    gpu_check(kbsrc_gpu_engine_run_host(cv.eng.e, span, cv.head.data(), cv.tail.data(), out), "GPU engine");
+}
+
+// The shares of a prepared (engine-less) conversion over `count` devices: contiguous block ranges.
+std::vector<kbsrc_gpu_shard> plan_shares(const Conversion& cv, int count) {
+    if (count < 1) throw std::invalid_argument("no devices given");
+    const int n = (int)std::min<long long>(count, std::max<long long>(1, cv.pl.nblk));
+    std::vector<kbsrc_gpu_shard> sh((size_t)n);
+    gpu_check(kbsrc_gpu_shard_plan(&cv.desc, n, sh.data()), "shard plan");
+    return sh;
+}
+
+// Plans a conversion and creates the engine of share `index` of `count` on the current device.
+std::unique_ptr<Conversion> prepare_share(const double* in, long long frames, int ch, int rate_in, int rate_out,
+                                          const Options& opt, int index, int count) {
+    auto cv = prepare(in, frames, ch, rate_in, rate_out, opt, false);
+    if (cv->pl.copy) return cv;
+    const std::vector<kbsrc_gpu_shard> sh = plan_shares(*cv, count);
+    if (index < 0 || index >= (int)sh.size()) throw std::invalid_argument("share index out of range");
+    cv->desc.shard = sh[(size_t)index];
+    gpu_ready();
+    gpu_check(kbsrc_gpu_engine_create(&cv->desc, &cv->eng.e), "GPU engine");
+    return cv;
 }
 
 std::vector<std::vector<double>> resample_gpu(const double* in, long long frames, int ch, int rate_in, int rate_out,
@@ -511,6 +535,57 @@ std::vector<std::vector<double>> resample(const double* in, long long frames, in
                                           const Options& opt, Stats* stats) {
     RoundToNearest rn(opt.precision == Precision::Exact || opt.precision == Precision::SplitTC);
     return resample_gpu(in, frames, channels, rate_in, rate_out, opt, stats);
+}
+
+std::vector<std::vector<double>> resample_devices(const double* in, long long frames, int channels, int rate_in,
+                                                  int rate_out, const int* devices, int ndevices, const Options& opt,
+                                                  Stats* stats) {
+    if (!devices || ndevices < 1) throw std::invalid_argument("no devices given");
+    RoundToNearest rn(opt.precision == Precision::Exact || opt.precision == Precision::SplitTC);
+    auto cv = prepare(in, frames, channels, rate_in, rate_out, opt, false);
+    const double t1 = now();
+    const long long nout = cv->pl.nout;
+    std::vector<std::vector<double>> out((size_t)channels, std::vector<double>((size_t)nout));
+    if (cv->pl.copy) {
+        for (int c = 0; c < channels; c++)
+            for (long long i = 0; i < frames; i++) out[c][i] = in[i * channels + c];
+        fill_stats(*cv, stats, now() - t1);
+        return out;
+    }
+    const std::vector<kbsrc_gpu_shard> sh = plan_shares(*cv, ndevices);
+    // one host thread per share: select its device, create its engine, copy its input span up, run its blocks,
+    // copy its output range down into the result; no data moves between devices
+    std::vector<std::string> errors(sh.size());
+    std::vector<int> nomem(sh.size(), 0);
+    std::vector<std::thread> workers;
+    for (size_t k = 0; k < sh.size(); k++)
+        workers.emplace_back([&, k] {
+            try {
+                gpu_check(kbsrc_gpu_use_device(devices[k]), "device");
+                kbsrc_gpu_desc d = cv->desc;
+                d.shard = sh[k];
+                EngineHandle e;
+                gpu_check(kbsrc_gpu_engine_create(&d, &e.e), "GPU engine");
+                std::vector<double> part((size_t)(channels * sh[k].nout));
+                gpu_check(kbsrc_gpu_engine_run_host(e.e, in + sh[k].frame0 * channels, cv->head.data(),
+                                                    cv->tail.data(), part.data()),
+                          "GPU engine");
+                for (int c = 0; c < channels; c++)
+                    std::copy(part.begin() + c * sh[k].nout, part.begin() + (c + 1) * sh[k].nout,
+                              out[c].begin() + sh[k].out0);
+            } catch (const std::bad_alloc&) {
+                nomem[k] = 1;
+            } catch (const std::exception& x) {
+                errors[k] = x.what();
+            }
+        });
+    for (auto& w : workers) w.join();
+    for (size_t k = 0; k < sh.size(); k++) {
+        if (nomem[k]) throw std::bad_alloc();
+        if (!errors[k].empty()) throw std::runtime_error("share " + std::to_string(k) + ": " + errors[k]);
+    }
+    fill_stats(*cv, stats, now() - t1);
+    return out;
 }
 
 std::vector<unsigned char> resample_wav_data(const double* in, long long frames, int channels, int rate_in,
@@ -657,6 +732,62 @@ extern "C" int kbsrc_prepare_c(const double* in, long long frames, int channels,
     } catch (const std::exception& x) {
         return (int)report(x.what(), -3, err, err_len);
     }
+}
+
+extern "C" long long kbsrc_resample_devices_c(const double* in, long long frames, int channels, int rate_in,
+                                              int rate_out, const int* devices, int ndevices,
+                                              const kbsrc_options_c* copt, double* out, long long out_cap,
+                                              kbsrc_stats_c* cst, char* err, int err_len) {
+    try {
+        kbsrc::Stats st;
+        auto y = kbsrc::resample_devices(in, frames, channels, rate_in, rate_out, devices, ndevices,
+                                         options_from_c(copt), &st);
+        const long long n = y.empty() ? 0 : (long long)y[0].size();
+        if (n > out_cap || (n > 0 && !out)) return report("output buffer too small", -2, err, err_len);
+        for (int c = 0; c < channels; c++)
+            if (n) std::memcpy(out + (size_t)c * out_cap, y[c].data(), (size_t)n * sizeof(double));
+        if (cst) {
+            cst->p = st.p; cst->q = st.q; cst->taps = st.taps; cst->block = st.block; cst->threads = st.threads;
+            cst->general_fold = st.general_fold; cst->design_seconds = st.design_seconds;
+            cst->process_seconds = st.process_seconds; cst->passband = st.passband; cst->stopband = st.stopband;
+            cst->isa = st.isa;
+        }
+        return n;
+    } catch (const std::invalid_argument& x) {
+        return report(x.what(), -1, err, err_len);
+    } catch (const std::bad_alloc&) {
+        return report("out of memory", -4, err, err_len);
+    } catch (const std::exception& x) {
+        return report(x.what(), -3, err, err_len);
+    }
+}
+
+extern "C" int kbsrc_prepare_share_c(const double* in, long long frames, int channels, int rate_in, int rate_out,
+                                     const kbsrc_options_c* copt, int index, int count, kbsrc_conversion** out,
+                                     char* err, int err_len) {
+    if (!out) return (int)report("null output pointer", -1, err, err_len);
+    *out = nullptr;
+    try {
+        const kbsrc::Options o = options_from_c(copt);
+        kbsrc::RoundToNearest rn(o.precision == kbsrc::Precision::Exact || o.precision == kbsrc::Precision::SplitTC);
+        *out = reinterpret_cast<kbsrc_conversion*>(
+            kbsrc::prepare_share(in, frames, channels, rate_in, rate_out, o, index, count).release());
+        return 0;
+    } catch (const std::invalid_argument& x) {
+        return (int)report(x.what(), -1, err, err_len);
+    } catch (const std::bad_alloc&) {
+        return (int)report("out of memory", -4, err, err_len);
+    } catch (const std::exception& x) {
+        return (int)report(x.what(), -3, err, err_len);
+    }
+}
+
+extern "C" int kbsrc_conversion_share_c(const kbsrc_conversion* cvp, long long* share6) {
+    if (!cvp || !share6) return -1;
+    const kbsrc_gpu_shard& s = reinterpret_cast<const kbsrc::Conversion*>(cvp)->desc.shard;
+    const long long v[6] = {s.blk0, s.blk1, s.frame0, s.frames, s.out0, s.nout};
+    std::memcpy(share6, v, sizeof v);
+    return 0;
 }
 
 extern "C" int kbsrc_conversion_run_c(kbsrc_conversion* cv, const double* in, double* out, char* err, int err_len) {

@@ -229,3 +229,16 @@ def split_work(plan, channels):
         per[pre + "_column"] = _tc_sub_ops(N1, N2)
         per[pre + "_row"] = _tc_sub_ops(N2, N1) if N2 > 1 else 0
     return {"tasks": tasks, "int8_ops_per_task": per, "int8_ops_total": sum(per.values()) * tasks}
+
+
+def error_stats(y, ref):
+    """Error of y against ref (the exact output): max and RMS of |y - ref| absolute, in dB of full scale 1.0, and in
+    float64 ULPs of each ref sample (samples below 2^-10 of the peak left out of the ULP figures)."""
+    import numpy as np
+    d = np.abs(np.asarray(y, dtype=np.float64) - ref)
+    mx, rms = float(d.max(initial=0.0)), float(np.sqrt(np.mean(d * d))) if d.size else 0.0
+    big = np.abs(ref) >= np.abs(ref).max(initial=0.0) * 2.0 ** -10
+    u = d[big] / np.spacing(np.abs(ref[big]))
+    db = lambda v: round(20 * np.log10(v), 2) if v > 0 else None
+    return {"max_abs": mx, "rms_abs": rms, "max_db": db(mx), "rms_db": db(rms),
+            "max_ulps": float(u.max(initial=0.0)), "rms_ulps": float(np.sqrt(np.mean(u * u))) if u.size else 0.0}

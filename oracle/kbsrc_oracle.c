@@ -657,6 +657,7 @@ typedef struct {
     long long P, Q, nout, Lk, E, pre, span, nblk, base, tot, o, c2, fk, fi, fo, mn;
     int up, nb, marg, hop, Nb, Mb, Jg, gen;
     double fml;
+    long long blk0, blk1; /* the blocks the engine runs: [0, nblk) unless a caller restricts them */
 } Plan;
 
 static long long gcdll(long long a, long long b) {
@@ -738,6 +739,8 @@ static int make_plan(Plan* pl, const double* in, long long frames, int ch, int r
     pl->Mb = (int)(nb * P);
     pl->hop = nb - 2 * marg;
     pl->nblk = (span + (long long)pl->hop * Q - 1) / ((long long)pl->hop * Q);
+    pl->blk0 = 0;
+    pl->blk1 = pl->nblk;
     pl->base = (long long)marg * Q;
     pl->tot = pl->base + pl->nblk * pl->hop * Q + pl->Nb;
     pl->E = E;
@@ -769,7 +772,7 @@ static void engine(const Plan* pl, double** xx, double** out, int ch, const dd* 
     cdd* y = malloc(sizeof(cdd) * (size_t)(mx / 2 + 1));
     const cdd zero = cx(D(0.0), D(0.0));
     for (int c = 0; c < ch; c++)
-        for (long long b = 0; b < pl->nblk; b++) {
+        for (long long b = pl->blk0; b < pl->blk1; b++) {
             const double* s = xx[c] + b * pl->hop * Q;
             for (int i = 0; i < Nb; i++) rin[i] = D(s[i]);
             rfft_forward(&Fw, rin, X, z, y);
@@ -1071,7 +1074,7 @@ static void engine_ld(const Plan* pl, double** xx, double** out, int ch, const d
     cld* y = malloc(sizeof(cld) * (size_t)(mx / 2 + 1));
     LD* r = malloc(sizeof(LD) * (size_t)Mb);
     for (int c = 0; c < ch; c++)
-        for (long long b = 0; b < pl->nblk; b++) {
+        for (long long b = pl->blk0; b < pl->blk1; b++) {
             const double* s = xx[c] + b * pl->hop * Q;
             /* forward real FFT (fft.hpp:362-408): pack, transform, conjugate-pair split */
             for (int i = 0; i < h; i++) z[i] = lc((LD)s[2 * i], (LD)s[2 * i + 1]);
@@ -1176,13 +1179,21 @@ long long oracle_plan(long long frames, int ch, int rate_in, int rate_out, int f
 
 /* Full conversion. mode: 0 exact, 1 fast, 2 long double. out: ch * out_cap doubles, planar. Returns nout, or a
  * negative error code. */
-long long oracle_resample(const double* in, long long frames, int ch, int rate_in, int rate_out, int mode,
-                          double length, double beta, int block, int lpc, double* out, long long out_cap,
-                          long long* info) {
+/* The conversion with its block loop restricted to blocks [blk0, blk1) of every channel (blk1 < 0: all blocks);
+ * output samples no block of the range writes stay as the caller left them. Test infrastructure for shares of a
+ * conversion split across devices; the reference runs all blocks (src/resampler.cpp:41-48). */
+long long oracle_resample_blocks(const double* in, long long frames, int ch, int rate_in, int rate_out, int mode,
+                                 double length, double beta, int block, int lpc, long long blk0, long long blk1,
+                                 double* out, long long out_cap, long long* info) {
     Plan pl;
     const int fast = mode == 1;
     int rc = make_plan(&pl, in, frames, ch, rate_in, rate_out, fast, length, beta, block);
     if (rc < 0) return rc;
+    if (blk1 >= 0) {
+        if (blk0 < 0 || blk1 < blk0 || blk1 > pl.nblk) return -101;
+        pl.blk0 = blk0;
+        pl.blk1 = blk1;
+    }
     if (pl.nout > out_cap) return -100;
     if (rc == 1) {
         for (int c = 0; c < ch; c++)
@@ -1249,6 +1260,13 @@ long long oracle_resample(const double* in, long long frames, int ch, int rate_i
     for (int c = 0; c < ch; c++) free(xx[c]);
     free(xx); free(op); free(H);
     return pl.nout;
+}
+
+long long oracle_resample(const double* in, long long frames, int ch, int rate_in, int rate_out, int mode,
+                          double length, double beta, int block, int lpc, double* out, long long out_cap,
+                          long long* info) {
+    return oracle_resample_blocks(in, frames, ch, rate_in, rate_out, mode, length, beta, block, lpc, 0, -1, out,
+                                  out_cap, info);
 }
 
 /* Pieces for unit checks ------------------------------------------------------------------------------- */

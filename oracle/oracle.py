@@ -45,6 +45,11 @@ def oracle_lib():
         lib.oracle_resample.argtypes = [_dp, ctypes.c_longlong, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                         ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int,
                                         _dp, ctypes.c_longlong, _lp]
+        lib.oracle_resample_blocks.restype = ctypes.c_longlong
+        lib.oracle_resample_blocks.argtypes = [_dp, ctypes.c_longlong, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                               ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                               ctypes.c_int, ctypes.c_longlong, ctypes.c_longlong, _dp,
+                                               ctypes.c_longlong, _lp]
         lib.oracle_plan.restype = ctypes.c_longlong
         lib.oracle_plan.argtypes = [ctypes.c_longlong, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                     ctypes.c_double, ctypes.c_double, ctypes.c_int, _lp]
@@ -100,6 +105,23 @@ def resample(x, rate_in, rate_out, fast=False, length=0.2, beta=40.0, block=0, l
         raise ValueError(ORACLE_ERRORS.get(n, f"error {n}"))
     if info is not None:
         info.update(zip(INFO_KEYS, inf.tolist()))
+    return out[:, :n]
+
+
+def resample_blocks(x, rate_in, rate_out, blk0, blk1, mode="exact", length=0.2, beta=40.0, block=0, lpc=True):
+    """The oracle conversion restricted to blocks [blk0, blk1) of every channel: planar (channels, nout) with the
+    samples no block of the range writes left at zero."""
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    if x.ndim == 1:
+        x = x[:, None]
+    frames, ch = x.shape
+    cap = max(1, nout_of(frames, rate_in, rate_out))
+    out = np.zeros((ch, cap), dtype=np.float64)
+    inf = np.zeros(16, dtype=np.int64)
+    n = oracle_lib().oracle_resample_blocks(_ptr(x), frames, ch, rate_in, rate_out, MODES[mode], length, beta,
+                                            block, int(lpc), blk0, blk1, _ptr(out), cap, inf.ctypes.data_as(_lp))
+    if n < 0:
+        raise ValueError(ORACLE_ERRORS.get(n, f"error {n}"))
     return out[:, :n]
 
 

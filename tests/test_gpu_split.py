@@ -8,7 +8,8 @@ import numpy as np
 import pytest
 
 import kbsrc_b200
-from cases import noise
+from cases import noise, sweep
+from kbsrc_b200.roofline import error_stats
 
 pytestmark = pytest.mark.gpu
 
@@ -41,6 +42,22 @@ def test_split_full_size_c2():
     es, ef, peak = errors(x, 96000, 44100)
     print(f"split {es:.3e} fast {ef:.3e} peak {peak:.3e}")
     assert es <= ef
+
+
+def test_split_c3_sweep_error_stated():
+    """60 s stereo 44.1 kHz -> 48 kHz log sine sweep 20 Hz - 20 kHz at amplitude 0.5: the upsampling path, whose
+    spectrum is extended periodically (the reference's src/resampler.cpp:72-78) instead of folded. The split form's
+    max and RMS error against the exact output, in dB and float64 ULPs, beside the fast engine's; the split form's
+    maximum may not exceed the fast engine's."""
+    x = sweep(60, 44100, 2)
+    st = {}
+    s = kbsrc_b200.resample(x, 44100, 48000, mode="split", stats=st)
+    e = kbsrc_b200.resample(x, 44100, 48000, mode="exact")
+    f = kbsrc_b200.resample(x, 44100, 48000, mode="fast")
+    assert st["isa"] == "sm_100a" and s.shape == e.shape == f.shape
+    es, ef = error_stats(s, e), error_stats(f, e)
+    print(f"split {es}\nfast  {ef}")
+    assert es["max_abs"] <= ef["max_abs"]
 
 
 def test_split_three_radix_sub_fft():
