@@ -146,6 +146,15 @@ def measured_hbm_gbs():
         return 6650.0, "fallback"
 
 
+def measured_bf16_tflops():
+    """The measured dense bf16 GEMM rate of this pool's B200 (burst), else the fallback figure."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["bf16_tflops"])
+    except Exception:
+        return 1590.0
+
+
 def load_traffic():
     """dram bytes per launch from the committed ncu summary, if any: {workload: {pass: bytes}}."""
     try:
@@ -284,7 +293,7 @@ def companion_form(mode, x, w, kw, dev, stream, args, ref_out, tune):
     for _ in range(args.warmup):
         cv.run_device(*ptrs, stream=stream)
     torch.cuda.synchronize()
-    shapes = cv.tune(*ptrs, stream=stream) if tune and mode != "split" else None
+    shapes = cv.tune(*ptrs, stream=stream) if tune and not mode.startswith("split") else None
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
     for _ in range(args.steps):
@@ -312,9 +321,12 @@ def companion_form(mode, x, w, kw, dev, stream, args, ref_out, tune):
                                    "bytes (each block's input span and kept output) / HBM peak (" + how + ")); "
                                    "frac = roofline time / measured time"}
     else:
-        tw = roofline.split_work(plan, ch)
-        out["int8_ops_per_step"] = tw["int8_ops_total"]
-        out["tensor_frac_of_nominal"] = round(tw["int8_ops_total"] / (ms * 1e-3) / 1e12 / TENSOR_INT8_PEAK_TOPS, 4)
+        eb = 2 if mode == "split16" else 1
+        tw = roofline.split_work(plan, ch, eb)
+        peak = TENSOR_INT8_PEAK_TOPS if eb == 1 else measured_bf16_tflops()  # f16 runs at the bf16 rate
+        out["tensor_ops_per_step"] = tw["ops_total"]
+        out["tensor_kind"] = "int8" if eb == 1 else "f16"
+        out["tensor_frac_of_nominal"] = round(tw["ops_total"] / (ms * 1e-3) / 1e12 / peak, 4)
     cv.close()
     return out
 
@@ -508,7 +520,7 @@ def product_arm(args, w, world, rank, local, pg):
         # the metric's other half: the split-precision form (and the fast engine) beside plain exact, same process,
         # same resident input, errors against the exact output just timed
         ref_y = got.copy()
-        for mode in ("split", "fast"):
+        for mode in ("split", "split16", "fast"):
             f = companion_form(mode, x, w, kw, dev, stream, args, ref_y, args.tune)
             f["vs_plain_exact"] = round((ms / args.steps) / f["ms_per_step"], 4)
             extra[mode] = f

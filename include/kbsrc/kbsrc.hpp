@@ -13,8 +13,9 @@ enum class Precision {
     Fast,        // float64 pipeline
     Exact,       // double-double (~106-bit) pipeline
     LongDouble,  // x87 80-bit extended; the GPU emulates its arithmetic in integers, bit for bit
-    SplitTC,     // not in the reference: the Exact plan with its FFT stages as int8 tensor-core contractions
-                 // (split precision); within float64 rounding of Exact, not byte-identical
+    SplitTC,     // not in the reference: the Exact plan with its FFT stages as tensor-core contractions of 8-bit
+                 // digit slices in int8 (split precision); within float64 rounding of Exact, not byte-identical
+    SplitTC16,   // not in the reference: the same with the digit slices in f16 (f32 accumulation); same output
 };
 
 struct Options {

@@ -9,7 +9,8 @@ extern "C" {
 
 typedef struct {
     int precision; /* 0 fast, 1 exact, 2 long double (x87 extended, emulated on the GPU), 3 split-precision
-                      tensor-core form (no reference counterpart; float64-level accuracy) */
+                      tensor-core form with int8 digit slices, 4 the same with f16 digit slices (no reference
+                      counterpart; float64-level accuracy) */
     double length; /* one-sided kernel length, seconds (reference default 0.2) */
     double beta;   /* Kaiser beta (default 40) */
     int threads;   /* host threads, 0 = automatic */

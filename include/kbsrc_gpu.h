@@ -29,8 +29,11 @@ extern "C" {
 #define KBSRC_GPU_FAST 0  /* float64 pipeline (reference Precision::Fast) */
 #define KBSRC_GPU_EXACT 1 /* double-double pipeline (reference Precision::Exact) */
 #define KBSRC_GPU_LD 2    /* x87 extended pipeline, emulated in integers (reference Precision::LongDouble) */
-#define KBSRC_GPU_SPLIT 3 /* split-precision form: tensor-core int8 DFT contractions, float64 elsewhere; not
-                             byte-identical, within float64 rounding of exact (no reference counterpart) */
+#define KBSRC_GPU_SPLIT 3 /* split-precision form: tensor-core DFT contractions of 8-bit digit slices as int8
+                             (int32 accumulators), float64 elsewhere; not byte-identical, within float64 rounding
+                             of exact (no reference counterpart) */
+#define KBSRC_GPU_SPLIT_F16 4 /* the same split-precision form with the digit slices as f16 (f32 accumulators):
+                                 the same products, exact in both, so the same output bytes as KBSRC_GPU_SPLIT */
 
 /* Sample formats of the interleaved input (kbsrc_gpu_desc.in_format). The GPU reads each sample as the
  * reference's WAV reader decodes it (src/io/wav.cpp:299-362): float64 as stored, float32 widened, integer PCM
@@ -62,7 +65,7 @@ typedef struct {
  * `lead` zeros/edge samples before input frame 0 (lead = marg*Q + pre), and writes output samples
  * [b*hop*P - o, (b+1)*hop*P - o) clipped to [0, nout). */
 typedef struct {
-    int precision;      /* KBSRC_GPU_FAST, KBSRC_GPU_EXACT, KBSRC_GPU_LD or KBSRC_GPU_SPLIT */
+    int precision;      /* KBSRC_GPU_FAST, KBSRC_GPU_EXACT, KBSRC_GPU_LD, KBSRC_GPU_SPLIT or KBSRC_GPU_SPLIT_F16 */
     int channels;       /* >= 1 */
     long long P, Q;     /* reduced rate ratio rate_out/rate_in = P/Q */
     int nb;             /* block size factor: forward FFT nb*Q points, inverse nb*P */

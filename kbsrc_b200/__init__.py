@@ -178,7 +178,7 @@ def _ptr(a):
 
 
 def _options(mode, length, beta, block, lpc, threads):
-    prec = {"fast": 0, "exact": 1, "ld": 2, "split": 3}[mode] if isinstance(mode, str) else int(mode)
+    prec = {"fast": 0, "exact": 1, "ld": 2, "split": 3, "split16": 4}[mode] if isinstance(mode, str) else int(mode)
     return Options(prec, float(length), float(beta), int(threads), int(block), int(bool(lpc)))
 
 
@@ -431,7 +431,7 @@ def shard_plan(frames, channels, rate_in, rate_out, count, mode="exact", length=
     if p["copy"]:
         raise ValueError("equal rates: no block loop to split")
     d = GpuDesc()
-    d.precision = {"fast": 0, "exact": 1, "ld": 2, "split": 3}[mode]
+    d.precision = {"fast": 0, "exact": 1, "ld": 2, "split": 3, "split16": 4}[mode]
     d.channels, d.P, d.Q, d.nb, d.marg, d.nblk = channels, p["P"], p["Q"], p["nb"], p["marg"], p["nblk"]
     d.lead, d.o, d.frames, d.nout, d.up = p["lead"], p["o"], frames, p["nout"], p["up"]
     n_spec = (p["Mb"] if p["up"] else p["Nb"]) // 2 + 1

@@ -561,16 +561,18 @@ struct TcParams {
 
 // Column pass, persistent: each CTA sets up its tensor memory and tables once, then takes items (column group
 // g, task slot y) in turn, item = y * groups + g (reading the signal: item = g * slots + y). An item: sequences
-// n2 in [c0, c0+F) of length N1 (stride N2), the sub-FFT, the four-step twiddle, stored in place; with N2 == 1
-// the single column is the whole transform and DST may write it as output samples.
-template <int SRC, int DST>
+// n2 in [c0, c0+F) of length N1 (stride N2) through the sub-FFT, its first stage reading the input straight from
+// global memory and its last stage storing, with the four-step twiddle, straight to global memory (in place);
+// with N2 == 1 the single column is the whole transform and DST may write it as output samples. S: the digit
+// slices' element kind (TcI8 or TcF16).
+template <class S, int SRC, int DST>
 __global__ void __launch_bounds__(kTcThreads, 1)
     k_tc_column(const __grid_constant__ PassParams<ArF64> P, const __grid_constant__ TcParams T) {
     extern __shared__ __align__(16) unsigned char smem[];
     using C = CxR<ArF64>;
-    const int F = T.sub.F, N1 = T.N1, N2 = T.N2, total = N1 * F, groups = (N2 + F - 1) / F;
-    Planes<ArF64> A, B;
-    const TcSmem m = tc_carve(carve<ArF64>(smem, total, A, B), T.sub);
+    const int F = T.sub.F, N1 = T.N1, N2 = T.N2, groups = (N2 + F - 1) / F;
+    Planes<ArF64> X, Y;
+    const TcSmem m = tc_carve(carve<ArF64>(smem, N1 * F, X, Y), T.sub);
     const uint32_t tmem = tc_setup(m, T.sub);
     uint32_t phase = 0;
     for (long long item = blockIdx.x; item < (long long)groups * T.slots; item += gridDim.x) {
@@ -581,97 +583,72 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         const C* src = P.src + slot * P.stride;
         C* dst = P.dst + slot * P.stride;
         const TaskSource ts = SRC == kSrcSignal ? task_source(P.work, task, 2LL * N1 * N2) : TaskSource{};
-        for (int e0 = threadIdx.x; e0 < total; e0 += kLoadBatch * blockDim.x) {
-            C v[kLoadBatch];
-#pragma unroll
-            for (int j = 0; j < kLoadBatch; j++) {
-                const int e = e0 + j * blockDim.x, r = e / F, n2 = c0 + (e - r * F);
-                if (e < total)
-                    v[j] = n2 < N2 ? load_input<ArF64, SRC>(P, ts, src, (long long)r * N2 + n2) : czero<ArF64>();
-            }
-#pragma unroll
-            for (int j = 0; j < kLoadBatch; j++)
-                if (e0 + j * blockDim.x < total) A.st(e0 + j * blockDim.x, v[j]);
-        }
-        __syncthreads();
-        tc_subfft(T.sub, A, B, m, tmem, phase, T.err);
         const TaskRef tr = DST == kDstOutput ? task_ref(P.work, task) : TaskRef{0, 0, 0};
         const Item it = DST == kDstOutput ? item_of(P.work, tr) : Item{};
-        // four-step twiddle and store; the table loads of a batch are issued before any of its products
-        for (int e0 = threadIdx.x; e0 < total; e0 += kLoadBatch * blockDim.x) {
-            double2 w[kLoadBatch];
-#pragma unroll
-            for (int j = 0; j < kLoadBatch; j++) {
-                const int e = e0 + j * blockDim.x, k1 = e / F, n2 = c0 + (e - k1 * F);
-                w[j] = make_double2(1.0, 0.0);
-                if (DST == kDstComplex && T.tw4 && e < total && n2 < N2) w[j] = __ldg(T.tw4 + (long long)k1 * N2 + n2);
-            }
-#pragma unroll
-            for (int j = 0; j < kLoadBatch; j++) {
-                const int e = e0 + j * blockDim.x, k1 = e / F, n2 = c0 + (e - k1 * F);
-                if (e >= total || n2 >= N2) continue;
-                C v = A.ld(e);
+        tc_subfft<S>(
+            T.sub, true, X, Y, m, tmem, phase, T.err,
+            [&](int n, int f) {
+                const int n2 = c0 + f;
+                if (n2 >= N2) return make_double2(0.0, 0.0);
+                const C v = load_input<ArF64, SRC>(P, ts, src, (long long)n * N2 + n2);
+                return make_double2(v.re, v.im);
+            },
+            [&](int k1, int f, double re, double im) {
+                const int n2 = c0 + f;
+                if (n2 >= N2) return;
                 if (DST == kDstComplex) {
-                    if (T.tw4) v = c_mulw<ArF64>(v, CxW<ArF64>{w[j].x, w[j].y});
-                    dst[(long long)k1 * N2 + n2] = v;
+                    const long long i = (long long)k1 * N2 + n2;
+                    double2 y = make_double2(re, im);
+                    if (T.tw4) y = tc_cmul(re, im, __ldg(T.tw4 + i));
+                    dst[i] = C{y.x, y.y};
                 } else {
-                    emit(P.work, it, tr.c, tr.b, 2LL * k1, v.re);
-                    emit(P.work, it, tr.c, tr.b, 2LL * k1 + 1, -v.im);
+                    emit(P.work, it, tr.c, tr.b, 2LL * k1, re);
+                    emit(P.work, it, tr.c, tr.b, 2LL * k1 + 1, -im);
                 }
-            }
-        }
-        __syncthreads();
+            });
     }
     tc_teardown(T.sub, tmem);
 }
 
 // Row pass, persistent like the column pass: items (row group g, task slot y); an item transforms rows r in
-// [r0, r0+F) of length N2 and stores them transposed to [N1*k2 + r], or writes them as output samples.
-template <int DST>
+// [r0, r0+F) of length N2 (its first stage reading them from global memory, neighbouring rows of the MMA taking
+// neighbouring inputs) and stores them transposed to [N1*k2 + r], or writes them as output samples.
+template <class S, int DST>
 __global__ void __launch_bounds__(kTcThreads, 1)
     k_tc_row(const __grid_constant__ PassParams<ArF64> P, const __grid_constant__ TcParams T) {
     extern __shared__ __align__(16) unsigned char smem[];
     using C = CxR<ArF64>;
-    const int F = T.sub.F, N1 = T.N1, N2 = T.N2, total = N2 * F, groups = (N1 + F - 1) / F;
-    Planes<ArF64> A, B;
-    const TcSmem m = tc_carve(carve<ArF64>(smem, total, A, B), T.sub);
+    const int F = T.sub.F, N1 = T.N1, N2 = T.N2, groups = (N1 + F - 1) / F;
+    Planes<ArF64> X, Y;
+    const TcSmem m = tc_carve(carve<ArF64>(smem, N2 * F, X, Y), T.sub);
     const uint32_t tmem = tc_setup(m, T.sub);
     uint32_t phase = 0;
     for (long long item = blockIdx.x; item < (long long)groups * T.slots; item += gridDim.x) {
         const int slot = (int)(item / groups), r0 = (int)(item - (long long)slot * groups) * F;
         const long long task = P.task0 + slot;
         const C* src = P.src + slot * P.stride;
-        for (int e0 = threadIdx.x; e0 < total; e0 += kLoadBatch * blockDim.x) {
-            C v[kLoadBatch];
-#pragma unroll
-            for (int j = 0; j < kLoadBatch; j++) {
-                const int e = e0 + j * blockDim.x, f = e / N2, i = e - f * N2, row = r0 + f;
-                if (e < total) v[j] = row < N1 ? src[(long long)row * N2 + i] : czero<ArF64>();
-            }
-#pragma unroll
-            for (int j = 0; j < kLoadBatch; j++) {
-                const int e = e0 + j * blockDim.x, f = e / N2, i = e - f * N2;
-                if (e < total) A.st(i * F + f, v[j]);
-            }
-        }
-        __syncthreads();
-        tc_subfft(T.sub, A, B, m, tmem, phase, T.err);
         C* dst = P.dst + slot * P.stride;
         const TaskRef tr = DST == kDstOutput ? task_ref(P.work, task) : TaskRef{0, 0, 0};
         const Item it = DST == kDstOutput ? item_of(P.work, tr) : Item{};
-        for (int e = threadIdx.x; e < total; e += blockDim.x) {
-            const int k2 = e / F, f = e - k2 * F, row = r0 + f;
-            if (row >= N1) continue;
-            const C v = A.ld(e);
-            const long long iz = (long long)N1 * k2 + row;
-            if (DST == kDstComplex) {
-                dst[iz] = v;
-            } else {
-                emit(P.work, it, tr.c, tr.b, 2 * iz, v.re);
-                emit(P.work, it, tr.c, tr.b, 2 * iz + 1, -v.im);
-            }
-        }
-        __syncthreads();
+        tc_subfft<S>(
+            T.sub, false, X, Y, m, tmem, phase, T.err,
+            [&](int n, int f) {
+                const int row = r0 + f;
+                if (row >= N1) return make_double2(0.0, 0.0);
+                const C v = src[(long long)row * N2 + n];
+                return make_double2(v.re, v.im);
+            },
+            [&](int k2, int f, double re, double im) {
+                const int row = r0 + f;
+                if (row >= N1) return;
+                const long long iz = (long long)N1 * k2 + row;
+                if (DST == kDstComplex) {
+                    dst[iz] = C{re, im};
+                } else {
+                    emit(P.work, it, tr.c, tr.b, 2 * iz, re);
+                    emit(P.work, it, tr.c, tr.b, 2 * iz + 1, -im);
+                }
+            });
     }
     tc_teardown(T.sub, tmem);
 }
@@ -985,14 +962,20 @@ int make_dev_cfft(int n, int tab, int fmax, DevCfft& d, cudaStream_t st) {
 // (or, where no such pair exists, Ra * Rb * Rc) with radices <= 32, so that every stage is one tcgen05
 // contraction with K, N <= 64.
 // ------------------------------------------------------------------------------------------------------
-// Ra * Rb = N with both <= 32, Ra the largest such divisor <= sqrt(N); false when there is none.
+// Ra * Rb = N with both in [2, 32], Ra the largest such divisor <= sqrt(N); a length of at most 32 without such a
+// split (a prime) is one stage, Ra = N and Rb = 1. False when there is neither.
 bool tc_factor(int N, int& Ra, int& Rb) {
     int best = 0;
-    for (int a = 1; a <= 32 && a * a <= N; a++)
+    for (int a = 2; a <= 32 && a * a <= N; a++)
         if (N % a == 0 && N / a <= 32) best = a;
-    if (!best) return false;
-    Ra = best;
-    Rb = N / best;
+    if (best) {
+        Ra = best;
+        Rb = N / best;
+        return true;
+    }
+    if (N < 2 || N > 32) return false;
+    Ra = N;
+    Rb = 1;
     return true;
 }
 // Ra * Rb * Rc = N, each <= 32 and >= N / 128 (so that every stage has at most 128 rows), the smallest radix as
@@ -1017,20 +1000,37 @@ bool tc_factor3(int N, int& Ra, int& Rb, int& Rc) {
 int tc_kh(int R) { return R <= 16 ? 16 : 32; }
 int tc_nh(int R) { return R <= 16 ? 16 : R <= 24 ? 24 : 32; }
 
+// f16 bits of a small integer v (|v| <= 128): exact
+uint16_t f16_bits(int v) {
+    if (v == 0) return 0;
+    const unsigned a = (unsigned)std::abs(v);
+    int e = 0;
+    while ((a >> (e + 1)) != 0) e++;                                      // 2^e <= a < 2^(e+1)
+    const unsigned mant = (a << (10 - e)) & 0x3FFu;                       // a < 2^8: exact in 10 bits
+    return (uint16_t)((v < 0 ? 0x8000u : 0u) | (unsigned)(e + 15) << 10 | mant);
+}
+
 // The real form of DFT_R (outputs n: real parts, then imaginary parts from nh; inputs k: real parts, then
 // imaginary parts from kh), y_re[k1] = sum_j xr_j cos + xi_j sin, y_im[k1] = sum_j xi_j cos - xr_j sin with the
-// angle 2 pi j k1 / R, each entry halved and cut into kTcSlices signed 7-bit slices of floor(|w| 2^55).
-void tc_matrix(int R, std::vector<unsigned char>& out) {
-    const int kh = tc_kh(R), nh = tc_nh(R), kpad = 2 * kh, npad = 2 * nh, nr = npad / tc_rounds(nh);
+// angle 2 pi j k1 / R. Each entry w becomes W = rint(w 2^54) in seven balanced base-256 digits; slice t holds digit
+// 6 - t of every entry as int8 (eb = 1) or f16 (eb = 2), slice kTcDigits stays zero. Layout [slice][2nh][2kh].
+void tc_matrix(int R, int eb, std::vector<unsigned char>& out) {
+    const int kh = tc_kh(R), nh = tc_nh(R), kpad = 2 * kh * eb, npad = 2 * nh;
     const size_t base = out.size();
-    out.resize(base + (size_t)kTcMats * npad * kpad, 0);  // slice kTcMats - 1 stays zero
+    out.resize(base + (size_t)kTcMats * npad * kpad, 0);
     auto put = [&](int n, int k, double w) {
-        const unsigned long long v = (unsigned long long)(std::fabs(w) * 36028797018963968.0);  // |w| 2^55, exact
-        const int rd = n / nr, nn = n - rd * nr;  // [round][slice][nr rows]
-        for (int i = 0; i < kTcSlices; i++) {
-            int sl = (int)((v >> (49 - 7 * i)) & 127);
-            if (w < 0) sl = -sl;
-            out[base + ((size_t)rd * kTcMats + i) * nr * kpad + umma_off(nn, k, kpad)] = (unsigned char)(signed char)sl;
+        const long long W = std::llrint(std::ldexp(w, 54));  // exact scaling, one rounding; |W| <= 2^54
+        const unsigned long long b = (unsigned long long)(W + 0x80808080808080LL);
+        for (int i = 0; i < kTcDigits; i++) {
+            const int digit = (int)((b >> (8 * i)) & 0xFF) - 128;
+            unsigned char* at = &out[base + (size_t)(kTcDigits - 1 - i) * npad * kpad + umma_off(n, k * eb, kpad)];
+            if (eb == 1) {
+                *at = (unsigned char)(signed char)digit;
+            } else {
+                const uint16_t h = f16_bits(digit);
+                at[0] = (unsigned char)(h & 0xFF);
+                at[1] = (unsigned char)(h >> 8);
+            }
         }
     };
     hd::RootTable rt(R);
@@ -1045,9 +1045,9 @@ void tc_matrix(int R, std::vector<unsigned char>& out) {
         }
 }
 
-// A transform of n points in the split form, resident on the device.
+// A transform of n points in the split form, resident on the device. eb: digit element bytes (1 int8, 2 f16).
 struct TcFftDev {
-    int n = 0, N1 = 0, N2 = 0;
+    int n = 0, N1 = 0, N2 = 0, eb = 1;
     int ctas = 148;  // persistent CTAs per pass: one per SM
     TcSub col{}, row{};
     size_t smem_col = 0, smem_row = 0;
@@ -1055,18 +1055,24 @@ struct TcFftDev {
     size_t bytes() const { return tw4.bytes + tw_in.bytes + mats.bytes; }
 };
 
-// Sub-FFT of N points over `count` sequences: radices, sequences per CTA within the shared-memory limit
-int tc_sub_plan(int N, int count, TcSub& sub, size_t& smem) {
+// Sub-FFT of N points over `count` sequences with digit elements of eb bytes: radices, TMEM columns, sequences
+// per CTA within the shared-memory limit
+int tc_sub_plan(int N, int count, int eb, TcSub& sub, size_t& smem) {
     int Ra, Rb, Rc = 1;
     if (!tc_factor(N, Ra, Rb) && !tc_factor3(N, Ra, Rb, Rc))
         return fail(KBSRC_GPU_E_UNSUPPORTED, "split-precision form: no radix-32 factorisation");
     sub = TcSub{};
     sub.N = N;
+    sub.ebytes = eb;
     sub.a = TcRadix{Ra, tc_kh(Ra), tc_nh(Ra), nullptr};
-    sub.b = TcRadix{Rb, tc_kh(Rb), tc_nh(Rb), nullptr};
+    if (Rb > 1) sub.b = TcRadix{Rb, tc_kh(Rb), tc_nh(Rb), nullptr};
+    else sub.b = TcRadix{1, 0, 0, nullptr};
     if (Rc > 1) sub.c = TcRadix{Rc, tc_kh(Rc), tc_nh(Rc), nullptr};
-    sub.ncols = 512;  // kTcAcc accumulators of up to 48 columns (or 32 per round): more than 256
-    const int rows1 = N / std::min({Ra, Rb, Rc > 1 ? Rc : Rb});  // rows of the largest stage for one sequence
+    const int nh = std::max({sub.a.nh, sub.b.nh, sub.c.nh});
+    sub.ncols = kTcAcc * 2 * nh <= 256 ? 256 : 512;  // a power of two holding kTcAcc accumulators of 2nh columns
+    int rmin = std::min(Ra, Rb > 1 ? Rb : Ra);
+    if (Rc > 1) rmin = std::min(rmin, Rc);
+    const int rows1 = N / rmin;  // rows of the largest stage for one sequence
     int F = std::max(1, std::min(kTcRows / rows1, count));
     for (;; F--) {
         sub.F = F;
@@ -1077,8 +1083,9 @@ int tc_sub_plan(int N, int count, TcSub& sub, size_t& smem) {
     return KBSRC_GPU_OK;
 }
 
-int make_tc_fft(int n, TcFftDev& t) {
+int make_tc_fft(int n, int eb, TcFftDev& t) {
     int rc, a, b, dev = 0;
+    t.eb = eb;
     KB_CUDA(cudaGetDevice(&dev));
     KB_CUDA(cudaDeviceGetAttribute(&t.ctas, cudaDevAttrMultiProcessorCount, dev));
     t.n = n;
@@ -1105,8 +1112,8 @@ int make_tc_fft(int n, TcFftDev& t) {
     if (!t.N1)
         return fail(KBSRC_GPU_E_UNSUPPORTED, "split-precision form: transform length " + std::to_string(n) +
                                                  " has no factorisation into radices <= 32");
-    if ((rc = tc_sub_plan(t.N1, t.N2, t.col, t.smem_col)) != KBSRC_GPU_OK) return rc;
-    if (t.N2 > 1 && (rc = tc_sub_plan(t.N2, t.N1, t.row, t.smem_row)) != KBSRC_GPU_OK) return rc;
+    if ((rc = tc_sub_plan(t.N1, t.N2, eb, t.col, t.smem_col)) != KBSRC_GPU_OK) return rc;
+    if (t.N2 > 1 && (rc = tc_sub_plan(t.N2, t.N1, eb, t.row, t.smem_row)) != KBSRC_GPU_OK) return rc;
     // sliced matrices of the (up to six) radices, the inner twiddles of each sub-FFT, and the four-step twiddles
     std::vector<unsigned char> mats;
     size_t off[6];
@@ -1114,7 +1121,7 @@ int make_tc_fft(int n, TcFftDev& t) {
     const int nr = t.N2 > 1 ? 6 : 3;
     for (int i = 0; i < nr; i++) {
         off[i] = mats.size();
-        if (rads[i]->R > 1) tc_matrix(rads[i]->R, mats);
+        if (rads[i]->R > 1) tc_matrix(rads[i]->R, eb, mats);
     }
     if ((rc = t.mats.alloc(mats.size())) != KBSRC_GPU_OK) return rc;
     KB_CUDA(cudaMemcpy(t.mats.p, mats.data(), mats.size(), cudaMemcpyHostToDevice));
@@ -1277,7 +1284,7 @@ int allow_large_smem() {
     int mx = 0;
     KB_CUDA(cudaDeviceGetAttribute(&mx, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     cudaFuncAttributes fa{};
-    KB_CUDA(cudaFuncGetAttributes(&fa, (const void*)k_tc_row<kDstOutput>));
+    KB_CUDA(cudaFuncGetAttributes(&fa, (const void*)k_tc_row<TcF16, kDstOutput>));
     if (fa.maxDynamicSharedSizeBytes >= mx) return KBSRC_GPU_OK;
 #define KB_SMEM(k) KB_CUDA(cudaFuncSetAttribute((const void*)(k), cudaFuncAttributeMaxDynamicSharedMemorySize, mx))
     KB_SMEM((k_column<ArF64, kSrcSignal>));
@@ -1305,11 +1312,16 @@ int allow_large_smem() {
     KB_SMEM((k_direct<ArX80, kSrcSignal, kDstComplex>));
     KB_SMEM((k_direct<ArX80, kSrcComplex, kDstComplex>));
     KB_SMEM((k_direct<ArX80, kSrcComplex, kDstOutput>));
-    KB_SMEM((k_tc_column<kSrcSignal, kDstComplex>));
-    KB_SMEM((k_tc_column<kSrcComplex, kDstComplex>));
-    KB_SMEM((k_tc_column<kSrcComplex, kDstOutput>));
-    KB_SMEM((k_tc_row<kDstComplex>));
-    KB_SMEM((k_tc_row<kDstOutput>));  // last: the marker read above
+    KB_SMEM((k_tc_column<TcI8, kSrcSignal, kDstComplex>));
+    KB_SMEM((k_tc_column<TcI8, kSrcComplex, kDstComplex>));
+    KB_SMEM((k_tc_column<TcI8, kSrcComplex, kDstOutput>));
+    KB_SMEM((k_tc_row<TcI8, kDstComplex>));
+    KB_SMEM((k_tc_row<TcI8, kDstOutput>));
+    KB_SMEM((k_tc_column<TcF16, kSrcSignal, kDstComplex>));
+    KB_SMEM((k_tc_column<TcF16, kSrcComplex, kDstComplex>));
+    KB_SMEM((k_tc_column<TcF16, kSrcComplex, kDstOutput>));
+    KB_SMEM((k_tc_row<TcF16, kDstComplex>));
+    KB_SMEM((k_tc_row<TcF16, kDstOutput>));  // last: the marker read above
 #undef KB_SMEM
     return KBSRC_GPU_OK;
 }
@@ -1530,7 +1542,7 @@ int enqueue_plan(const PlanCore& pc, const Work& work, long long t_begin, long l
 
 // One split-form transform of every slot: column pass (x in place, or straight to y / the output when N2 == 1),
 // then the row pass x -> y or to the output epilogue (DST).
-template <int SRC, int DST>
+template <class S, int SRC, int DST>
 int launch_tc(const TcFftDev& t, const Slots& sl, void* x, void* y, int* err, cudaStream_t st, Trail& tr, int kA,
               int kB) {
     PassParams<ArF64> p{};
@@ -1548,10 +1560,10 @@ int launch_tc(const TcFftDev& t, const Slots& sl, void* x, void* y, int* err, cu
     T.err = err;
     auto grid = [&](long long items) { return (unsigned)std::max(1LL, std::min(items, (long long)t.ctas)); };
     if (t.N2 == 1) {
-        k_tc_column<SRC, DST><<<grid(sl.nt), kTcThreads, t.smem_col, st>>>(p, T);
+        k_tc_column<S, SRC, DST><<<grid(sl.nt), kTcThreads, t.smem_col, st>>>(p, T);
         return tr.mark(st, kA);
     }
-    k_tc_column<SRC, kDstComplex>
+    k_tc_column<S, SRC, kDstComplex>
         <<<grid((long long)((t.N2 + t.col.F - 1) / t.col.F) * sl.nt), kTcThreads, t.smem_col, st>>>(p, T);
     int rc = tr.mark(st, kA);
     if (rc) return rc;
@@ -1559,11 +1571,13 @@ int launch_tc(const TcFftDev& t, const Slots& sl, void* x, void* y, int* err, cu
     p.dst = static_cast<CxR<ArF64>*>(y);
     T.sub = t.row;
     T.tw4 = nullptr;
-    k_tc_row<DST><<<grid((long long)((t.N1 + t.row.F - 1) / t.row.F) * sl.nt), kTcThreads, t.smem_row, st>>>(p, T);
+    k_tc_row<S, DST><<<grid((long long)((t.N1 + t.row.F - 1) / t.row.F) * sl.nt), kTcThreads, t.smem_row, st>>>(p, T);
     return tr.mark(st, kB);
 }
 
-// The block loop in the split-precision form: tensor-core transforms, float64 split, spectrum and merge.
+// The block loop in the split-precision form: tensor-core transforms, float64 split, spectrum and merge. S: the
+// digit slices' element kind.
+template <class S>
 int enqueue_split(const PlanCore& pc, const Work& work, long long t_begin, long long t_end, void* a, void* b,
                   long long stride, long long wave, cudaStream_t st, Trail& tr) {
     const kbsrc_gpu_desc& d = pc.d;
@@ -1575,7 +1589,7 @@ int enqueue_split(const PlanCore& pc, const Work& work, long long t_begin, long 
     for (long long t0 = t_begin; t0 < t_end; t0 += wave) {
         sl.task0 = t0;
         sl.nt = (unsigned)std::min(wave, t_end - t0);
-        if ((rc = launch_tc<kSrcSignal, kDstComplex>(pc.tfw, sl, a, b, err, st, tr, kFwdA, kFwdB)) != KBSRC_GPU_OK)
+        if ((rc = launch_tc<S, kSrcSignal, kDstComplex>(pc.tfw, sl, a, b, err, st, tr, kFwdA, kFwdB)) != KBSRC_GPU_OK)
             return rc;
         SpecParams<ArF64> s{};
         s.Z = static_cast<CxR<ArF64>*>(b);
@@ -1590,7 +1604,7 @@ int enqueue_split(const PlanCore& pc, const Work& work, long long t_begin, long 
         if ((rc = tr.mark(st, kSplit)) != KBSRC_GPU_OK) return rc;
         k_merge<ArF64><<<dim3(grid_for(pc.hi, 256), sl.nt), 256, 0, st>>>(s);
         if ((rc = tr.mark(st, kMerge)) != KBSRC_GPU_OK) return rc;
-        if ((rc = launch_tc<kSrcComplex, kDstOutput>(pc.tiv, sl, b, nullptr, err, st, tr, kInvA, kInvB)) !=
+        if ((rc = launch_tc<S, kSrcComplex, kDstOutput>(pc.tiv, sl, b, nullptr, err, st, tr, kInvA, kInvB)) !=
             KBSRC_GPU_OK)
             return rc;
     }
@@ -1599,7 +1613,8 @@ int enqueue_split(const PlanCore& pc, const Work& work, long long t_begin, long 
 
 int enqueue_any(const PlanCore& pc, const Work& work, long long t_begin, long long t_end, void* a, void* b,
                 long long stride, long long wave, cudaStream_t st, Trail& tr) {
-    if (pc.split) return enqueue_split(pc, work, t_begin, t_end, a, b, stride, wave, st, tr);
+    if (pc.split && pc.tfw.eb == 2) return enqueue_split<TcF16>(pc, work, t_begin, t_end, a, b, stride, wave, st, tr);
+    if (pc.split) return enqueue_split<TcI8>(pc, work, t_begin, t_end, a, b, stride, wave, st, tr);
     if (pc.tab == kTabX80) return enqueue_plan<ArX80, ArX80>(pc, work, t_begin, t_end, a, b, stride, wave, st, tr);
     if (pc.exact) return enqueue_plan<ArDDShort, ArDDAccurate>(pc, work, t_begin, t_end, a, b, stride, wave, st, tr);
     return enqueue_plan<ArF64, ArF64>(pc, work, t_begin, t_end, a, b, stride, wave, st, tr);
@@ -1673,7 +1688,7 @@ int shard_span(const kbsrc_gpu_desc& d, long long b0, long long b1, kbsrc_gpu_sh
 int check_desc(const kbsrc_gpu_desc* d) {
     if (!d) return fail(KBSRC_GPU_E_ARG, "null descriptor");
     if (d->precision != KBSRC_GPU_FAST && d->precision != KBSRC_GPU_EXACT && d->precision != KBSRC_GPU_LD &&
-        d->precision != KBSRC_GPU_SPLIT)
+        d->precision != KBSRC_GPU_SPLIT && d->precision != KBSRC_GPU_SPLIT_F16)
         return fail(KBSRC_GPU_E_ARG, "precision");
     if (d->channels < 1 || d->P < 1 || d->Q < 1 || d->nb < 2 || d->nb % 2 || d->marg < 0 || d->nb <= 2 * d->marg)
         return fail(KBSRC_GPU_E_ARG, "bad plan shape");
@@ -1725,7 +1740,7 @@ int make_core(const kbsrc_gpu_desc* desc, PlanCore& pc, cudaStream_t st) {
     pc.d = *desc;
     pc.d.H = nullptr;
     pc.exact = desc->precision == KBSRC_GPU_EXACT;
-    pc.split = desc->precision == KBSRC_GPU_SPLIT;
+    pc.split = desc->precision == KBSRC_GPU_SPLIT || desc->precision == KBSRC_GPU_SPLIT_F16;
     pc.tab = desc->precision == KBSRC_GPU_FAST || pc.split ? kTabF64
              : desc->precision == KBSRC_GPU_EXACT          ? kTabDD
                                                            : kTabX80;
@@ -1736,8 +1751,9 @@ int make_core(const kbsrc_gpu_desc* desc, PlanCore& pc, cudaStream_t st) {
     pc.hop = desc->nb - 2 * desc->marg;
     const int fmax = env_int("KBSRC_GPU_FMAX", pc.tab == kTabF64 ? 5 : 8);
     if (pc.split) {
-        if ((rc = make_tc_fft(pc.hf, pc.tfw)) != KBSRC_GPU_OK) return rc;
-        if ((rc = make_tc_fft(pc.hi, pc.tiv)) != KBSRC_GPU_OK) return rc;
+        const int eb = desc->precision == KBSRC_GPU_SPLIT_F16 ? 2 : 1;
+        if ((rc = make_tc_fft(pc.hf, eb, pc.tfw)) != KBSRC_GPU_OK) return rc;
+        if ((rc = make_tc_fft(pc.hi, eb, pc.tiv)) != KBSRC_GPU_OK) return rc;
         if ((rc = pc.tc_err.alloc(16)) != KBSRC_GPU_OK) return rc;
         KB_CUDA(cudaMemset(pc.tc_err.p, 0, 16));
     } else {

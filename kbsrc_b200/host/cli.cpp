@@ -70,7 +70,7 @@ void help() {
         "usage: kbsrc [options] input.wav output.wav\n"
         "\n"
         "  -r, --rate N        output sample rate in Hz (default 44100)\n"
-        "  -m, --mode M        exact (default), fast, ld, or split (tensor-core form, float64 accuracy)\n"
+        "  -m, --mode M        exact (default), fast, ld, split or split16 (tensor-core forms, float64 accuracy)\n"
         "  -f, --format F      f64 (default), f32, s32, s24 or s16\n"
         "      --dither        TPDF dither for integer formats\n"
         "  -t, --threads N     host threads for kernel design and LPC (default: up to 8)\n"
@@ -102,6 +102,7 @@ int run(int argc, char** argv) {
             else if (m == "fast") opt.precision = kbsrc::Precision::Fast;
             else if (m == "ld") opt.precision = kbsrc::Precision::LongDouble;
             else if (m == "split") opt.precision = kbsrc::Precision::SplitTC;
+            else if (m == "split16") opt.precision = kbsrc::Precision::SplitTC16;
             else throw BadCommandLine{"mode must be exact, fast or ld"};
         } else if (a == "-f" || a == "--format") format = value();
         else if (a == "-t" || a == "--threads") opt.threads = option_value<int>(value(), "--threads");

@@ -48,6 +48,12 @@ using host::dd;
 
 double now() { return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count(); }
 
+// Exact and the split-precision forms (which keep Exact's plan and kernel) run their host arithmetic in
+// round-to-nearest.
+bool is_split_or_exact(Precision p) {
+    return p == Precision::Exact || p == Precision::SplitTC || p == Precision::SplitTC16;
+}
+
 // Runs Exact's host arithmetic in round-to-nearest and restores the caller's rounding mode on exit; only the
 // SSE rounding-control bits are touched on x86 (the reference's dispatch.cpp:37-67 contract).
 class RoundToNearest {
@@ -431,6 +437,7 @@ std::unique_ptr<Conversion> prepare(const void* in, long long frames, int ch, in
     d.precision = opt.precision == Precision::Fast         ? KBSRC_GPU_FAST
                   : opt.precision == Precision::LongDouble ? KBSRC_GPU_LD
                   : opt.precision == Precision::SplitTC    ? KBSRC_GPU_SPLIT
+                  : opt.precision == Precision::SplitTC16  ? KBSRC_GPU_SPLIT_F16
                                                            : KBSRC_GPU_EXACT;
     d.channels = ch;
     d.P = P;
@@ -533,7 +540,7 @@ std::vector<std::vector<double>> resample_gpu(const double* in, long long frames
 
 std::vector<std::vector<double>> resample(const double* in, long long frames, int channels, int rate_in, int rate_out,
                                           const Options& opt, Stats* stats) {
-    RoundToNearest rn(opt.precision == Precision::Exact || opt.precision == Precision::SplitTC);
+    RoundToNearest rn(is_split_or_exact(opt.precision));
     return resample_gpu(in, frames, channels, rate_in, rate_out, opt, stats);
 }
 
@@ -541,7 +548,7 @@ std::vector<std::vector<double>> resample_devices(const double* in, long long fr
                                                   int rate_out, const int* devices, int ndevices, const Options& opt,
                                                   Stats* stats) {
     if (!devices || ndevices < 1) throw std::invalid_argument("no devices given");
-    RoundToNearest rn(opt.precision == Precision::Exact || opt.precision == Precision::SplitTC);
+    RoundToNearest rn(is_split_or_exact(opt.precision));
     auto cv = prepare(in, frames, channels, rate_in, rate_out, opt, false);
     const double t1 = now();
     const long long nout = cv->pl.nout;
@@ -594,7 +601,7 @@ std::vector<unsigned char> resample_wav_data(const double* in, long long frames,
     const std::string f = format ? format : "";
     const int fmt = f == "f64" ? 0 : f == "f32" ? 1 : f == "s32" ? 2 : f == "s24" ? 3 : f == "s16" ? 4 : -1;
     if (fmt < 0) throw std::invalid_argument("format must be f64, f32, s32, s24 or s16");
-    RoundToNearest rn(opt.precision == Precision::Exact || opt.precision == Precision::SplitTC);
+    RoundToNearest rn(is_split_or_exact(opt.precision));
     auto cv = prepare(in, frames, channels, rate_in, rate_out, opt);
     if (cv->pl.copy) throw std::invalid_argument("equal rates: nothing to convert");
     const double t1 = now();
@@ -621,7 +628,7 @@ std::vector<unsigned char> resample_wav_pcm(const void* pcm, const char* sample_
                        : sf == "u8"  ? KBSRC_GPU_IN_U8
                                      : -1;
     if (in_fmt < 0) throw std::invalid_argument("sample format must be f64, f32, s32, s24, s16 or u8");
-    RoundToNearest rn(opt.precision == Precision::Exact || opt.precision == Precision::SplitTC);
+    RoundToNearest rn(is_split_or_exact(opt.precision));
     auto cv = prepare(pcm, frames, channels, rate_in, rate_out, opt, true, nullptr, in_fmt);
     if (cv->pl.copy) throw std::invalid_argument("equal rates: nothing to convert");
     const double t1 = now();
@@ -667,6 +674,8 @@ extern "C" long long kbsrc_resample_c(const double* in, long long frames, int ch
             o.precision = copt->precision == 0   ? kbsrc::Precision::Fast
                           : copt->precision == 2 ? kbsrc::Precision::LongDouble
                           : copt->precision == 3 ? kbsrc::Precision::SplitTC
+                      : copt->precision == 4 ? kbsrc::Precision::SplitTC16
+                          : copt->precision == 4 ? kbsrc::Precision::SplitTC16
                                                  : kbsrc::Precision::Exact;
             o.length = copt->length;
             o.beta = copt->beta;
@@ -705,6 +714,7 @@ kbsrc::Options options_from_c(const kbsrc_options_c* copt) {
         o.precision = copt->precision == 0   ? kbsrc::Precision::Fast
                       : copt->precision == 2 ? kbsrc::Precision::LongDouble
                       : copt->precision == 3 ? kbsrc::Precision::SplitTC
+                      : copt->precision == 4 ? kbsrc::Precision::SplitTC16
                                              : kbsrc::Precision::Exact;
         o.length = copt->length;
         o.beta = copt->beta;
@@ -722,7 +732,7 @@ extern "C" int kbsrc_prepare_c(const double* in, long long frames, int channels,
     *out = nullptr;
     try {
         const kbsrc::Options o = options_from_c(copt);
-        kbsrc::RoundToNearest rn(o.precision == kbsrc::Precision::Exact || o.precision == kbsrc::Precision::SplitTC);
+        kbsrc::RoundToNearest rn(kbsrc::is_split_or_exact(o.precision));
         *out = reinterpret_cast<kbsrc_conversion*>(kbsrc::prepare(in, frames, channels, rate_in, rate_out, o).release());
         return 0;
     } catch (const std::invalid_argument& x) {
@@ -769,7 +779,7 @@ extern "C" int kbsrc_prepare_share_c(const double* in, long long frames, int cha
     *out = nullptr;
     try {
         const kbsrc::Options o = options_from_c(copt);
-        kbsrc::RoundToNearest rn(o.precision == kbsrc::Precision::Exact || o.precision == kbsrc::Precision::SplitTC);
+        kbsrc::RoundToNearest rn(kbsrc::is_split_or_exact(o.precision));
         *out = reinterpret_cast<kbsrc_conversion*>(
             kbsrc::prepare_share(in, frames, channels, rate_in, rate_out, o, index, count).release());
         return 0;
@@ -888,7 +898,7 @@ extern "C" int kbsrc_batch_prepare_c(const kbsrc_batch_item_c* items, int count,
     *out = nullptr;
     try {
         const kbsrc::Options o = options_from_c(copt);
-        kbsrc::RoundToNearest rn(o.precision == kbsrc::Precision::Exact || o.precision == kbsrc::Precision::SplitTC);
+        kbsrc::RoundToNearest rn(kbsrc::is_split_or_exact(o.precision));
         auto b = std::make_unique<kbsrc::BatchRun>();
         b->convs.resize(count);
         kbsrc::SpectrumCache cache;
@@ -898,8 +908,7 @@ extern "C" int kbsrc_batch_prepare_c(const kbsrc_batch_item_c* items, int count,
         kbsrc::Options inner = o;
         inner.threads = 1;  // parallel over conversions instead
         kbsrc::parallel_for(o.threads ? o.threads : hw, count, 1, [&](long long i) {
-            kbsrc::RoundToNearest rn_worker(o.precision == kbsrc::Precision::Exact ||
-                                                     o.precision == kbsrc::Precision::SplitTC);
+            kbsrc::RoundToNearest rn_worker(kbsrc::is_split_or_exact(o.precision));
             try {
                 b->convs[i] = kbsrc::prepare(items[i].in, items[i].frames, items[i].channels, items[i].rate_in,
                                              items[i].rate_out, inner, false, &cache);

@@ -139,21 +139,24 @@ def pass_bytes(plan, exact):
 # ---------------------------------------------------------------------------------------------------------------
 # split-precision form: tensor-core work (mirrors the planner of kbsrc_b200/csrc/engine.cu, make_tc_fft)
 # ---------------------------------------------------------------------------------------------------------------
-TC_SLICES, TC_ACC, TC_ROWS = 8, 9, 128
-TC_PRODUCTS = sum(min(d, TC_SLICES - 1) - max(0, d - TC_SLICES + 1) + 1 for d in range(TC_ACC))  # 43
-# issued accumulator blocks: data slice i against matrix slices 0..8-i (the ninth one zero) in wide MMAs
-TC_ISSUED = sum(TC_ACC - i for i in range(TC_SLICES))  # 44
+TC_DIGITS, TC_ACC, TC_ROWS = 7, 8, 128
+TC_PRODUCTS = sum(1 for a in range(TC_DIGITS) for b in range(TC_DIGITS) if a + b < TC_ACC)  # 34
+# issued accumulator blocks: data slice ta against matrix slices 0..7-ta (the eighth one zero) in wide MMAs
+TC_ISSUED = sum(TC_ACC - ta for ta in range(TC_DIGITS))  # 35
 
 
 def tc_factor(N):
-    """(Ra, Rb) with Ra * Rb = N, both <= 32, Ra the largest such divisor <= sqrt(N); None if there is none."""
+    """(Ra, Rb) with Ra * Rb = N, both in [2, 32], Ra the largest such divisor <= sqrt(N); (N, 1) for a prime N of
+    at most 32; None if there is neither."""
     best = 0
-    a = 1
+    a = 2
     while a <= 32 and a * a <= N:
         if N % a == 0 and N // a <= 32:
             best = a
         a += 1
-    return (best, N // best) if best else None
+    if best:
+        return best, N // best
+    return (N, 1) if 2 <= N <= 32 else None
 
 
 def tc_factor3(N):
@@ -192,43 +195,50 @@ def tc_split(n):
     return None
 
 
-def _tc_stage_ops(R):
-    kh = 16 if R <= 16 else 32
-    nh = 16 if R <= 16 else 24 if R <= 24 else 32
-    kpad, npad = 2 * kh, 2 * nh
-    rounds = 1 if TC_ACC * npad <= 512 else 2
-    nr = npad // rounds
-    return TC_ISSUED * (kpad // 32) * rounds * 2 * TC_ROWS * nr * 32  # issued int8 ops (M x N x K x 2)
+def _kh(R):
+    return 16 if R <= 16 else 32
 
 
-def _tc_sub_ops(N, count):
+def _nh(R):
+    return 16 if R <= 16 else 24 if R <= 24 else 32
+
+
+def _tc_stage_ops(R, eb=1):
+    """Issued tensor-core operations (M x N x K x 2, padding included) of one stage of radix R."""
+    if R <= 1:
+        return 0
+    return TC_ISSUED * 2 * TC_ROWS * 2 * _nh(R) * 2 * _kh(R)
+
+
+def _tc_smem(rads, N, eb=1):
+    al = lambda v: (v + 127) // 128 * 128
+    rr = [R for R in rads if R > 1]
+    kpad = 2 * max(_kh(R) for R in rr) * eb
+    bm = lambda R: (TC_DIGITS + 1) * 2 * _nh(R) * 2 * _kh(R) * eb
+    ntw = N + (rads[1] * rads[2] if len(rads) == 3 else 0)
+    return al(TC_DIGITS * TC_ROWS * kpad) + sum(al(bm(R)) for R in rr) + al(ntw * 16) + al(TC_ROWS * 4) + 128
+
+
+def _tc_sub_ops(N, count, eb=1):
     rads = tc_radices(N)
-    F = max(1, min(TC_ROWS // (N // min(rads)), count))
-    while F > 1 and 2 * N * F * 16 + _tc_smem(rads, N) > 227 * 1024:
+    F = max(1, min(TC_ROWS // (N // min(R for R in rads if R > 1)), count))
+    while F > 1 and 2 * N * F * 16 + _tc_smem(rads, N, eb) > 227 * 1024:
         F -= 1
     items = -(-count // F)
-    return items * sum(_tc_stage_ops(R) for R in rads)
+    return items * sum(_tc_stage_ops(R, eb) for R in rads)
 
 
-def _tc_smem(rads, N):
-    al = lambda v: (v + 127) // 128 * 128
-    kh = lambda R: 16 if R <= 16 else 32
-    nh = lambda R: 16 if R <= 16 else 24 if R <= 24 else 32
-    kpad = 2 * max(kh(R) for R in rads)
-    bm = lambda R: (TC_SLICES + 1) * 2 * nh(R) * 2 * kh(R)
-    ntw = N + (rads[1] * rads[2] if len(rads) == 3 else 0)
-    return al(TC_SLICES * TC_ROWS * kpad) + sum(al(bm(R)) for R in rads) + al(ntw * 16) + al(4 * TC_ROWS * 4) + 128
-
-
-def split_work(plan, channels):
-    """Issued int8 tensor-core operations per task of each split-form pass, and in all."""
+def split_work(plan, channels, eb=1):
+    """Issued tensor-core operations (int8 for eb = 1, f16 for eb = 2) per task of each split-form pass, and in
+    all."""
     tasks = channels * plan["nblk"]
     per = {}
     for pre, n in (("fwd", plan["Nb"] // 2), ("inv", plan["Mb"] // 2)):
         N1, N2 = tc_split(n)
-        per[pre + "_column"] = _tc_sub_ops(N1, N2)
-        per[pre + "_row"] = _tc_sub_ops(N2, N1) if N2 > 1 else 0
-    return {"tasks": tasks, "int8_ops_per_task": per, "int8_ops_total": sum(per.values()) * tasks}
+        per[pre + "_column"] = _tc_sub_ops(N1, N2, eb)
+        per[pre + "_row"] = _tc_sub_ops(N2, N1, eb) if N2 > 1 else 0
+    return {"tasks": tasks, "int8_ops_per_task": per, "int8_ops_total": sum(per.values()) * tasks,
+            "ops_per_task": per, "ops_total": sum(per.values()) * tasks}
 
 
 def error_stats(y, ref):

@@ -69,6 +69,28 @@ def test_split_three_radix_sub_fft():
     assert es <= ef
 
 
+@pytest.mark.parametrize("fi,fo,n,ch", CASES[:4])
+def test_f16_slices_give_the_int8_bytes(fi, fo, n, ch):
+    """The f16 form feeds the same 8-bit digits to kind::f16 MMAs with f32 accumulation; every digit product and
+    every accumulator is an integer below 2^24, so the sums are exact there too and the output is the same."""
+    x = np.random.default_rng(fi + n).uniform(-0.5, 0.5, (n, ch))
+    st = {}
+    a = kbsrc_b200.resample(x, fi, fo, mode="split")
+    b = kbsrc_b200.resample(x, fi, fo, mode="split16", stats=st)
+    assert st["isa"] == "sm_100a"
+    assert a.tobytes() == b.tobytes()
+
+
+def test_f16_slices_full_size_c2():
+    x = noise(2, 180, 96000, 2)
+    b = kbsrc_b200.resample(x, 96000, 44100, mode="split16")
+    e = kbsrc_b200.resample(x, 96000, 44100, mode="exact")
+    f = kbsrc_b200.resample(x, 96000, 44100, mode="fast")
+    eb, ef = error_stats(b, e), error_stats(f, e)
+    print(f"split16 {eb}\nfast    {ef}")
+    assert eb["max_abs"] <= ef["max_abs"]
+
+
 def test_split_runs_twice_the_same():
     x = np.random.default_rng(3).uniform(-0.5, 0.5, (30000, 2))
     cv = kbsrc_b200.Conversion(x, 96000, 44100, mode="split")
