@@ -174,7 +174,7 @@ __device__ __forceinline__ TaskSource task_source(const Work& w, long long task,
 // Complex input value i of a task: (x[2i], x[2i+1]) of the staged signal (fft.hpp:363), a buffer value, or a
 // dd real pair (kernel design).
 template <class Ar, int SRC>
-__device__ __forceinline__ CxR<Ar> load_input(const PassParams<Ar>& P, const TaskSource& ts, const CxR<Ar>* src,
+__device__ __forceinline__ CxR<Ar> load_input(const double* ddreal, const TaskSource& ts, const CxR<Ar>* src,
                                               long long i) {
     using R = typename Ar::R;
     if constexpr (SRC == kSrcSignal) {
@@ -191,12 +191,17 @@ __device__ __forceinline__ CxR<Ar> load_input(const PassParams<Ar>& P, const Tas
     } else if constexpr (SRC == kSrcComplex) {
         return src[i];
     } else if constexpr (Ar::kWide) {
-        const double2 a = __ldg(reinterpret_cast<const double2*>(P.ddreal) + 2 * i);
-        const double2 b = __ldg(reinterpret_cast<const double2*>(P.ddreal) + 2 * i + 1);
+        const double2 a = __ldg(reinterpret_cast<const double2*>(ddreal) + 2 * i);
+        const double2 b = __ldg(reinterpret_cast<const double2*>(ddreal) + 2 * i + 1);
         return CxR<Ar>{R{a.x, a.y}, R{b.x, b.y}};
     } else {
-        return CxR<Ar>{P.ddreal[4 * i], P.ddreal[4 * i + 2]};
+        return CxR<Ar>{ddreal[4 * i], ddreal[4 * i + 2]};
     }
+}
+template <class Ar, int SRC>
+__device__ __forceinline__ CxR<Ar> load_input(const PassParams<Ar>& P, const TaskSource& ts, const CxR<Ar>* src,
+                                              long long i) {
+    return load_input<Ar, SRC>(P.ddreal, ts, src, i);
 }
 
 template <class Ar>
@@ -220,41 +225,40 @@ __device__ __forceinline__ CxW<Ar>* twiddle_smem(unsigned char* after_planes) {
 // (fft.hpp:283-299). blockIdx.x: column group; blockIdx.y: task slot. Reading the staged signal, the two are
 // swapped (task slot fastest): the channels of a block are consecutive tasks, and their CTAs for one column group
 // then run side by side and share the interleaved input's sectors in L2.
+// One column-pass unit: sequences n2 in [c0, c0+F) of length N1 (stride N2) of one task's slot (src, dst), or of
+// the staged signal `ts` (SRC), through the sub-plan sp, then the four-step twiddle, stored in place. Shared by the
+// per-plan grid kernel and the batch queue kernel.
 template <class Ar, int SRC>
-__global__ void __launch_bounds__(Ar::kColMaxThreads, Ar::kColMinBlocks) k_column(const __grid_constant__ PassParams<Ar> P) {
-    extern __shared__ __align__(16) unsigned char smem[];
+__device__ __forceinline__ void column_unit(const SubPlan& sp, int N1, int N2, int F, int c0,
+                                            const CxW<Ar>* tw_stage, const CxW<Ar>* tw4,
+                                            const OddRoots<typename Ar::W>& odd, const CxR<Ar>* src, CxR<Ar>* dst,
+                                            const TaskSource& ts, const double* ddreal, unsigned char* smem) {
     using C = CxR<Ar>;
-    const int F = P.F, N1 = P.N1, N2 = P.N2, total = N1 * F;
+    const int total = N1 * F;
     const FastDiv dF = fast_div(F);
     Planes<Ar> A, B;
     unsigned char* rest = carve<Ar>(smem, total, A, B);
-    const unsigned slot = SRC == kSrcSignal ? blockIdx.x : blockIdx.y, group = SRC == kSrcSignal ? blockIdx.y : blockIdx.x;
-    const long long task = P.task0 + slot;
-    const int c0 = group * F;
-    const C* src = P.src + slot * P.stride;
-    C* dst = P.dst + slot * P.stride;
-    const TaskSource ts = SRC == kSrcSignal ? task_source(P.work, task, 2LL * N1 * N2) : TaskSource{};
-    const CxW<Ar>* tws = stage_twiddles<Ar>(P.sp, P.tw_stage, twiddle_smem<Ar>(rest));
+    const CxW<Ar>* tws = stage_twiddles<Ar>(sp, tw_stage, twiddle_smem<Ar>(rest));
     for (int e0 = threadIdx.x; e0 < total; e0 += kLoadBatch * blockDim.x) {
         C v[kLoadBatch];
 #pragma unroll
         for (int j = 0; j < kLoadBatch; j++) {
             const int e = e0 + j * blockDim.x, r = (int)fdiv(e, dF), n2 = c0 + (e - r * F);
-            if (e < total) v[j] = n2 < N2 ? load_input<Ar, SRC>(P, ts, src, (long long)r * N2 + n2) : czero<Ar>();
+            if (e < total) v[j] = n2 < N2 ? load_input<Ar, SRC>(ddreal, ts, src, (long long)r * N2 + n2) : czero<Ar>();
         }
 #pragma unroll
         for (int j = 0; j < kLoadBatch; j++)
             if (e0 + j * blockDim.x < total) A.st(e0 + j * blockDim.x, v[j]);
     }
     __syncthreads();
-    const Planes<Ar> res = stockham<Ar>(P.sp, A, B, F, tws, P.odd);
+    const Planes<Ar> res = stockham<Ar>(sp, A, B, F, tws, odd);
     // four-step twiddle and store; the table loads of a batch are issued before any of its products
     for (int e0 = threadIdx.x; e0 < total; e0 += kLoadBatch * blockDim.x) {
         CxW<Ar> w[kLoadBatch];
 #pragma unroll
         for (int j = 0; j < kLoadBatch; j++) {
             const int e = e0 + j * blockDim.x, k1 = (int)fdiv(e, dF), n2 = c0 + (e - k1 * F);
-            if (e < total && n2 < N2 && k1 && (Ar::kLanes || n2)) w[j] = ld_tw(P.tw4 + (long long)k1 * N2 + n2);
+            if (e < total && n2 < N2 && k1 && (Ar::kLanes || n2)) w[j] = ld_tw(tw4 + (long long)k1 * N2 + n2);
         }
 #pragma unroll
         for (int j = 0; j < kLoadBatch; j++) {
@@ -268,20 +272,31 @@ __global__ void __launch_bounds__(Ar::kColMaxThreads, Ar::kColMinBlocks) k_colum
     }
 }
 
+template <class Ar, int SRC>
+__global__ void __launch_bounds__(Ar::kColMaxThreads, Ar::kColMinBlocks) k_column(const __grid_constant__ PassParams<Ar> P) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const unsigned slot = SRC == kSrcSignal ? blockIdx.x : blockIdx.y, group = SRC == kSrcSignal ? blockIdx.y : blockIdx.x;
+    const long long task = P.task0 + slot;
+    const TaskSource ts = SRC == kSrcSignal ? task_source(P.work, task, 2LL * P.N1 * P.N2) : TaskSource{};
+    column_unit<Ar, SRC>(P.sp, P.N1, P.N2, P.F, (int)group * P.F, P.tw_stage, P.tw4, P.odd, P.src + slot * P.stride,
+                         P.dst + slot * P.stride, ts, P.ddreal, smem);
+}
+
 // Row pass: rows r in [r0, r0+F) of length N2 (contiguous), stored transposed to [N1*k2 + r]
 // (fft.hpp:300-311), or written straight to the output as real samples (fft.hpp:459-460).
+// One row-pass unit: rows r in [r0, r0+F) of length N2 of one task's slot through sp, stored transposed to
+// dst[N1*k2 + r], or written to the output as real samples (DST; `work` and the task place them). Shared by the
+// per-plan grid kernel and the batch queue kernel.
 template <class Ar, int DST>
-__global__ void __launch_bounds__(Ar::kMaxThreads, Ar::kMinBlocks) k_row(const __grid_constant__ PassParams<Ar> P) {
-    extern __shared__ __align__(16) unsigned char smem[];
+__device__ __forceinline__ void row_unit(const SubPlan& sp, int N1, int N2, int F, int r0, const CxW<Ar>* tw_stage,
+                                         const OddRoots<typename Ar::W>& odd, const CxR<Ar>* src, CxR<Ar>* dst,
+                                         const Work& work, long long task, unsigned char* smem) {
     using C = CxR<Ar>;
-    const int F = P.F, N1 = P.N1, N2 = P.N2, total = N2 * F;
+    const int total = N2 * F;
     const FastDiv dF = fast_div(F), dN2 = fast_div(N2);
     Planes<Ar> A, B;
     unsigned char* rest = carve<Ar>(smem, total, A, B);
-    const long long task = P.task0 + blockIdx.y;
-    const int r0 = blockIdx.x * F;
-    const C* src = P.src + blockIdx.y * P.stride;
-    const CxW<Ar>* tws = stage_twiddles<Ar>(P.sp, P.tw_stage, twiddle_smem<Ar>(rest));
+    const CxW<Ar>* tws = stage_twiddles<Ar>(sp, tw_stage, twiddle_smem<Ar>(rest));
     for (int e0 = threadIdx.x; e0 < total; e0 += kLoadBatch * blockDim.x) {
         C v[kLoadBatch];
 #pragma unroll
@@ -296,10 +311,9 @@ __global__ void __launch_bounds__(Ar::kMaxThreads, Ar::kMinBlocks) k_row(const _
         }
     }
     __syncthreads();
-    const Planes<Ar> res = stockham<Ar>(P.sp, A, B, F, tws, P.odd);
-    C* dst = P.dst + blockIdx.y * P.stride;
-    const TaskRef tr = DST == kDstOutput ? task_ref(P.work, task) : TaskRef{0, 0, 0};
-    const Item it = DST == kDstOutput ? item_of(P.work, tr) : Item{};
+    const Planes<Ar> res = stockham<Ar>(sp, A, B, F, tws, odd);
+    const TaskRef tr = DST == kDstOutput ? task_ref(work, task) : TaskRef{0, 0, 0};
+    const Item it = DST == kDstOutput ? item_of(work, tr) : Item{};
     for (int e = threadIdx.x; e < total; e += blockDim.x) {
         const int k2 = (int)fdiv(e, dF), f = e - k2 * F, row = r0 + f;
         if (row >= N1) continue;
@@ -309,10 +323,17 @@ __global__ void __launch_bounds__(Ar::kMaxThreads, Ar::kMinBlocks) k_row(const _
         if (DST == kDstComplex) {
             dst[iz] = v;
         } else {
-            emit(P.work, it, tr.c, tr.b, 2 * iz, Ar::to_f64(v.re));
-            emit(P.work, it, tr.c, tr.b, 2 * iz + 1, Ar::to_f64(Ar::neg(v.im)));
+            emit(work, it, tr.c, tr.b, 2 * iz, Ar::to_f64(v.re));
+            emit(work, it, tr.c, tr.b, 2 * iz + 1, Ar::to_f64(Ar::neg(v.im)));
         }
     }
+}
+
+template <class Ar, int DST>
+__global__ void __launch_bounds__(Ar::kMaxThreads, Ar::kMinBlocks) k_row(const __grid_constant__ PassParams<Ar> P) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    row_unit<Ar, DST>(P.sp, P.N1, P.N2, P.F, (int)blockIdx.x * P.F, P.tw_stage, P.odd, P.src + blockIdx.y * P.stride,
+                      P.dst + blockIdx.y * P.stride, P.work, P.task0 + blockIdx.y, smem);
 }
 
 // Whole FFT of n <= 2048 points in one CTA (the reference's direct SFFT path, fft.hpp:241-244,279).
@@ -413,15 +434,18 @@ struct SpecParams {
 
 // X[k] = (E + O w[k]) / 2 with E = z[k] + conj z[h-k], O = -i (z[k] - conj z[h-k]) (fft.hpp:365-408).
 // Double-double computes conjugate pairs together (one E, O for k and h-k); f64 computes each k alone.
+// Bins k = k0, k0 + step, ... <= k_end of one task's split (Z -> X); the last bin a task needs is split_last.
 template <class Ar>
-__global__ void k_split(const __grid_constant__ SpecParams<Ar> P) {
+__device__ __forceinline__ int split_last(int h) {
+    return Ar::kWide ? h / 2 : h - 1;
+}
+template <class Ar>
+__device__ __forceinline__ void split_range(const SpecParams<Ar>& P, const CxR<Ar>* Z, CxR<Ar>* X, int k0, int k_end,
+                                            int step) {
     using C = CxR<Ar>;
-    const C* Z = P.Z + blockIdx.y * P.stride;
-    C* X = P.X + blockIdx.y * P.stride;
     const int h = P.h;
     const typename Ar::R half = Ar::from_f64(0.5);
-    const int last = Ar::kWide ? h / 2 : h - 1;
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k <= last; k += gridDim.x * blockDim.x) {
+    for (int k = k0; k <= k_end; k += step) {
         if (k == 0) {
             const C z0 = Z[0];
             X[0] = C{Ar::add(z0.re, z0.im), Ar::zero()};
@@ -438,6 +462,12 @@ __global__ void k_split(const __grid_constant__ SpecParams<Ar> P) {
             X[j] = c_scale<Ar>(u, half);
         }
     }
+}
+
+template <class Ar>
+__global__ void k_split(const __grid_constant__ SpecParams<Ar> P) {
+    split_range<Ar>(P, P.Z + blockIdx.y * P.stride, P.X + blockIdx.y * P.stride, blockIdx.x * blockDim.x + threadIdx.x,
+                    split_last<Ar>(P.h), gridDim.x * blockDim.x);
 }
 
 template <class W>
@@ -502,13 +532,11 @@ __device__ __forceinline__ CxR<Ar> spectrum_bin(const SpecParams<Ar>& P, const C
 // Inverse merge z[k] = conj(E + i D), E = Y[k] + conj Y[hi-k], D = (Y[k] - conj Y[hi-k]) conj w[k]
 // (fft.hpp:411-458); pairs in dd, each k alone in f64.
 template <class Ar>
-__global__ void k_merge(const __grid_constant__ SpecParams<Ar> P) {
+__device__ __forceinline__ void merge_range(const SpecParams<Ar>& P, const CxR<Ar>* X, CxR<Ar>* Zi, int k0, int k_end,
+                                            int step) {
     using C = CxR<Ar>;
-    const C* X = P.X + blockIdx.y * P.stride;
-    C* Zi = P.Zi + blockIdx.y * P.stride;
     const int hi = P.hi;
-    const int last = Ar::kWide ? hi / 2 : hi - 1;
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k <= last; k += gridDim.x * blockDim.x) {
+    for (int k = k0; k <= k_end; k += step) {
         const int j = hi - k;
         const C a = spectrum_bin<Ar>(P, X, k), bb = c_conj<Ar>(spectrum_bin<Ar>(P, X, j));
         const C E = c_add<Ar>(a, bb), split = c_sub<Ar>(a, bb);
@@ -524,6 +552,12 @@ __global__ void k_merge(const __grid_constant__ SpecParams<Ar> P) {
             Zi[j] = c_conj<Ar>(u);
         }
     }
+}
+
+template <class Ar>
+__global__ void k_merge(const __grid_constant__ SpecParams<Ar> P) {
+    merge_range<Ar>(P, P.X + blockIdx.y * P.stride, P.Zi + blockIdx.y * P.stride, blockIdx.x * blockDim.x + threadIdx.x,
+                    split_last<Ar>(P.hi), gridDim.x * blockDim.x);
 }
 
 // dd / double (double_double.hpp:80-84) with IEEE division
@@ -546,6 +580,155 @@ __device__ __forceinline__ dd div_dd_f64(dd a, double b) {
 __global__ void k_design_out(const __grid_constant__ SpecParams<ArDDAccurate> P) {
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k <= P.h; k += gridDim.x * blockDim.x)
         P.Hout[k] = div_dd_f64(P.X[k].re, P.scale);
+}
+
+// ------------------------------------------------------------------------------------------------------
+// batch queue: the tasks of every plan group of a batch wave through one persistent launch per pass
+// ------------------------------------------------------------------------------------------------------
+// The reference hands (channel, block) tasks to its workers through one atomic counter (src/resampler.cpp:42-49,
+// src/parallel.cpp:9-32). Here each pass of a batch wave is one persistent launch whose CTAs take work units from
+// an atomic counter: a unit is one column or row group of one task, or a range of spectrum bins, of any plan group.
+// Units are listed largest transform first, so the long units start early and the short ones fill in at the end.
+
+// One plan group as the queue kernels read it (four-step forward and inverse transforms, split/merge roots,
+// kernel spectrum, block hop); W: the table type.
+struct QueueGroup {
+    SubPlan fs1, fs2, is1, is2;
+    int fN1, fN2, iN1, iN2;
+    int fcF, frF, icF, irF;  // sequences per unit: forward column, forward row, inverse column, inverse row
+    const void* ftw_stage;
+    const void* ftw4;
+    const void* itw_stage;
+    const void* itw4;
+    const void* w_fw;
+    const void* w_iv;
+    const void* H;
+    int h, hi, Nb, Mb, up, Jg;
+    long long hopQ, hopP, margP;
+};
+// One task of a wave: its conversion, channel and block, its plan group, and its slot in the wave buffers (the
+// first complex element of its slot; slots of different groups have different sizes).
+struct QueueTask {
+    TaskRef ref;
+    int group;
+    long long slot;
+};
+struct QueueUnit {
+    int task, unit;
+};
+constexpr int kQueueBins = 1024;      // spectrum bins per split or merge unit
+constexpr int kQueueBinThreads = 256;
+
+template <class W>
+struct QueueParams {
+    const QueueGroup* groups;
+    const QueueTask* tasks;
+    const QueueUnit* units;
+    int nunits;
+    int* counter;       // next unit (zero before the launch)
+    const Item* items;  // the batch's conversions
+    void* A;            // wave buffers
+    void* B;
+    OddRoots<W> odd;
+};
+
+// The next unit for this CTA (the whole CTA agrees on it; the previous unit's shared memory is free again).
+__device__ __forceinline__ int queue_next(int* counter, int* slot) {
+    __syncthreads();
+    if (threadIdx.x == 0) *slot = atomicAdd(counter, 1);
+    __syncthreads();
+    return *slot;
+}
+
+// The Work view of one queue task: its conversion as the only item (task = b * ch + c), the group's hop.
+__device__ __forceinline__ Work queue_work(const QueueGroup& g, const Item* items, const QueueTask& t, long long& task) {
+    Work w{};
+    w.item0 = items[t.ref.item];
+    w.hopQ = g.hopQ;
+    w.hopP = g.hopP;
+    w.margP = g.margP;
+    task = t.ref.b * w.item0.ch + t.ref.c;
+    return w;
+}
+
+// Column pass: forward (reads the signal, writes buffer A in place) or inverse (buffer B in place).
+template <class Ar, int SRC, bool FWD>
+__global__ void __launch_bounds__(Ar::kColMaxThreads, Ar::kColMinBlocks)
+    k_column_q(const __grid_constant__ QueueParams<typename Ar::W> Q) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ int next;
+    using C = CxR<Ar>;
+    for (;;) {
+        const int u = queue_next(Q.counter, &next);
+        if (u >= Q.nunits) break;
+        const QueueUnit qu = Q.units[u];
+        const QueueTask t = Q.tasks[qu.task];
+        const QueueGroup& g = Q.groups[t.group];
+        const int N1 = FWD ? g.fN1 : g.iN1, N2 = FWD ? g.fN2 : g.iN2, F = FWD ? g.fcF : g.icF;
+        C* x = static_cast<C*>(FWD ? Q.A : Q.B) + t.slot;
+        long long task;
+        const Work w = queue_work(g, Q.items, t, task);
+        const TaskSource ts = SRC == kSrcSignal ? task_source(w, task, 2LL * N1 * N2) : TaskSource{};
+        column_unit<Ar, SRC>(FWD ? g.fs1 : g.is1, N1, N2, F, qu.unit * F,
+                             static_cast<const CxW<Ar>*>(FWD ? g.ftw_stage : g.itw_stage),
+                             static_cast<const CxW<Ar>*>(FWD ? g.ftw4 : g.itw4), Q.odd, x, x, ts, nullptr, smem);
+    }
+}
+
+// Row pass: forward (buffer A to B, natural order) or inverse (buffer B to the output samples).
+template <class Ar, int DST, bool FWD>
+__global__ void __launch_bounds__(Ar::kMaxThreads, Ar::kMinBlocks)
+    k_row_q(const __grid_constant__ QueueParams<typename Ar::W> Q) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ int next;
+    using C = CxR<Ar>;
+    for (;;) {
+        const int u = queue_next(Q.counter, &next);
+        if (u >= Q.nunits) break;
+        const QueueUnit qu = Q.units[u];
+        const QueueTask t = Q.tasks[qu.task];
+        const QueueGroup& g = Q.groups[t.group];
+        const int N1 = FWD ? g.fN1 : g.iN1, N2 = FWD ? g.fN2 : g.iN2, F = FWD ? g.frF : g.irF;
+        long long task;
+        const Work w = queue_work(g, Q.items, t, task);
+        const C* src = static_cast<const C*>(FWD ? Q.A : Q.B) + t.slot;
+        C* dst = static_cast<C*>(Q.B) + t.slot;
+        row_unit<Ar, DST>(FWD ? g.fs2 : g.is2, N1, N2, F, qu.unit * F,
+                          static_cast<const CxW<Ar>*>(FWD ? g.ftw_stage : g.itw_stage), Q.odd, src, dst, w, task, smem);
+    }
+}
+
+template <class Ar>
+__device__ __forceinline__ SpecParams<Ar> queue_spec(const QueueGroup& g) {
+    SpecParams<Ar> s{};
+    s.w_fw = static_cast<const CxW<Ar>*>(g.w_fw);
+    s.w_iv = static_cast<const CxW<Ar>*>(g.w_iv);
+    s.H = static_cast<const typename Ar::W*>(g.H);
+    s.h = g.h; s.hi = g.hi; s.Nb = g.Nb; s.Mb = g.Mb; s.up = g.up; s.Jg = g.Jg;
+    return s;
+}
+
+// Real-FFT split (buffer B to A, bins of one unit) or spectrum multiply and merge (buffer A to B).
+template <class Ar, bool SPLIT>
+__global__ void __launch_bounds__(kQueueBinThreads) k_bins_q(const __grid_constant__ QueueParams<typename Ar::W> Q) {
+    __shared__ int next;
+    using C = CxR<Ar>;
+    for (;;) {
+        const int u = queue_next(Q.counter, &next);
+        if (u >= Q.nunits) break;
+        const QueueUnit qu = Q.units[u];
+        const QueueTask t = Q.tasks[qu.task];
+        const QueueGroup& g = Q.groups[t.group];
+        const SpecParams<Ar> sp = queue_spec<Ar>(g);
+        const int k0 = qu.unit * kQueueBins, last = split_last<Ar>(SPLIT ? g.h : g.hi);
+        const int k_end = min(last, k0 + kQueueBins - 1);
+        if (SPLIT)
+            split_range<Ar>(sp, static_cast<const C*>(Q.B) + t.slot, static_cast<C*>(Q.A) + t.slot,
+                            k0 + (int)threadIdx.x, k_end, blockDim.x);
+        else
+            merge_range<Ar>(sp, static_cast<const C*>(Q.A) + t.slot, static_cast<C*>(Q.B) + t.slot,
+                            k0 + (int)threadIdx.x, k_end, blockDim.x);
+    }
 }
 
 // ------------------------------------------------------------------------------------------------------
@@ -1205,11 +1388,27 @@ struct BatchGroup : PlanCore {
     std::vector<int> members;
     long long tasks = 0, stride = 0, wave = 0;
     DevBuf refs;  // TaskRef[tasks]
+    bool queued = false;  // runs through the batch queue (else its own launches)
+};
+
+// A wave of the batch queue: tasks of any groups, largest transform first, and the units of each pass.
+struct QueueWave {
+    long long ntasks = 0;
+    DevBuf tasks;                 // QueueTask[ntasks]
+    DevBuf units[6];              // QueueUnit lists: forward column, forward row, split, merge, inverse column, row
+    int nunits[6] = {};
 };
 
 struct kbsrc_gpu_batch {
     std::vector<kbsrc_gpu_desc> descs;  // per conversion (H not kept)
     std::vector<std::unique_ptr<BatchGroup>> groups;
+    bool queued = false;                // some groups run through the queue kernels
+    bool q_exact = false;               // their arithmetic: double-double (else float64)
+    DevBuf q_groups;                    // QueueGroup[queued groups]
+    std::vector<QueueWave> q_waves;
+    DevBuf q_counters;                  // int[waves * 6], zeroed at the start of every run
+    int q_threads[6] = {}, q_ctas[6] = {};
+    size_t q_smem[6] = {};
     std::vector<int> group_of;          // conversion -> group, -1 when it has no tasks
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -1312,6 +1511,14 @@ int allow_large_smem() {
     KB_SMEM((k_direct<ArX80, kSrcSignal, kDstComplex>));
     KB_SMEM((k_direct<ArX80, kSrcComplex, kDstComplex>));
     KB_SMEM((k_direct<ArX80, kSrcComplex, kDstOutput>));
+    KB_SMEM((k_column_q<ArDDShort, kSrcSignal, true>));
+    KB_SMEM((k_column_q<ArDDShort, kSrcComplex, false>));
+    KB_SMEM((k_row_q<ArDDShort, kDstComplex, true>));
+    KB_SMEM((k_row_q<ArDDShort, kDstOutput, false>));
+    KB_SMEM((k_column_q<ArF64, kSrcSignal, true>));
+    KB_SMEM((k_column_q<ArF64, kSrcComplex, false>));
+    KB_SMEM((k_row_q<ArF64, kDstComplex, true>));
+    KB_SMEM((k_row_q<ArF64, kDstOutput, false>));
     KB_SMEM((k_tc_column<TcI8, kSrcSignal, kDstComplex>));
     KB_SMEM((k_tc_column<TcI8, kSrcComplex, kDstComplex>));
     KB_SMEM((k_tc_column<TcI8, kSrcComplex, kDstOutput>));
@@ -2217,6 +2424,164 @@ bool same_plan(const kbsrc_gpu_desc& a, const kbsrc_gpu_desc& b) {
     return a.H == b.H || std::memcmp(a.H, b.H, (size_t)a.H_len * 16) == 0;
 }
 
+// Whether a group can run through the queue kernels: double-double or float64, both transforms four-step and
+// 7-smooth (no direct or Bluestein transform).
+bool queue_eligible(const BatchGroup& g) {
+    if (g.split || g.tab == kTabX80) return false;
+    return g.fw.host.four && !g.fw.m && g.iv.host.four && !g.iv.m;
+}
+
+template <class K>
+int queue_ctas(K kernel, int threads, size_t smem, int sms, int& ctas) {
+    int per = 0;
+    KB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, smem));
+    ctas = std::max(1, per) * sms;
+    return KBSRC_GPU_OK;
+}
+
+// Builds the batch queue of the eligible groups of the first eligible group's arithmetic (KBSRC_GPU_QUEUE=0 keeps
+// every group on its own launches): the group table, waves of their tasks (largest transform first) within the slot
+// buffers, each pass's units. The other groups run their own launches after the queue.
+int build_queue(kbsrc_gpu_batch& b) {
+    if (b.groups.empty() || !env_int("KBSRC_GPU_QUEUE", 1)) return KBSRC_GPU_OK;
+    std::vector<int> qi;  // queued groups in the batch's group order
+    for (size_t i = 0; i < b.groups.size(); i++)
+        if (queue_eligible(*b.groups[i]) && (qi.empty() || b.groups[i]->exact == b.groups[qi[0]]->exact))
+            qi.push_back((int)i);
+    if (qi.empty()) return KBSRC_GPU_OK;
+    const bool exact = b.groups[qi[0]]->exact;
+    const size_t es = b.groups[qi[0]]->esize();
+    std::vector<QueueGroup> qg(qi.size());
+    int T[6] = {}, sms = 0;
+    size_t S[6] = {};
+    for (size_t i = 0; i < qi.size(); i++) {
+        const BatchGroup& g = *b.groups[qi[i]];
+        QueueGroup& q = qg[i];
+        q.fs1 = g.fw.host.s1; q.fs2 = g.fw.host.s2; q.is1 = g.iv.host.s1; q.is2 = g.iv.host.s2;
+        q.fN1 = g.fw.host.N1; q.fN2 = g.fw.host.N2; q.iN1 = g.iv.host.N1; q.iN2 = g.iv.host.N2;
+        q.fcF = g.fw.col.F; q.frF = g.fw.row.F; q.icF = g.iv.col.F; q.irF = g.iv.row.F;
+        q.ftw_stage = g.fw.tw_stage.p; q.ftw4 = g.fw.tw4.p; q.itw_stage = g.iv.tw_stage.p; q.itw4 = g.iv.tw4.p;
+        q.w_fw = g.w_fw.p; q.w_iv = g.w_iv.p; q.H = g.H.p;
+        q.h = g.hf; q.hi = g.hi; q.Nb = g.Nb; q.Mb = g.Mb; q.up = g.d.up; q.Jg = g.d.Jg;
+        q.hopQ = (long long)g.hop * g.d.Q; q.hopP = (long long)g.hop * g.d.P; q.margP = (long long)g.d.marg * g.d.P;
+        const Shape sh[4] = {g.fw.col, g.fw.row, g.iv.col, g.iv.row};
+        const int pass[4] = {0, 1, 4, 5};
+        for (int k = 0; k < 4; k++) {
+            T[pass[k]] = std::max(T[pass[k]], sh[k].T);
+            S[pass[k]] = std::max(S[pass[k]], sh[k].smem);
+        }
+    }
+    T[2] = T[3] = kQueueBinThreads;
+    int rc;
+    if ((rc = b.q_groups.alloc(qg.size() * sizeof(QueueGroup))) != KBSRC_GPU_OK) return rc;
+    KB_CUDA(cudaMemcpy(b.q_groups.p, qg.data(), qg.size() * sizeof(QueueGroup), cudaMemcpyHostToDevice));
+    // every task, largest forward transform first (ties: group, then the group's own block-major order)
+    struct Pending {
+        int group;
+        TaskRef ref;
+    };
+    std::vector<Pending> all;
+    for (size_t k = 0; k < qi.size(); k++)
+        for (int i : b.groups[qi[k]]->members)
+            for (long long blk = 0; blk < b.descs[i].nblk; blk++)
+                for (int c = 0; c < b.descs[i].channels; c++) all.push_back(Pending{(int)k, TaskRef{i, c, blk}});
+    std::stable_sort(all.begin(), all.end(), [&](const Pending& x, const Pending& y) {
+        return b.groups[qi[x.group]]->hf > b.groups[qi[y.group]]->hf;
+    });
+    const long long budget = (long long)b.bufA.bytes;
+    size_t at = 0;
+    while (at < all.size()) {
+        std::vector<QueueTask> tasks;
+        long long used = 0;
+        while (at < all.size()) {
+            const BatchGroup& g = *b.groups[qi[all[at].group]];
+            const long long bytes = g.stride * (long long)es;
+            if (!tasks.empty() && used + bytes > budget) break;
+            tasks.push_back(QueueTask{all[at].ref, all[at].group, used / (long long)es});
+            used += bytes;
+            at++;
+        }
+        QueueWave w;
+        w.ntasks = (long long)tasks.size();
+        std::vector<QueueUnit> units[6];
+        for (int ti = 0; ti < (int)tasks.size(); ti++) {
+            const QueueGroup& q = qg[tasks[ti].group];
+            const int split_last_bin = exact ? q.h / 2 : q.h - 1, merge_last_bin = exact ? q.hi / 2 : q.hi - 1;
+            const int n[6] = {(q.fN2 + q.fcF - 1) / q.fcF, (q.fN1 + q.frF - 1) / q.frF,
+                              split_last_bin / kQueueBins + 1, merge_last_bin / kQueueBins + 1,
+                              (q.iN2 + q.icF - 1) / q.icF, (q.iN1 + q.irF - 1) / q.irF};
+            for (int p = 0; p < 6; p++)
+                for (int u = 0; u < n[p]; u++) units[p].push_back(QueueUnit{ti, u});
+        }
+        if ((rc = w.tasks.alloc(tasks.size() * sizeof(QueueTask))) != KBSRC_GPU_OK) return rc;
+        KB_CUDA(cudaMemcpy(w.tasks.p, tasks.data(), tasks.size() * sizeof(QueueTask), cudaMemcpyHostToDevice));
+        for (int p = 0; p < 6; p++) {
+            w.nunits[p] = (int)units[p].size();
+            if ((rc = w.units[p].alloc(units[p].size() * sizeof(QueueUnit))) != KBSRC_GPU_OK) return rc;
+            KB_CUDA(cudaMemcpy(w.units[p].p, units[p].data(), units[p].size() * sizeof(QueueUnit),
+                               cudaMemcpyHostToDevice));
+        }
+        b.q_waves.push_back(std::move(w));
+    }
+    if ((rc = b.q_counters.alloc(b.q_waves.size() * 6 * sizeof(int))) != KBSRC_GPU_OK) return rc;
+    KB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b.device));
+    for (int p = 0; p < 6; p++) {
+        b.q_threads[p] = T[p];
+        b.q_smem[p] = S[p];
+    }
+    if (exact) {
+        if ((rc = queue_ctas(k_column_q<ArDDShort, kSrcSignal, true>, T[0], S[0], sms, b.q_ctas[0])) ||
+            (rc = queue_ctas(k_row_q<ArDDShort, kDstComplex, true>, T[1], S[1], sms, b.q_ctas[1])) ||
+            (rc = queue_ctas(k_bins_q<ArDDAccurate, true>, T[2], 0, sms, b.q_ctas[2])) ||
+            (rc = queue_ctas(k_bins_q<ArDDAccurate, false>, T[3], 0, sms, b.q_ctas[3])) ||
+            (rc = queue_ctas(k_column_q<ArDDShort, kSrcComplex, false>, T[4], S[4], sms, b.q_ctas[4])) ||
+            (rc = queue_ctas(k_row_q<ArDDShort, kDstOutput, false>, T[5], S[5], sms, b.q_ctas[5])))
+            return rc;
+    } else {
+        if ((rc = queue_ctas(k_column_q<ArF64, kSrcSignal, true>, T[0], S[0], sms, b.q_ctas[0])) ||
+            (rc = queue_ctas(k_row_q<ArF64, kDstComplex, true>, T[1], S[1], sms, b.q_ctas[1])) ||
+            (rc = queue_ctas(k_bins_q<ArF64, true>, T[2], 0, sms, b.q_ctas[2])) ||
+            (rc = queue_ctas(k_bins_q<ArF64, false>, T[3], 0, sms, b.q_ctas[3])) ||
+            (rc = queue_ctas(k_column_q<ArF64, kSrcComplex, false>, T[4], S[4], sms, b.q_ctas[4])) ||
+            (rc = queue_ctas(k_row_q<ArF64, kDstOutput, false>, T[5], S[5], sms, b.q_ctas[5])))
+            return rc;
+    }
+    for (int i : qi) b.groups[i]->queued = true;
+    b.q_exact = exact;
+    b.queued = true;
+    return KBSRC_GPU_OK;
+}
+
+// One wave's six queue launches; every unit counter of the run was zeroed before the first.
+template <class ArL, class ArS>
+int enqueue_queue_wave(const kbsrc_gpu_batch& b, size_t wi, cudaStream_t st, Trail& tr) {
+    const QueueWave& w = b.q_waves[wi];
+    int* counters = static_cast<int*>(b.q_counters.p) + 6 * wi;
+    QueueParams<typename ArL::W> q{};
+    q.groups = static_cast<const QueueGroup*>(b.q_groups.p);
+    q.tasks = static_cast<const QueueTask*>(w.tasks.p);
+    q.items = static_cast<const Item*>(b.items.p);
+    q.A = b.bufA.p;
+    q.B = b.bufB.p;
+    q.odd = odd_table<typename ArL::W>();
+    auto set = [&](int p) {
+        q.units = static_cast<const QueueUnit*>(w.units[p].p);
+        q.nunits = w.nunits[p];
+        q.counter = counters + p;
+    };
+    auto launch = [&](auto kernel, int p) -> int {
+        set(p);
+        kernel<<<b.q_ctas[p], b.q_threads[p], b.q_smem[p], st>>>(q);
+        return tr.mark(st, p);
+    };
+    int rc;
+    if ((rc = launch(k_column_q<ArL, kSrcSignal, true>, 0)) || (rc = launch(k_row_q<ArL, kDstComplex, true>, 1)) ||
+        (rc = launch(k_bins_q<ArS, true>, 2)) || (rc = launch(k_bins_q<ArS, false>, 3)) ||
+        (rc = launch(k_column_q<ArL, kSrcComplex, false>, 4)) || (rc = launch(k_row_q<ArL, kDstOutput, false>, 5)))
+        return rc;
+    return KBSRC_GPU_OK;
+}
+
 int batch_create_impl(const kbsrc_gpu_desc* descs, int count, kbsrc_gpu_batch** out) {
     if (!descs || count < 1) return fail(KBSRC_GPU_E_ARG, "empty batch");
     int rc;
@@ -2274,6 +2639,7 @@ int batch_create_impl(const kbsrc_gpu_desc* descs, int count, kbsrc_gpu_batch** 
     }
     if ((rc = b.items.alloc((size_t)count * sizeof(Item))) != KBSRC_GPU_OK) return rc;
     KB_CUDA(cudaMallocHost(&b.items_host, (size_t)count * sizeof(Item)));
+    if ((rc = build_queue(b)) != KBSRC_GPU_OK) return rc;
     *out = bp.release();
     return KBSRC_GPU_OK;
 }
@@ -2287,8 +2653,17 @@ int batch_enqueue(kbsrc_gpu_batch& b, cudaStream_t st, Trail& tr) {
     k_zero_items<<<dim3(grid_for(most, 256), count), 256, 0, st>>>(static_cast<const Item*>(b.items.p), count);
     int rc;
     if ((rc = tr.mark(st, -2)) != KBSRC_GPU_OK) return rc;
+    if (b.queued) {
+        KB_CUDA(cudaMemsetAsync(b.q_counters.p, 0, b.q_counters.bytes, st));
+        for (size_t wi = 0; wi < b.q_waves.size(); wi++) {
+            rc = b.q_exact ? enqueue_queue_wave<ArDDShort, ArDDAccurate>(b, wi, st, tr)
+                           : enqueue_queue_wave<ArF64, ArF64>(b, wi, st, tr);
+            if (rc) return rc;
+        }
+    }
     for (auto& gp : b.groups) {
         const BatchGroup& g = *gp;
+        if (g.queued) continue;
         Work w{};
         w.items = static_cast<const Item*>(b.items.p);
         w.refs = static_cast<const TaskRef*>(g.refs.p);
@@ -3198,6 +3573,11 @@ int kbsrc_gpu_batch_info(const kbsrc_gpu_batch* b, long long* groups, long long*
     for (const auto& g : b->groups) {
         t += g->tasks;
         l += plan_launches(*g) * ((g->tasks + g->wave - 1) / g->wave);
+    }
+    if (b->queued) {
+        l = 6 * (long long)b->q_waves.size();
+        for (const auto& g : b->groups)
+            if (!g->queued) l += plan_launches(*g) * ((g->tasks + g->wave - 1) / g->wave);
     }
     if (groups) *groups = (long long)b->groups.size();
     if (tasks) *tasks = t;

@@ -59,3 +59,25 @@ def test_batch_device_run_with_new_buffers():
         torch.cuda.synchronize()
         for o, w, n in zip(d_o, want, b.nout):
             assert o.cpu().numpy().reshape(-1, n).tobytes() == w.tobytes()
+
+
+@pytest.mark.parametrize("mode", ["exact", "fast"])
+def test_queue_equals_group_launches(mode, monkeypatch):
+    """The batch queue (one persistent launch per pass and wave over all groups' tasks) against each group run on
+    its own launches (KBSRC_GPU_QUEUE=0): the same bytes per file, in fewer launches. The queue holds the groups
+    with four-step 7-smooth transforms; the short files' direct transforms run on their own launches after it."""
+    rng = np.random.default_rng(21)
+    items = [(rng.uniform(-0.5, 0.5, (n, ch)), fi, fo) for n, ch, fi, fo in
+             [(400000, 2, 96000, 44100), (300000, 1, 48000, 96000), (250000, 3, 44100, 48000),
+              (500000, 1, 192000, 44100), (120000, 2, 88200, 48000), (2000, 1, 48000, 44100),
+              (60000, 2, 48000, 48000), (350000, 2, 96000, 44100)]]
+    queued = kbsrc_b200.Batch(items, mode=mode)
+    monkeypatch.setenv("KBSRC_GPU_QUEUE", "0")
+    grouped = kbsrc_b200.Batch(items, mode=mode)
+    a, b = queued.run(), grouped.run()
+    assert all(x.tobytes() == y.tobytes() for x, y in zip(a, b))
+    assert queued.gpu_info()["launches"] < grouped.gpu_info()["launches"]
+    for (x, fi, fo), y in zip(items[:2], a[:2]):
+        assert y.tobytes() == kbsrc_b200.resample(x, fi, fo, mode=mode).tobytes()
+    queued.close()
+    grouped.close()
