@@ -1485,7 +1485,14 @@ int allow_large_smem() {
     cudaFuncAttributes fa{};
     KB_CUDA(cudaFuncGetAttributes(&fa, (const void*)k_tc_row<TcF16, kDstOutput>));
     if (fa.maxDynamicSharedSizeBytes >= mx) return KBSRC_GPU_OK;
-#define KB_SMEM(k) KB_CUDA(cudaFuncSetAttribute((const void*)(k), cudaFuncAttributeMaxDynamicSharedMemorySize, mx))
+    // the dynamic limit is what the static shared memory of the kernel leaves of the opt-in maximum
+#define KB_SMEM(k)                                                                                          \
+    do {                                                                                                    \
+        cudaFuncAttributes ka{};                                                                            \
+        KB_CUDA(cudaFuncGetAttributes(&ka, (const void*)(k)));                                              \
+        KB_CUDA(cudaFuncSetAttribute((const void*)(k), cudaFuncAttributeMaxDynamicSharedMemorySize,          \
+                                     mx - (int)ka.sharedSizeBytes));                                        \
+    } while (0)
     KB_SMEM((k_column<ArF64, kSrcSignal>));
     KB_SMEM((k_column<ArF64, kSrcComplex>));
     KB_SMEM((k_column<ArDDShort, kSrcSignal>));
