@@ -747,18 +747,21 @@ struct TcParams {
 // n2 in [c0, c0+F) of length N1 (stride N2) through the sub-FFT, its first stage reading the input straight from
 // global memory and its last stage storing, with the four-step twiddle, straight to global memory (in place);
 // with N2 == 1 the single column is the whole transform and DST may write it as output samples. S: the digit
-// slices' element kind (TcI8 or TcF16).
-template <class S, int SRC, int DST>
+// slices' element kind (TcI8 or TcF16). H: items in flight per CTA (1, or 2: one per half of the CTA, which take
+// alternate items of the CTA's share).
+template <class S, int SRC, int DST, int H>
 __global__ void __launch_bounds__(kTcThreads, 1)
     k_tc_column(const __grid_constant__ PassParams<ArF64> P, const __grid_constant__ TcParams T) {
     extern __shared__ __align__(16) unsigned char smem[];
     using C = CxR<ArF64>;
+    constexpr int kT = kTcThreads / H;
     const int F = T.sub.F, N1 = T.N1, N2 = T.N2, groups = (N2 + F - 1) / F;
-    Planes<ArF64> X, Y;
-    const TcSmem m = tc_carve(carve<ArF64>(smem, N1 * F, X, Y), T.sub);
+    const TcSmem m = tc_carve(smem, T.sub);
     const uint32_t tmem = tc_setup(m, T.sub);
+    const TcHalf hf = tc_half(m, T.sub, H == 2 ? (int)(threadIdx.x >> 8) : 0, tmem);
     uint32_t phase = 0;
-    for (long long item = blockIdx.x; item < (long long)groups * T.slots; item += gridDim.x) {
+    for (long long item = blockIdx.x + (long long)hf.id * gridDim.x; item < (long long)groups * T.slots;
+         item += (long long)H * gridDim.x) {
         // reading the signal, the task slot varies fastest: the channels of a block share input sectors in L2
         const int slot = SRC == kSrcSignal ? (int)(item % T.slots) : (int)(item / groups);
         const int c0 = (SRC == kSrcSignal ? (int)(item / T.slots) : (int)(item - (long long)slot * groups)) * F;
@@ -768,8 +771,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         const TaskSource ts = SRC == kSrcSignal ? task_source(P.work, task, 2LL * N1 * N2) : TaskSource{};
         const TaskRef tr = DST == kDstOutput ? task_ref(P.work, task) : TaskRef{0, 0, 0};
         const Item it = DST == kDstOutput ? item_of(P.work, tr) : Item{};
-        tc_subfft<S>(
-            T.sub, true, X, Y, m, tmem, phase, T.err,
+        tc_subfft<S, kT>(
+            T.sub, true, hf, phase, T.err,
             [&](int n, int f) {
                 const int n2 = c0 + f;
                 if (n2 >= N2) return make_double2(0.0, 0.0);
@@ -790,31 +793,33 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 }
             });
     }
-    tc_teardown(T.sub, tmem);
+    tc_teardown(tmem);
 }
 
 // Row pass, persistent like the column pass: items (row group g, task slot y); an item transforms rows r in
 // [r0, r0+F) of length N2 (its first stage reading them from global memory, neighbouring rows of the MMA taking
 // neighbouring inputs) and stores them transposed to [N1*k2 + r], or writes them as output samples.
-template <class S, int DST>
+template <class S, int DST, int H>
 __global__ void __launch_bounds__(kTcThreads, 1)
     k_tc_row(const __grid_constant__ PassParams<ArF64> P, const __grid_constant__ TcParams T) {
     extern __shared__ __align__(16) unsigned char smem[];
     using C = CxR<ArF64>;
+    constexpr int kT = kTcThreads / H;
     const int F = T.sub.F, N1 = T.N1, N2 = T.N2, groups = (N1 + F - 1) / F;
-    Planes<ArF64> X, Y;
-    const TcSmem m = tc_carve(carve<ArF64>(smem, N2 * F, X, Y), T.sub);
+    const TcSmem m = tc_carve(smem, T.sub);
     const uint32_t tmem = tc_setup(m, T.sub);
+    const TcHalf hf = tc_half(m, T.sub, H == 2 ? (int)(threadIdx.x >> 8) : 0, tmem);
     uint32_t phase = 0;
-    for (long long item = blockIdx.x; item < (long long)groups * T.slots; item += gridDim.x) {
+    for (long long item = blockIdx.x + (long long)hf.id * gridDim.x; item < (long long)groups * T.slots;
+         item += (long long)H * gridDim.x) {
         const int slot = (int)(item / groups), r0 = (int)(item - (long long)slot * groups) * F;
         const long long task = P.task0 + slot;
         const C* src = P.src + slot * P.stride;
         C* dst = P.dst + slot * P.stride;
         const TaskRef tr = DST == kDstOutput ? task_ref(P.work, task) : TaskRef{0, 0, 0};
         const Item it = DST == kDstOutput ? item_of(P.work, tr) : Item{};
-        tc_subfft<S>(
-            T.sub, false, X, Y, m, tmem, phase, T.err,
+        tc_subfft<S, kT>(
+            T.sub, false, hf, phase, T.err,
             [&](int n, int f) {
                 const int row = r0 + f;
                 if (row >= N1) return make_double2(0.0, 0.0);
@@ -833,7 +838,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 }
             });
     }
-    tc_teardown(T.sub, tmem);
+    tc_teardown(tmem);
 }
 
 // ------------------------------------------------------------------------------------------------------
@@ -1181,7 +1186,14 @@ bool tc_factor3(int N, int& Ra, int& Rb, int& Rc) {
     return best > 0;
 }
 int tc_kh(int R) { return R <= 16 ? 16 : 32; }
-int tc_nh(int R) { return R <= 16 ? 16 : R <= 24 ? 24 : 32; }
+// Output columns per half of the matrix (real, imaginary): 16, 24 or 32; with two CTA halves a radix above 16 runs
+// in two rounds of nh columns, and an MMA's N (blocks of nh) must stay a multiple of 16, so 24 becomes 32.
+int tc_nh(int R, int halves) { return R <= 16 ? 16 : R <= 24 && halves == 1 ? 24 : 32; }
+TcRadix tc_radix(int R, int halves) {
+    if (R <= 1) return TcRadix{1, 0, 0, 1, nullptr};
+    const int nh = tc_nh(R, halves);
+    return TcRadix{R, tc_kh(R), nh, tc_rounds_for(nh, halves), nullptr};
+}
 
 // f16 bits of a small integer v (|v| <= 128): exact
 uint16_t f16_bits(int v) {
@@ -1196,17 +1208,20 @@ uint16_t f16_bits(int v) {
 // The real form of DFT_R (outputs n: real parts, then imaginary parts from nh; inputs k: real parts, then
 // imaginary parts from kh), y_re[k1] = sum_j xr_j cos + xi_j sin, y_im[k1] = sum_j xi_j cos - xr_j sin with the
 // angle 2 pi j k1 / R. Each entry w becomes W = rint(w 2^54) in seven balanced base-256 digits; slice t holds digit
-// 6 - t of every entry as int8 (eb = 1) or f16 (eb = 2), slice kTcDigits stays zero. Layout [slice][2nh][2kh].
-void tc_matrix(int R, int eb, std::vector<unsigned char>& out) {
-    const int kh = tc_kh(R), nh = tc_nh(R), kpad = 2 * kh * eb, npad = 2 * nh;
+// 6 - t of every entry as int8 (eb = 1) or f16 (eb = 2), slice kTcDigits stays zero. Layout
+// [round][slice][2nh / rounds rows][2kh] (rad.rounds, rad.nh as planned).
+void tc_matrix(const TcRadix& rad, int eb, std::vector<unsigned char>& out) {
+    const int R = rad.R, kh = rad.kh, nh = rad.nh, kpad = 2 * kh * eb, npad = 2 * nh, nr = npad / rad.rounds;
     const size_t base = out.size();
     out.resize(base + (size_t)kTcMats * npad * kpad, 0);
     auto put = [&](int n, int k, double w) {
         const long long W = std::llrint(std::ldexp(w, 54));  // exact scaling, one rounding; |W| <= 2^54
         const unsigned long long b = (unsigned long long)(W + 0x80808080808080LL);
+        const int rd = n / nr, nn = n - rd * nr;
         for (int i = 0; i < kTcDigits; i++) {
             const int digit = (int)((b >> (8 * i)) & 0xFF) - 128;
-            unsigned char* at = &out[base + (size_t)(kTcDigits - 1 - i) * npad * kpad + umma_off(n, k * eb, kpad)];
+            unsigned char* at = &out[base + ((size_t)rd * kTcMats + (kTcDigits - 1 - i)) * nr * kpad +
+                                     umma_off(nn, k * eb, kpad)];
             if (eb == 1) {
                 *at = (unsigned char)(signed char)digit;
             } else {
@@ -1238,31 +1253,40 @@ struct TcFftDev {
     size_t bytes() const { return tw4.bytes + tw_in.bytes + mats.bytes; }
 };
 
-// Sub-FFT of N points over `count` sequences with digit elements of eb bytes: radices, TMEM columns, sequences
-// per CTA within the shared-memory limit
+// Sub-FFT of N points over `count` sequences with digit elements of eb bytes: radices, items in flight per CTA
+// (two halves when they can hold at least half the sequences per item of one, KBSRC_GPU_TC_HALVES forces 1 or 2),
+// sequences per item within the shared-memory limit
 int tc_sub_plan(int N, int count, int eb, TcSub& sub, size_t& smem) {
-    int Ra, Rb, Rc = 1;
+    int Ra = 1, Rb = 1, Rc = 1;
     if (!tc_factor(N, Ra, Rb) && !tc_factor3(N, Ra, Rb, Rc))
         return fail(KBSRC_GPU_E_UNSUPPORTED, "split-precision form: no radix-32 factorisation");
-    sub = TcSub{};
-    sub.N = N;
-    sub.ebytes = eb;
-    sub.a = TcRadix{Ra, tc_kh(Ra), tc_nh(Ra), nullptr};
-    if (Rb > 1) sub.b = TcRadix{Rb, tc_kh(Rb), tc_nh(Rb), nullptr};
-    else sub.b = TcRadix{1, 0, 0, nullptr};
-    if (Rc > 1) sub.c = TcRadix{Rc, tc_kh(Rc), tc_nh(Rc), nullptr};
-    const int nh = std::max({sub.a.nh, sub.b.nh, sub.c.nh});
-    sub.ncols = kTcAcc * 2 * nh <= 256 ? 256 : 512;  // a power of two holding kTcAcc accumulators of 2nh columns
     int rmin = std::min(Ra, Rb > 1 ? Rb : Ra);
     if (Rc > 1) rmin = std::min(rmin, Rc);
     const int rows1 = N / rmin;  // rows of the largest stage for one sequence
-    int F = std::max(1, std::min(kTcRows / rows1, count));
-    for (;; F--) {
-        sub.F = F;
-        smem = 2 * (size_t)N * F * 16 + tc_smem_bytes(sub);
-        if (smem <= 227 * 1024 || F == 1) break;
-    }
-    if (smem > 227 * 1024) return fail(KBSRC_GPU_E_UNSUPPORTED, "split-precision form: sub-FFT too large");
+    const size_t limit = 227 * 1024;
+    auto plan = [&](int halves, TcSub& t, size_t& bytes) {  // the most sequences per item that fit; 0: none
+        t = TcSub{};
+        t.N = N;
+        t.ebytes = eb;
+        t.halves = halves;
+        t.a = tc_radix(Ra, halves);
+        t.b = tc_radix(Rb, halves);
+        t.c = tc_radix(Rc, halves);
+        for (int F = std::max(1, std::min(kTcRows / rows1, count)); F >= 1; F--) {
+            t.F = F;
+            bytes = tc_smem_bytes(t);
+            if (bytes <= limit) return F;
+        }
+        return 0;
+    };
+    TcSub one, two;
+    size_t b1 = 0, b2 = 0;
+    const int f1 = plan(1, one, b1), f2 = plan(2, two, b2);
+    const int force = env_int("KBSRC_GPU_TC_HALVES", 0);
+    const bool use2 = f2 > 0 && (force == 2 || (force != 1 && 2 * f2 >= f1));
+    if (!use2 && f1 == 0) return fail(KBSRC_GPU_E_UNSUPPORTED, "split-precision form: sub-FFT too large");
+    sub = use2 ? two : one;
+    smem = use2 ? b2 : b1;
     return KBSRC_GPU_OK;
 }
 
@@ -1304,7 +1328,7 @@ int make_tc_fft(int n, int eb, TcFftDev& t) {
     const int nr = t.N2 > 1 ? 6 : 3;
     for (int i = 0; i < nr; i++) {
         off[i] = mats.size();
-        if (rads[i]->R > 1) tc_matrix(rads[i]->R, eb, mats);
+        if (rads[i]->R > 1) tc_matrix(*rads[i], eb, mats);
     }
     if ((rc = t.mats.alloc(mats.size())) != KBSRC_GPU_OK) return rc;
     KB_CUDA(cudaMemcpy(t.mats.p, mats.data(), mats.size(), cudaMemcpyHostToDevice));
@@ -1483,7 +1507,7 @@ int allow_large_smem() {
     int mx = 0;
     KB_CUDA(cudaDeviceGetAttribute(&mx, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     cudaFuncAttributes fa{};
-    KB_CUDA(cudaFuncGetAttributes(&fa, (const void*)k_tc_row<TcF16, kDstOutput>));
+    KB_CUDA(cudaFuncGetAttributes(&fa, (const void*)k_tc_row<TcF16, kDstOutput, 1>));
     if (fa.maxDynamicSharedSizeBytes >= mx) return KBSRC_GPU_OK;
     // the dynamic limit is what the static shared memory of the kernel leaves of the opt-in maximum
 #define KB_SMEM(k)                                                                                          \
@@ -1526,16 +1550,17 @@ int allow_large_smem() {
     KB_SMEM((k_column_q<ArF64, kSrcComplex, false>));
     KB_SMEM((k_row_q<ArF64, kDstComplex, true>));
     KB_SMEM((k_row_q<ArF64, kDstOutput, false>));
-    KB_SMEM((k_tc_column<TcI8, kSrcSignal, kDstComplex>));
-    KB_SMEM((k_tc_column<TcI8, kSrcComplex, kDstComplex>));
-    KB_SMEM((k_tc_column<TcI8, kSrcComplex, kDstOutput>));
-    KB_SMEM((k_tc_row<TcI8, kDstComplex>));
-    KB_SMEM((k_tc_row<TcI8, kDstOutput>));
-    KB_SMEM((k_tc_column<TcF16, kSrcSignal, kDstComplex>));
-    KB_SMEM((k_tc_column<TcF16, kSrcComplex, kDstComplex>));
-    KB_SMEM((k_tc_column<TcF16, kSrcComplex, kDstOutput>));
-    KB_SMEM((k_tc_row<TcF16, kDstComplex>));
-    KB_SMEM((k_tc_row<TcF16, kDstOutput>));  // last: the marker read above
+#define KB_SMEM_TC(S, H)                                 \
+    KB_SMEM((k_tc_column<S, kSrcSignal, kDstComplex, H>));  \
+    KB_SMEM((k_tc_column<S, kSrcComplex, kDstComplex, H>)); \
+    KB_SMEM((k_tc_column<S, kSrcComplex, kDstOutput, H>));  \
+    KB_SMEM((k_tc_row<S, kDstComplex, H>));                 \
+    KB_SMEM((k_tc_row<S, kDstOutput, H>))
+    KB_SMEM_TC(TcI8, 1);
+    KB_SMEM_TC(TcI8, 2);
+    KB_SMEM_TC(TcF16, 2);
+    KB_SMEM_TC(TcF16, 1);  // last: k_tc_row<TcF16, kDstOutput, 1> is the marker read above
+#undef KB_SMEM_TC
 #undef KB_SMEM
     return KBSRC_GPU_OK;
 }
@@ -1772,20 +1797,32 @@ int launch_tc(const TcFftDev& t, const Slots& sl, void* x, void* y, int* err, cu
     T.N2 = t.N2;
     T.slots = (int)sl.nt;
     T.err = err;
-    auto grid = [&](long long items) { return (unsigned)std::max(1LL, std::min(items, (long long)t.ctas)); };
+    // persistent CTAs, one per SM at most, each working on `halves` items at once
+    auto grid = [&](long long items, int halves) {
+        return (unsigned)std::max(1LL, std::min((items + halves - 1) / halves, (long long)t.ctas));
+    };
+    auto column = [&](auto kernel, long long items) {
+        kernel<<<grid(items, T.sub.halves), kTcThreads, t.smem_col, st>>>(p, T);
+    };
+    const long long col_items = t.N2 == 1 ? (long long)sl.nt : (long long)((t.N2 + t.col.F - 1) / t.col.F) * sl.nt;
     if (t.N2 == 1) {
-        k_tc_column<S, SRC, DST><<<grid(sl.nt), kTcThreads, t.smem_col, st>>>(p, T);
+        if (T.sub.halves == 2) column(k_tc_column<S, SRC, DST, 2>, col_items);
+        else column(k_tc_column<S, SRC, DST, 1>, col_items);
         return tr.mark(st, kA);
     }
-    k_tc_column<S, SRC, kDstComplex>
-        <<<grid((long long)((t.N2 + t.col.F - 1) / t.col.F) * sl.nt), kTcThreads, t.smem_col, st>>>(p, T);
+    if (T.sub.halves == 2) column(k_tc_column<S, SRC, kDstComplex, 2>, col_items);
+    else column(k_tc_column<S, SRC, kDstComplex, 1>, col_items);
     int rc = tr.mark(st, kA);
     if (rc) return rc;
     p.src = static_cast<CxR<ArF64>*>(x);
     p.dst = static_cast<CxR<ArF64>*>(y);
     T.sub = t.row;
     T.tw4 = nullptr;
-    k_tc_row<S, DST><<<grid((long long)((t.N1 + t.row.F - 1) / t.row.F) * sl.nt), kTcThreads, t.smem_row, st>>>(p, T);
+    const long long row_items = (long long)((t.N1 + t.row.F - 1) / t.row.F) * sl.nt;
+    if (T.sub.halves == 2)
+        k_tc_row<S, DST, 2><<<grid(row_items, 2), kTcThreads, t.smem_row, st>>>(p, T);
+    else
+        k_tc_row<S, DST, 1><<<grid(row_items, 1), kTcThreads, t.smem_row, st>>>(p, T);
     return tr.mark(st, kB);
 }
 
@@ -2579,6 +2616,11 @@ int enqueue_queue_wave(const kbsrc_gpu_batch& b, size_t wi, cudaStream_t st, Tra
     auto launch = [&](auto kernel, int p) -> int {
         set(p);
         kernel<<<b.q_ctas[p], b.q_threads[p], b.q_smem[p], st>>>(q);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess)
+            return fail(KBSRC_GPU_E_CUDA, "batch queue pass " + std::to_string(p) + " (" + std::to_string(b.q_ctas[p]) +
+                                              " CTAs of " + std::to_string(b.q_threads[p]) + " threads, " +
+                                              std::to_string(b.q_smem[p]) + " bytes): " + cudaGetErrorString(e));
         return tr.mark(st, p);
     };
     int rc;

@@ -54,57 +54,88 @@ struct TcF16 {
     static __device__ __forceinline__ int acc_value(int32_t v) { return __float2int_rn(__int_as_float(v)); }
 };
 
-// One radix of the split form: the sliced real DFT_R matrix (global memory, kTcMats * 2nh * 2kh elements), its
-// slices one after the other, so that consecutive slices form one operand of kTcMats times 2nh columns.
+// One radix of the split form: the sliced real DFT_R matrix (global memory, kTcMats * 2nh * 2kh elements). Its
+// output columns come in `rounds` (1, or 2 when the accumulators of all 2nh columns do not fit the TMEM columns a
+// CTA half owns: real outputs, then imaginary outputs), laid out [round][slice][2nh / rounds rows][2kh], so that
+// consecutive slices of a round form one operand of kTcMats times its columns.
 struct TcRadix {
-    int R, kh, nh;
+    int R, kh, nh, rounds;
     const uint4* slices;
 };
 
-// A sub-FFT of N = a.R * b.R * c.R points (c.R == 1: two radices) on F sequences per CTA, every stage at most 128
-// rows (F * N / R <= 128 for each radix R); ebytes: element kind (1 int8, 2 f16); ncols: TMEM columns to allocate.
-// Inner twiddles, M = b.R * c.R: tw[k1 * M + m] = e^{-2 pi i m k1 / N}, then (three radices)
+// A sub-FFT of N = a.R * b.R * c.R points (b.R == 1: one stage; c.R == 1: two stages) on F sequences per item,
+// every stage at most 128 rows (F * N / R <= 128 for each radix R); ebytes: element kind (1 int8, 2 f16). halves:
+// items a CTA works on at once (1, or 2: each half of the CTA, 256 threads, with its own planes, slices, TMEM
+// columns and mbarrier, so that one item's MMAs and waits overlap the other's slicing and recombination). Inner
+// twiddles, M = b.R * c.R: tw[k1 * M + m] = e^{-2 pi i m k1 / N}, then (three radices)
 // tw[N + c1 * c.R + v] = e^{-2 pi i v c1 / M}.
 struct TcSub {
-    int N, F, ncols, ebytes;
+    int N, F, ebytes, halves;
     TcRadix a, b, c;
     const double2* tw;
 };
 __host__ __device__ inline int tc_tw_count(const TcSub& s) { return s.c.R > 1 ? s.N + s.b.R * s.c.R : s.N; }
-
-// Per-CTA shared memory of the split form after its data planes.
-struct TcSmem {
-    unsigned char* slices;  // kTcDigits * 128 * kpad bytes
-    unsigned char* bm_a;    // sliced DFT matrices
-    unsigned char* bm_b;
-    unsigned char* bm_c;
-    double2* tw;            // tc_tw_count inner twiddles
-    int* expo;              // row exponents E of the current stage
-    uint64_t* mbar;
-    uint32_t* tmem_slot;
-};
+// TMEM columns a CTA half owns, and the rounds of a radix with 2nh output columns
+__host__ __device__ inline int tc_half_cols(int halves) { return halves == 2 ? 256 : 512; }
+__host__ __device__ inline int tc_rounds_for(int nh, int halves) {
+    return kTcAcc * 2 * nh <= tc_half_cols(halves) ? 1 : 2;
+}
 
 __host__ __device__ inline int tc_bm_bytes(const TcRadix& r, int eb) {
     return r.R > 1 ? kTcMats * (2 * r.nh) * (2 * r.kh) * eb : 0;
 }
 // K row bytes of the data slices: the widest radix of the sub-FFT
 __host__ __device__ inline int tc_kpad(const TcSub& s) {
-    const int k = s.a.kh > s.b.kh ? s.a.kh : s.b.kh;
-    return 2 * (s.c.R > 1 && s.c.kh > k ? s.c.kh : k) * s.ebytes;
+    int k = s.a.kh > s.b.kh ? s.a.kh : s.b.kh;
+    if (s.c.R > 1 && s.c.kh > k) k = s.c.kh;
+    return 2 * k * s.ebytes;
 }
 __host__ __device__ inline size_t tc_align(size_t v) { return (v + 127) & ~(size_t)127; }
-
-// Shared bytes the split-form part of a CTA needs after its data planes.
-__host__ __device__ inline size_t tc_smem_bytes(const TcSub& s) {
-    return tc_align((size_t)kTcDigits * kTcRows * tc_kpad(s)) + tc_align(tc_bm_bytes(s.a, s.ebytes)) +
-           tc_align(tc_bm_bytes(s.b, s.ebytes)) + tc_align(tc_bm_bytes(s.c, s.ebytes)) +
-           tc_align((size_t)tc_tw_count(s) * 16) + tc_align(kTcRows * 4) + 128;
+// plane pairs an item needs: Y between the stages, and X too with three radices
+__host__ __device__ inline int tc_plane_pairs(const TcSub& s) { return s.c.R > 1 ? 2 : 1; }
+__host__ __device__ inline size_t tc_half_bytes(const TcSub& s) {
+    return tc_align((size_t)tc_plane_pairs(s) * s.N * s.F * 16) + tc_align((size_t)kTcDigits * kTcRows * tc_kpad(s)) +
+           tc_align(kTcRows * 4);
 }
+
+// Shared bytes of a split-form CTA: per half its planes, slices and row exponents; then the sliced matrices, the
+// inner twiddles, the mbarriers and the TMEM address.
+__host__ __device__ inline size_t tc_smem_bytes(const TcSub& s) {
+    return s.halves * tc_half_bytes(s) + tc_align(tc_bm_bytes(s.a, s.ebytes)) + tc_align(tc_bm_bytes(s.b, s.ebytes)) +
+           tc_align(tc_bm_bytes(s.c, s.ebytes)) + tc_align((size_t)tc_tw_count(s) * 16) + 128;
+}
+
+// What one half of a CTA works with: its threads (t = index within the half, kT of them), planes, slices, row
+// exponents, TMEM columns and mbarrier; the shared matrices and twiddles.
+struct TcHalf {
+    int id, t;
+    Planes<ArF64> X, Y;
+    unsigned char* slices;
+    int* expo;
+    uint64_t* mbar;
+    uint32_t tmem;
+    const unsigned char* bm_a;
+    const unsigned char* bm_b;
+    const unsigned char* bm_c;
+    const double2* tw;
+};
+
+struct TcSmem {
+    unsigned char* half[2];
+    unsigned char* bm_a;
+    unsigned char* bm_b;
+    unsigned char* bm_c;
+    double2* tw;
+    uint64_t* mbar;  // one per half
+    uint32_t* tmem_slot;
+};
 
 __device__ inline TcSmem tc_carve(unsigned char* p, const TcSub& s) {
     TcSmem m;
-    m.slices = p;
-    p += tc_align((size_t)kTcDigits * kTcRows * tc_kpad(s));
+    for (int h = 0; h < 2; h++) {
+        m.half[h] = p;
+        if (h < s.halves) p += tc_half_bytes(s);
+    }
     m.bm_a = p;
     p += tc_align(tc_bm_bytes(s.a, s.ebytes));
     m.bm_b = p;
@@ -113,18 +144,42 @@ __device__ inline TcSmem tc_carve(unsigned char* p, const TcSub& s) {
     p += tc_align(tc_bm_bytes(s.c, s.ebytes));
     m.tw = reinterpret_cast<double2*>(p);
     p += tc_align((size_t)tc_tw_count(s) * 16);
-    m.expo = reinterpret_cast<int*>(p);
-    p += tc_align(kTcRows * 4);
     m.mbar = reinterpret_cast<uint64_t*>(p);
-    m.tmem_slot = reinterpret_cast<uint32_t*>(p + 8);
+    m.tmem_slot = reinterpret_cast<uint32_t*>(p + 16);
     return m;
 }
 
-// TMEM allocation, the mbarrier, and the CTA's copies of the sliced matrices and inner twiddles. Ends with the
-// CTA synchronised; returns the TMEM base address.
+// The view of half `id` (threads 256 id .. when there are two halves, all threads otherwise).
+__device__ inline TcHalf tc_half(const TcSmem& m, const TcSub& s, int id, uint32_t tmem) {
+    TcHalf h;
+    h.id = id;
+    h.t = s.halves == 2 ? (int)threadIdx.x - 256 * id : (int)threadIdx.x;
+    unsigned char* p = m.half[id];
+    const int nf = s.N * s.F;
+    double* pl = reinterpret_cast<double*>(p);
+    h.Y = Planes<ArF64>{pl, pl + nf};
+    h.X = tc_plane_pairs(s) > 1 ? Planes<ArF64>{pl + 2 * nf, pl + 3 * nf} : h.Y;
+    p += tc_align((size_t)tc_plane_pairs(s) * nf * 16);
+    h.slices = p;
+    p += tc_align((size_t)kTcDigits * kTcRows * tc_kpad(s));
+    h.expo = reinterpret_cast<int*>(p);
+    h.mbar = m.mbar + id;
+    h.tmem = tmem + (uint32_t)(id * tc_half_cols(s.halves));
+    h.bm_a = m.bm_a;
+    h.bm_b = m.bm_b;
+    h.bm_c = m.bm_c;
+    h.tw = m.tw;
+    return h;
+}
+
+// TMEM allocation (all 512 columns), the mbarriers, and the CTA's copies of the sliced matrices and inner
+// twiddles. Ends with the CTA synchronised; returns the TMEM base address.
 __device__ inline uint32_t tc_setup(const TcSmem& m, const TcSub& s) {
-    if (threadIdx.x < 32) tmem_alloc(m.tmem_slot, (uint32_t)s.ncols);
-    if (threadIdx.x == 0) mbar_init(m.mbar, 1);
+    if (threadIdx.x < 32) tmem_alloc(m.tmem_slot, 512u);
+    if (threadIdx.x == 0) {
+        mbar_init(m.mbar, 1);
+        mbar_init(m.mbar + 1, 1);
+    }
     const int na = tc_bm_bytes(s.a, s.ebytes) / 16, nb = tc_bm_bytes(s.b, s.ebytes) / 16,
               nc = tc_bm_bytes(s.c, s.ebytes) / 16, nt = tc_tw_count(s);
 #pragma unroll 4
@@ -140,10 +195,20 @@ __device__ inline uint32_t tc_setup(const TcSmem& m, const TcSub& s) {
     return *m.tmem_slot;
 }
 
-__device__ inline void tc_teardown(const TcSub& s, uint32_t tmem) {
+__device__ inline void tc_teardown(uint32_t tmem) {
     tc_fence_before();
     __syncthreads();
-    if (threadIdx.x < 32) tmem_dealloc(tmem, (uint32_t)s.ncols);
+    if (threadIdx.x < 32) tmem_dealloc(tmem, 512u);
+}
+
+// Barrier of the threads of one half (named barrier 1 + id, kT threads; the whole CTA when there is one half)
+template <int kT>
+__device__ __forceinline__ void tc_half_sync(const TcHalf& h) {
+    if constexpr (kT == kTcThreads) {
+        __syncthreads();
+    } else {
+        asm volatile("bar.sync %0, %1;" ::"r"(1 + h.id), "r"(kT) : "memory");
+    }
 }
 
 // 2^k as a float64 for k in the normal range [-1022, 1023]
@@ -226,107 +291,180 @@ __device__ __forceinline__ double tc_combine(const int32_t (&c)[kTcAcc][4], int 
     return __dadd_rn(__dmul_rn(__ll2double_rn(hi), s1), __dmul_rn(__ll2double_rn(lo), s2));
 }
 
-// One contraction stage: `nrows` rows of R complex values. load(row, j) -> double2 (real, imaginary) for j < R;
-// store(row, k, re, im) for output k < R. `phase` counts the mbarrier phases completed so far. Starts and ends
-// with the CTA synchronised (what load reads must be visible on entry; what store writes is visible on return).
-//   slicing        thread t: row t / 4, elements 8 (t % 4) .. + 7 of both halves; the row exponent by shuffles
-//   MMA            thread 0: data slice ta against matrix slices 0..7-ta side by side, accumulators ta..7
-//   recombination  warp w: TMEM lanes 32 (w % 4) ..; warpgroup w / 4 takes every fourth group of 4 outputs
-template <class S, class Load, class Store>
-__device__ inline void tc_stage(const TcRadix& rad, int nrows, const TcSmem& m, const unsigned char* bmat,
-                                uint32_t tmem, uint32_t& phase, int* err, Load load, Store store) {
+// One contraction stage on one half: `nrows` rows of R complex values. load(row, j) -> double2 (real, imaginary)
+// for j < R; store(row, k, re, im) for output k < R. `phase` counts the half's mbarrier phases completed so far.
+// Starts and ends with the half synchronised (what load reads must be visible on entry; what store writes is
+// visible on return). kT: threads of the half (512 or 256); kRounds: the radix's rounds (1, or 2 with kT = 256).
+//   slicing        thread t: row t / (kT/128), 8-element chunks 8 (t % (kT/128)) + 8 (kT/128) i of both halves of K;
+//                  the row exponent by shuffles between the row's threads (with two chunks per thread the values
+//                  are read twice, once for the exponent and once for the digits, to keep them out of registers)
+//   MMA            thread 0: per round, data slice ta against matrix slices 0..7-ta side by side, accumulators ta..7
+//   recombination  warp w: TMEM lanes 32 (w % 4) ..; the warpgroups take interleaved groups of 4 outputs; with two
+//                  rounds the real parts wait in registers for the imaginary parts
+template <class S, int kT, int kRounds, class Load, class Store>
+__device__ inline void tc_stage(const TcRadix& rad, int nrows, const TcHalf& h, const unsigned char* bmat,
+                                uint32_t& phase, int* err, Load load, Store store) {
+    constexpr int kTPR = kT / kTcRows, kGroups = kT / 128;  // threads per row while slicing; warpgroups
+    constexpr int kChunks = 32 / kTPR / 8;                  // 8-element chunks per thread, at most
+    constexpr int kIters = 32 / (4 * kGroups);              // output groups of 4 per warpgroup, at most
     const int R = rad.R, kh = rad.kh, nh = rad.nh, npad = 2 * nh, kpad = 2 * kh * S::kBytes;
-    const int t = threadIdx.x;
+    const int nr = npad / kRounds;
+    const int t = h.t;
     {
-        const int row = t >> 2, j0 = 8 * (t & 3);
-        const bool act = row < nrows && j0 < kh;
-        double2 v[8];
-        unsigned long long mx = 0;
+        const int row = t / kTPR, q = t % kTPR;
+        const bool live = row < nrows;
+        auto chunk = [&](int i, double2 (&v)[8]) {
+            const int j0 = 8 * (q + kTPR * i);
 #pragma unroll
-        for (int u = 0; u < 8; u++) {
-            v[u] = act && j0 + u < R ? load(row, j0 + u) : make_double2(0.0, 0.0);
-            mx = max(mx, (unsigned long long)__double_as_longlong(v[u].x) & 0x7FFFFFFFFFFFFFFFull);
-            mx = max(mx, (unsigned long long)__double_as_longlong(v[u].y) & 0x7FFFFFFFFFFFFFFFull);
-        }
-        mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, 1));
-        mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, 2));
-        const int E = tc_row_expo(mx);
-        if ((t & 3) == 0) m.expo[row] = E;
-        if (act) {
+            for (int u = 0; u < 8; u++) v[u] = live && j0 + u < R ? load(row, j0 + u) : make_double2(0.0, 0.0);
+        };
+        auto magnitude = [](const double2 (&v)[8], unsigned long long mx) {
+#pragma unroll
+            for (int u = 0; u < 8; u++) {
+                mx = max(mx, (unsigned long long)__double_as_longlong(v[u].x) & 0x7FFFFFFFFFFFFFFFull);
+                mx = max(mx, (unsigned long long)__double_as_longlong(v[u].y) & 0x7FFFFFFFFFFFFFFFull);
+            }
+            return mx;
+        };
+        auto put = [&](int i, const double2 (&v)[8], int E) {
+            const int j0 = 8 * (q + kTPR * i);
+            if (!live || j0 >= kh) return;
             unsigned long long br[8], bi[8];
 #pragma unroll
             for (int u = 0; u < 8; u++) {
                 br[u] = tc_biased_digits(v[u].x, E);
                 bi[u] = tc_biased_digits(v[u].y, E);
             }
-            tc_put_digits<S>(m.slices, kpad, row, j0, br);
-            tc_put_digits<S>(m.slices, kpad, row, kh + j0, bi);
+            tc_put_digits<S>(h.slices, kpad, row, j0, br);
+            tc_put_digits<S>(h.slices, kpad, row, kh + j0, bi);
+        };
+        double2 v[8];
+        unsigned long long mx = 0;
+        if constexpr (kChunks == 1) {
+            chunk(0, v);
+            mx = magnitude(v, mx);
+        } else {
+#pragma unroll 1
+            for (int i = 0; i < kChunks; i++) {
+                chunk(i, v);
+                mx = magnitude(v, mx);
+            }
+        }
+#pragma unroll
+        for (int o = 1; o < kTPR; o <<= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        const int E = tc_row_expo(mx);
+        if (q == 0) h.expo[row] = E;
+        if constexpr (kChunks == 1) {
+            put(0, v, E);
+        } else {
+#pragma unroll 1
+            for (int i = 0; i < kChunks; i++) {
+                chunk(i, v);
+                put(i, v, E);
+            }
         }
     }
     fence_async_smem();
-    tc_fence_before();
-    __syncthreads();
-    tc_fence_after();
-    if (t == 0) {
-        const uint32_t sa = smem_u32(m.slices), sb = smem_u32(bmat), sbo = 8 * kpad;
-        const int bpc = 256 / npad, ksteps = kpad / 32;
-        for (int ta = 0; ta < kTcDigits; ta++)
-            for (int d0 = ta; d0 < kTcAcc; d0 += bpc) {
-                const int nb = min(bpc, kTcAcc - d0);
-                const uint32_t idesc = S::idesc(kTcRows, nb * npad);
-                for (int ks = 0; ks < ksteps; ks++)
-                    S::mma(tmem + d0 * npad, umma_desc(sa + ta * kTcRows * kpad + 256 * ks, 128, sbo),
-                           umma_desc(sb + (d0 - ta) * npad * kpad + 256 * ks, 128, sbo), idesc, (ta || ks) ? 1u : 0u);
-            }
-        umma_commit(m.mbar);
-    }
-    bool ok = mbar_wait(m.mbar, phase & 1u, kTcWaitLimit);
-    phase++;
-    ok = __all_sync(0xffffffffu, ok);  // the TMEM loads below are warp-collective
-    tc_fence_after();
-    if (!ok) {
-        if ((t & 31) == 0) atomicExch(err, 1);
-    } else {
-        const int warp = t >> 5, lq = warp & 3, row = 32 * lq + (t & 31);
-        const uint32_t lane_addr = tmem + ((uint32_t)(32 * lq) << 16);
-        const int E = m.expo[row];
+    const int warp = t >> 5, lq = warp & 3, g = warp >> 2, row = 32 * lq + (t & 31);
+    const uint32_t lane_addr = h.tmem + ((uint32_t)(32 * lq) << 16);
+    double yre[kRounds == 2 ? 4 * kIters : 1];  // real outputs of round 0 while round 1 runs
+#pragma unroll
+    for (int rd = 0; rd < kRounds; rd++) {
+        tc_fence_before();
+        tc_half_sync<kT>(h);  // slices written (round 0), or the previous round's TMEM reads done (round 1)
+        tc_fence_after();
+        if (t == 0) {
+            const uint32_t sa = smem_u32(h.slices), sb = smem_u32(bmat) + rd * kTcMats * nr * kpad,
+                           sbo = 8 * kpad;
+            const int bpc = 256 / nr, ksteps = kpad / 32;
+            for (int ta = 0; ta < kTcDigits; ta++)
+                for (int d0 = ta; d0 < kTcAcc; d0 += bpc) {
+                    const int nb = min(bpc, kTcAcc - d0);
+                    const uint32_t idesc = S::idesc(kTcRows, nb * nr);
+                    for (int ks = 0; ks < ksteps; ks++)
+                        S::mma(h.tmem + d0 * nr, umma_desc(sa + ta * kTcRows * kpad + 256 * ks, 128, sbo),
+                               umma_desc(sb + (d0 - ta) * nr * kpad + 256 * ks, 128, sbo), idesc,
+                               (ta || ks) ? 1u : 0u);
+                }
+            umma_commit(h.mbar);
+        }
+        bool ok = mbar_wait(h.mbar, phase & 1u, kTcWaitLimit);
+        phase++;
+        ok = __all_sync(0xffffffffu, ok);  // the TMEM loads below are warp-collective
+        tc_fence_after();
+        if (!ok) {
+            if ((t & 31) == 0) atomicExch(err, 1);
+            continue;
+        }
+        const int E = h.expo[row];
         const double s1 = tc_pow2_low(E - 37), s2 = tc_pow2_low(E - 69);
-        for (int k0 = 4 * (warp >> 2); k0 < R; k0 += 16) {
-            int32_t cr[kTcAcc][4], ci[kTcAcc][4];
 #pragma unroll
-            for (int d = 0; d < kTcAcc; d++) {
-                tmem_ld4(lane_addr + d * npad + k0, cr[d]);
-                tmem_ld4(lane_addr + d * npad + nh + k0, ci[d]);
-            }
-            tmem_wait_ld();
-            if (row < nrows) {
+        for (int it = 0; it < kIters; it++) {
+            const int k0 = 4 * g + 4 * kGroups * it;
+            if (k0 >= R) break;
+            if constexpr (kRounds == 1) {
+                int32_t cr[kTcAcc][4], ci[kTcAcc][4];
 #pragma unroll
-                for (int u = 0; u < 4; u++)
-                    if (k0 + u < R) store(row, k0 + u, tc_combine<S>(cr, u, s1, s2), tc_combine<S>(ci, u, s1, s2));
+                for (int d = 0; d < kTcAcc; d++) {
+                    tmem_ld4(lane_addr + d * nr + k0, cr[d]);
+                    tmem_ld4(lane_addr + d * nr + nh + k0, ci[d]);
+                }
+                tmem_wait_ld();
+                if (row < nrows) {
+#pragma unroll
+                    for (int u = 0; u < 4; u++)
+                        if (k0 + u < R)
+                            store(row, k0 + u, tc_combine<S>(cr, u, s1, s2), tc_combine<S>(ci, u, s1, s2));
+                }
+            } else {
+                int32_t c[kTcAcc][4];
+#pragma unroll
+                for (int d = 0; d < kTcAcc; d++) tmem_ld4(lane_addr + d * nr + k0, c[d]);
+                tmem_wait_ld();
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    const double y = tc_combine<S>(c, u, s1, s2);
+                    if (rd == 0) yre[4 * it + u] = y;
+                    else if (row < nrows && k0 + u < R) store(row, k0 + u, yre[4 * it + u], y);
+                }
             }
         }
     }
     tc_fence_before();
-    __syncthreads();
+    tc_half_sync<kT>(h);
     tc_fence_after();
+}
+
+// tc_stage with the radix's rounds (two rounds only arise with two halves)
+template <class S, int kT, class Load, class Store>
+__device__ __forceinline__ void tc_stage_r(const TcRadix& rad, int nrows, const TcHalf& h, const unsigned char* bmat,
+                                           uint32_t& phase, int* err, Load load, Store store) {
+    if constexpr (kT == kTcThreads) {
+        tc_stage<S, kT, 1>(rad, nrows, h, bmat, phase, err, load, store);
+    } else {
+        if (rad.rounds == 2) tc_stage<S, kT, 2>(rad, nrows, h, bmat, phase, err, load, store);
+        else tc_stage<S, kT, 1>(rad, nrows, h, bmat, phase, err, load, store);
+    }
 }
 
 __device__ __forceinline__ double2 tc_cmul(double re, double im, double2 w) {
     return make_double2(__dsub_rn(__dmul_rn(re, w.x), __dmul_rn(im, w.y)), __dadd_rn(__dmul_rn(re, w.y), __dmul_rn(im, w.x)));
 }
 
-// Sub-FFT of N points on F sequences, Cooley-Tukey through the stages of TcSub, from load_in(n, f) -> double2
-// (input n of sequence f) to store_out(k, f, re, im) (output k of sequence f, natural order). Intermediate stages
-// live in the plane pairs Y (and X, three radices), element j of sequence f at j * F + f; each inter-stage
-// twiddle is applied as the stage's outputs are stored. seq_fast: the first stage's rows run the sequences
-// fastest (inputs of neighbouring rows are neighbours in a column pass) rather than the inputs (a row pass).
+// Sub-FFT of N points on F sequences by one half of the CTA, Cooley-Tukey through the stages of TcSub, from
+// load_in(n, f) -> double2 (input n of sequence f) to store_out(k, f, re, im) (output k of sequence f, natural
+// order). Intermediate stages live in the half's plane pairs Y (and X, three radices), element j of sequence f at
+// j * F + f; each inter-stage twiddle is applied as the stage's outputs are stored. seq_fast: the first stage's
+// rows run the sequences fastest (inputs of neighbouring rows are neighbours in a column pass) rather than the
+// inputs (a row pass).
 //   two radices,   n = Rb j + m, k = k1 + Ra k2: DFT_Ra over j, twiddle w_N^{m k1}, DFT_Rb over m
 //   three radices, M = Rb Rc, n = M j + m, m = Rc u + v, k = k1 + Ra (c1 + Rb c2): DFT_Ra over j, w_N^{m k1},
 //                  DFT_Rb over u, w_M^{v c1}, DFT_Rc over v
-template <class S, class LoadIn, class StoreOut>
-__device__ inline void tc_subfft(const TcSub& s, bool seq_fast, const Planes<ArF64>& X, const Planes<ArF64>& Y,
-                                 const TcSmem& m, uint32_t tmem, uint32_t& phase, int* err, LoadIn load_in,
-                                 StoreOut store_out) {
+template <class S, int kT, class LoadIn, class StoreOut>
+__device__ inline void tc_subfft(const TcSub& s, bool seq_fast, const TcHalf& h, uint32_t& phase, int* err,
+                                 LoadIn load_in, StoreOut store_out) {
+    const Planes<ArF64>& X = h.X;
+    const Planes<ArF64>& Y = h.Y;
     const int F = s.F, Ra = s.a.R, Rb = s.b.R, Rc = s.c.R, M = Rb * (Rc > 1 ? Rc : 1);
     const FastDiv dF = fast_div(F), dM = fast_div(M);
     auto first_row = [&](int r, int& mm, int& f) {
@@ -338,7 +476,7 @@ __device__ inline void tc_subfft(const TcSub& s, bool seq_fast, const Planes<ArF
             mm = r - f * M;
         }
     };
-    tc_stage<S>(s.a, M * F, m, m.bm_a, tmem, phase, err,
+    tc_stage_r<S, kT>(s.a, M * F, h, h.bm_a, phase, err,
                 [&](int r, int j) {
                     int mm, f;
                     first_row(r, mm, f);
@@ -351,14 +489,14 @@ __device__ inline void tc_subfft(const TcSub& s, bool seq_fast, const Planes<ArF
                         store_out(k1, f, re, im);
                         return;
                     }
-                    const double2 y = tc_cmul(re, im, m.tw[k1 * M + mm]);
+                    const double2 y = tc_cmul(re, im, h.tw[k1 * M + mm]);
                     const int i = (k1 * M + mm) * F + f;
                     Y.re[i] = y.x;
                     Y.im[i] = y.y;
                 });
     if (Rb <= 1) return;
     if (Rc <= 1) {
-        tc_stage<S>(s.b, Ra * F, m, m.bm_b, tmem, phase, err,
+        tc_stage_r<S, kT>(s.b, Ra * F, h, h.bm_b, phase, err,
                     [&](int r, int mm) {
                         const int k1 = (int)fdiv(r, dF), f = r - k1 * F, i = (k1 * Rb + mm) * F + f;
                         return make_double2(Y.re[i], Y.im[i]);
@@ -370,7 +508,7 @@ __device__ inline void tc_subfft(const TcSub& s, bool seq_fast, const Planes<ArF
         return;
     }
     const FastDiv dRb = fast_div(Rb), dRc = fast_div(Rc);
-    tc_stage<S>(s.b, Ra * Rc * F, m, m.bm_b, tmem, phase, err,
+    tc_stage_r<S, kT>(s.b, Ra * Rc * F, h, h.bm_b, phase, err,
                 [&](int r, int u) {
                     const int q = (int)fdiv(r, dF), f = r - q * F, k1 = (int)fdiv(q, dRc), v = q - k1 * Rc;
                     const int i = (k1 * M + Rc * u + v) * F + f;
@@ -378,12 +516,12 @@ __device__ inline void tc_subfft(const TcSub& s, bool seq_fast, const Planes<ArF
                 },
                 [&](int r, int c1, double re, double im) {
                     const int q = (int)fdiv(r, dF), f = r - q * F, k1 = (int)fdiv(q, dRc), v = q - k1 * Rc;
-                    const double2 y = tc_cmul(re, im, m.tw[s.N + c1 * Rc + v]);
+                    const double2 y = tc_cmul(re, im, h.tw[s.N + c1 * Rc + v]);
                     const int i = (k1 * M + Rc * c1 + v) * F + f;
                     X.re[i] = y.x;
                     X.im[i] = y.y;
                 });
-    tc_stage<S>(s.c, Ra * Rb * F, m, m.bm_c, tmem, phase, err,
+    tc_stage_r<S, kT>(s.c, Ra * Rb * F, h, h.bm_c, phase, err,
                 [&](int r, int v) {
                     const int q = (int)fdiv(r, dF), f = r - q * F, k1 = (int)fdiv(q, dRb), c1 = q - k1 * Rb;
                     const int i = (k1 * M + Rc * c1 + v) * F + f;
