@@ -225,9 +225,9 @@ __device__ __forceinline__ CxW<Ar>* twiddle_smem(unsigned char* after_planes) {
 // (fft.hpp:283-299). blockIdx.x: column group; blockIdx.y: task slot. Reading the staged signal, the two are
 // swapped (task slot fastest): the channels of a block are consecutive tasks, and their CTAs for one column group
 // then run side by side and share the interleaved input's sectors in L2.
-// One column-pass unit: sequences n2 in [c0, c0+F) of length N1 (stride N2) of one task's slot (src, dst), or of
-// the staged signal `ts` (SRC), through the sub-plan sp, then the four-step twiddle, stored in place. Shared by the
-// per-plan grid kernel and the batch queue kernel.
+// One column-pass unit for the batch queue: sequences n2 in [c0, c0+F) of length N1 (stride N2) of one task's slot
+// (src, dst), or of the staged signal `ts` (SRC), through the sub-plan sp (in global memory), then the four-step
+// twiddle, stored in place (fft.hpp:283-299).
 template <class Ar, int SRC>
 __device__ __forceinline__ void column_unit(const SubPlan& sp, int N1, int N2, int F, int c0,
                                             const CxW<Ar>* tw_stage, const CxW<Ar>* tw4,
@@ -272,21 +272,61 @@ __device__ __forceinline__ void column_unit(const SubPlan& sp, int N1, int N2, i
     }
 }
 
+// The per-plan grid kernel runs the same loop as column_unit with every plan value read straight from its
+// parameters: a reference to the parameter block would turn those reads into generic loads (C2 exact: forward
+// column 1.05 -> 1.10 ms).
 template <class Ar, int SRC>
 __global__ void __launch_bounds__(Ar::kColMaxThreads, Ar::kColMinBlocks) k_column(const __grid_constant__ PassParams<Ar> P) {
     extern __shared__ __align__(16) unsigned char smem[];
+    using C = CxR<Ar>;
+    const int F = P.F, N1 = P.N1, N2 = P.N2, total = N1 * F;
+    const FastDiv dF = fast_div(F);
+    Planes<Ar> A, B;
+    unsigned char* rest = carve<Ar>(smem, total, A, B);
     const unsigned slot = SRC == kSrcSignal ? blockIdx.x : blockIdx.y, group = SRC == kSrcSignal ? blockIdx.y : blockIdx.x;
     const long long task = P.task0 + slot;
-    const TaskSource ts = SRC == kSrcSignal ? task_source(P.work, task, 2LL * P.N1 * P.N2) : TaskSource{};
-    column_unit<Ar, SRC>(P.sp, P.N1, P.N2, P.F, (int)group * P.F, P.tw_stage, P.tw4, P.odd, P.src + slot * P.stride,
-                         P.dst + slot * P.stride, ts, P.ddreal, smem);
+    const int c0 = group * F;
+    const C* src = P.src + slot * P.stride;
+    C* dst = P.dst + slot * P.stride;
+    const TaskSource ts = SRC == kSrcSignal ? task_source(P.work, task, 2LL * N1 * N2) : TaskSource{};
+    const CxW<Ar>* tws = stage_twiddles<Ar>(P.sp, P.tw_stage, twiddle_smem<Ar>(rest));
+    for (int e0 = threadIdx.x; e0 < total; e0 += kLoadBatch * blockDim.x) {
+        C v[kLoadBatch];
+#pragma unroll
+        for (int j = 0; j < kLoadBatch; j++) {
+            const int e = e0 + j * blockDim.x, r = (int)fdiv(e, dF), n2 = c0 + (e - r * F);
+            if (e < total) v[j] = n2 < N2 ? load_input<Ar, SRC>(P, ts, src, (long long)r * N2 + n2) : czero<Ar>();
+        }
+#pragma unroll
+        for (int j = 0; j < kLoadBatch; j++)
+            if (e0 + j * blockDim.x < total) A.st(e0 + j * blockDim.x, v[j]);
+    }
+    __syncthreads();
+    const Planes<Ar> res = stockham<Ar>(P.sp, A, B, F, tws, P.odd);
+    for (int e0 = threadIdx.x; e0 < total; e0 += kLoadBatch * blockDim.x) {
+        CxW<Ar> w[kLoadBatch];
+#pragma unroll
+        for (int j = 0; j < kLoadBatch; j++) {
+            const int e = e0 + j * blockDim.x, k1 = (int)fdiv(e, dF), n2 = c0 + (e - k1 * F);
+            if (e < total && n2 < N2 && k1 && (Ar::kLanes || n2)) w[j] = ld_tw(P.tw4 + (long long)k1 * N2 + n2);
+        }
+#pragma unroll
+        for (int j = 0; j < kLoadBatch; j++) {
+            const int e = e0 + j * blockDim.x, k1 = (int)fdiv(e, dF), n2 = c0 + (e - k1 * F);
+            if (e >= total || n2 >= N2) continue;
+            C v = res.ld(e);
+            if (k1 && (Ar::kLanes || n2)) v = c_mulw<Ar>(v, w[j]);
+            if (Ar::kLaneRenorm) v = c_renorm<Ar>(v);
+            dst[(long long)k1 * N2 + n2] = v;
+        }
+    }
 }
 
 // Row pass: rows r in [r0, r0+F) of length N2 (contiguous), stored transposed to [N1*k2 + r]
 // (fft.hpp:300-311), or written straight to the output as real samples (fft.hpp:459-460).
-// One row-pass unit: rows r in [r0, r0+F) of length N2 of one task's slot through sp, stored transposed to
-// dst[N1*k2 + r], or written to the output as real samples (DST; `work` and the task place them). Shared by the
-// per-plan grid kernel and the batch queue kernel.
+// One row-pass unit for the batch queue: rows r in [r0, r0+F) of length N2 of one task's slot through sp, stored
+// transposed to dst[N1*k2 + r], or written to the output as real samples (DST; `work` and the task place them)
+// (fft.hpp:300-311,459-460).
 template <class Ar, int DST>
 __device__ __forceinline__ void row_unit(const SubPlan& sp, int N1, int N2, int F, int r0, const CxW<Ar>* tw_stage,
                                          const OddRoots<typename Ar::W>& odd, const CxR<Ar>* src, CxR<Ar>* dst,
@@ -329,11 +369,50 @@ __device__ __forceinline__ void row_unit(const SubPlan& sp, int N1, int N2, int 
     }
 }
 
+// The per-plan grid kernel: row_unit's loop with the plan read straight from the parameters (see k_column).
 template <class Ar, int DST>
 __global__ void __launch_bounds__(Ar::kMaxThreads, Ar::kMinBlocks) k_row(const __grid_constant__ PassParams<Ar> P) {
     extern __shared__ __align__(16) unsigned char smem[];
-    row_unit<Ar, DST>(P.sp, P.N1, P.N2, P.F, (int)blockIdx.x * P.F, P.tw_stage, P.odd, P.src + blockIdx.y * P.stride,
-                      P.dst + blockIdx.y * P.stride, P.work, P.task0 + blockIdx.y, smem);
+    using C = CxR<Ar>;
+    const int F = P.F, N1 = P.N1, N2 = P.N2, total = N2 * F;
+    const FastDiv dF = fast_div(F), dN2 = fast_div(N2);
+    Planes<Ar> A, B;
+    unsigned char* rest = carve<Ar>(smem, total, A, B);
+    const long long task = P.task0 + blockIdx.y;
+    const int r0 = blockIdx.x * F;
+    const C* src = P.src + blockIdx.y * P.stride;
+    const CxW<Ar>* tws = stage_twiddles<Ar>(P.sp, P.tw_stage, twiddle_smem<Ar>(rest));
+    for (int e0 = threadIdx.x; e0 < total; e0 += kLoadBatch * blockDim.x) {
+        C v[kLoadBatch];
+#pragma unroll
+        for (int j = 0; j < kLoadBatch; j++) {
+            const int e = e0 + j * blockDim.x, f = (int)fdiv(e, dN2), i = e - f * N2, row = r0 + f;
+            if (e < total) v[j] = row < N1 ? src[(long long)row * N2 + i] : czero<Ar>();
+        }
+#pragma unroll
+        for (int j = 0; j < kLoadBatch; j++) {
+            const int e = e0 + j * blockDim.x, f = (int)fdiv(e, dN2), i = e - f * N2;
+            if (e < total) A.st(i * F + f, v[j]);
+        }
+    }
+    __syncthreads();
+    const Planes<Ar> res = stockham<Ar>(P.sp, A, B, F, tws, P.odd);
+    C* dst = P.dst + blockIdx.y * P.stride;
+    const TaskRef tr = DST == kDstOutput ? task_ref(P.work, task) : TaskRef{0, 0, 0};
+    const Item it = DST == kDstOutput ? item_of(P.work, tr) : Item{};
+    for (int e = threadIdx.x; e < total; e += blockDim.x) {
+        const int k2 = (int)fdiv(e, dF), f = e - k2 * F, row = r0 + f;
+        if (row >= N1) continue;
+        C v = res.ld(e);
+        if (Ar::kLaneRenorm) v = c_renorm<Ar>(v);
+        const long long iz = (long long)N1 * k2 + row;
+        if (DST == kDstComplex) {
+            dst[iz] = v;
+        } else {
+            emit(P.work, it, tr.c, tr.b, 2 * iz, Ar::to_f64(v.re));
+            emit(P.work, it, tr.c, tr.b, 2 * iz + 1, Ar::to_f64(Ar::neg(v.im)));
+        }
+    }
 }
 
 // Whole FFT of n <= 2048 points in one CTA (the reference's direct SFFT path, fft.hpp:241-244,279).
@@ -1254,8 +1333,8 @@ struct TcFftDev {
 };
 
 // Sub-FFT of N points over `count` sequences with digit elements of eb bytes: radices, items in flight per CTA
-// (two halves when they can hold at least half the sequences per item of one, KBSRC_GPU_TC_HALVES forces 1 or 2),
-// sequences per item within the shared-memory limit
+// (one; KBSRC_GPU_TC_HALVES=2 selects two halves of 256 threads, which measured slower on C2: 3.80 against 3.33 ms
+// per step, the radices above 16 needing two rounds), sequences per item within the shared-memory limit
 int tc_sub_plan(int N, int count, int eb, TcSub& sub, size_t& smem) {
     int Ra = 1, Rb = 1, Rc = 1;
     if (!tc_factor(N, Ra, Rb) && !tc_factor3(N, Ra, Rb, Rc))
@@ -1283,7 +1362,7 @@ int tc_sub_plan(int N, int count, int eb, TcSub& sub, size_t& smem) {
     size_t b1 = 0, b2 = 0;
     const int f1 = plan(1, one, b1), f2 = plan(2, two, b2);
     const int force = env_int("KBSRC_GPU_TC_HALVES", 0);
-    const bool use2 = f2 > 0 && (force == 2 || (force != 1 && 2 * f2 >= f1));
+    const bool use2 = f2 > 0 && (force == 2 || (f1 == 0 && force != 1));
     if (!use2 && f1 == 0) return fail(KBSRC_GPU_E_UNSUPPORTED, "split-precision form: sub-FFT too large");
     sub = use2 ? two : one;
     smem = use2 ? b2 : b1;
@@ -2615,6 +2694,9 @@ int enqueue_queue_wave(const kbsrc_gpu_batch& b, size_t wi, cudaStream_t st, Tra
     };
     auto launch = [&](auto kernel, int p) -> int {
         set(p);
+        const cudaError_t before = cudaPeekAtLastError();
+        if (before != cudaSuccess)
+            return fail(KBSRC_GPU_E_CUDA, std::string("before the batch queue: ") + cudaGetErrorString(before));
         kernel<<<b.q_ctas[p], b.q_threads[p], b.q_smem[p], st>>>(q);
         const cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess)
