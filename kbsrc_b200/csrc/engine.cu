@@ -1027,9 +1027,28 @@ std::vector<HostCx> split_roots(int N) {
 }
 
 // Device copy of a table: dd pairs for double-double, the high parts for f64 (fft.hpp:16)
+// An owned device allocation. Move-only: a copy would free the same pointer twice (and leave the survivor
+// pointing at freed memory).
 struct DevBuf {
     void* p = nullptr;
     size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    DevBuf(DevBuf&& o) noexcept : p(o.p), bytes(o.bytes) {
+        o.p = nullptr;
+        o.bytes = 0;
+    }
+    DevBuf& operator=(DevBuf&& o) noexcept {
+        if (this != &o) {
+            release();
+            p = o.p;
+            bytes = o.bytes;
+            o.p = nullptr;
+            o.bytes = 0;
+        }
+        return *this;
+    }
     ~DevBuf() { release(); }
     void release() {
         if (p) cudaFree(p);
