@@ -521,7 +521,11 @@ def product_arm(args, w, world, rank, local, pg):
         # same resident input, errors against the exact output just timed
         ref_y = got.copy()
         for mode in ("split", "split16", "fast"):
-            f = companion_form(mode, x, w, kw, dev, stream, args, ref_y, args.tune)
+            try:
+                f = companion_form(mode, x, w, kw, dev, stream, args, ref_y, args.tune)
+            except RuntimeError as e:  # a form without a plan for this workload's transform lengths
+                extra[mode] = {"unsupported": str(e)}
+                continue
             f["vs_plain_exact"] = round((ms / args.steps) / f["ms_per_step"], 4)
             extra[mode] = f
     if split:  # the comparison the form exists for: accuracy against exact, throughput against plain exact
