@@ -163,12 +163,12 @@ int kbsrc_gpu_engine_info(const kbsrc_gpu_engine* e, long long* tasks, long long
 void kbsrc_gpu_engine_destroy(kbsrc_gpu_engine* e);
 
 /* Batches: many conversions at once (the uneven multi-file queue). Conversions whose plans are equal (precision,
- * P/Q, block, margin, fold, kernel spectrum) form one group and share FFT tables. When every group is exact or
- * every group fast, with four-step 7-smooth transforms (the common rates), all groups' (channel, block) tasks run
- * together as one work queue: waves of tasks of any groups, largest transform first, and per wave one persistent
- * launch per pass whose CTAs take units of work (a column or row group of a task, a range of spectrum bins) from an
- * atomic counter, like the reference's workers take tasks (src/resampler.cpp:42-49). Other batches run group after
- * group. The first run records the whole launch sequence in a CUDA graph and later runs replay it: every buffer
+ * P/Q, block, margin, fold, kernel spectrum) form one group and share FFT tables. A group with enough work to fill
+ * the GPU on every pass runs on its own launches; the other groups of the batch's arithmetic (exact or fast, with
+ * four-step 7-smooth transforms: the common rates) run together as one work queue: waves of tasks of any of them,
+ * largest transform first, and per wave one persistent launch per pass whose CTAs take units of work (a column or
+ * row group of a task, a range of spectrum bins) from an atomic counter, like the reference's workers take tasks
+ * (src/resampler.cpp:42-49). KBSRC_GPU_QUEUE=0 runs every group on its own launches. The first run records the whole launch sequence in a CUDA graph and later runs replay it: every buffer
  * pointer is read from a small per-run table, so new buffers need no new recording. Replaces running run_engine
  * once per file (src/resampler.cpp:34-88). descs[i] as for kbsrc_gpu_engine_create (H copied at create; shards are
  * not accepted). */

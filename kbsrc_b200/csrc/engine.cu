@@ -18,6 +18,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -711,12 +712,56 @@ struct QueueParams {
     OddRoots<W> odd;
 };
 
-// The next unit for this CTA (the whole CTA agrees on it; the previous unit's shared memory is free again).
-__device__ __forceinline__ int queue_next(int* counter, int* slot) {
+// A CTA's place in a queue pass: the unit it works on (in shared memory, so that the whole CTA agrees on it) and
+// the next one, claimed from the counter and fetched by thread 0 while the CTA works on the current one, so that
+// the dependent loads of the unit and task descriptors overlap the work instead of preceding it.
+struct QueueSlot {
+    int u;
+    QueueUnit qu;
+    QueueTask t;
+};
+template <class W>
+struct QueueCursor {
+    const QueueParams<W>& Q;
+    QueueSlot& cur;  // shared memory
+    QueueSlot nxt;   // thread 0
+    __device__ __forceinline__ void claim() {
+        nxt.u = atomicAdd(Q.counter, 1);
+        if (nxt.u < Q.nunits) {
+            nxt.qu = Q.units[nxt.u];
+            nxt.t = Q.tasks[nxt.qu.task];
+        }
+    }
+    // the first unit; ends with the CTA synchronised
+    __device__ __forceinline__ void start() {
+        if (threadIdx.x == 0) {
+            claim();
+            cur = nxt;
+        }
+        __syncthreads();
+    }
+    // claim and fetch the unit after the current one (thread 0; the loads complete while the CTA works)
+    __device__ __forceinline__ void prefetch() {
+        if (threadIdx.x == 0) claim();
+    }
+    // the current unit is done: move to the prefetched one; ends with the CTA synchronised
+    __device__ __forceinline__ void advance() {
+        __syncthreads();
+        if (threadIdx.x == 0) cur = nxt;
+        __syncthreads();
+    }
+};
+
+// Copies a unit's sub-FFT plan from the group table to shared memory, where the pass's stage loops read it (from
+// the group table in global memory every read of the plan would be a load; the per-plan kernels have it in their
+// parameters). Ends with the CTA synchronised.
+__device__ __forceinline__ void queue_plan(const SubPlan& from, SubPlan& to) {
+    static_assert(sizeof(SubPlan) % 4 == 0, "SubPlan is copied as 32-bit words");
+    constexpr int kWords = (int)(sizeof(SubPlan) / 4);
+    const int* src = reinterpret_cast<const int*>(&from);
+    int* dst = reinterpret_cast<int*>(&to);
+    for (int i = threadIdx.x; i < kWords; i += blockDim.x) dst[i] = __ldg(src + i);
     __syncthreads();
-    if (threadIdx.x == 0) *slot = atomicAdd(counter, 1);
-    __syncthreads();
-    return *slot;
 }
 
 // The Work view of one queue task: its conversion as the only item (task = b * ch + c), the group's hop.
@@ -735,20 +780,22 @@ template <class Ar, int SRC, bool FWD>
 __global__ void __launch_bounds__(Ar::kColMaxThreads, Ar::kColMinBlocks)
     k_column_q(const __grid_constant__ QueueParams<typename Ar::W> Q) {
     extern __shared__ __align__(16) unsigned char smem[];
-    __shared__ int next;
+    __shared__ QueueSlot slot;
+    __shared__ SubPlan sp;
     using C = CxR<Ar>;
-    for (;;) {
-        const int u = queue_next(Q.counter, &next);
-        if (u >= Q.nunits) break;
-        const QueueUnit qu = Q.units[u];
-        const QueueTask t = Q.tasks[qu.task];
+    QueueCursor<typename Ar::W> qc{Q, slot};
+    for (qc.start(); slot.u < Q.nunits; qc.advance()) {
+        const QueueUnit qu = slot.qu;
+        const QueueTask t = slot.t;
+        qc.prefetch();
         const QueueGroup& g = Q.groups[t.group];
+        queue_plan(FWD ? g.fs1 : g.is1, sp);
         const int N1 = FWD ? g.fN1 : g.iN1, N2 = FWD ? g.fN2 : g.iN2, F = FWD ? g.fcF : g.icF;
         C* x = static_cast<C*>(FWD ? Q.A : Q.B) + t.slot;
         long long task;
         const Work w = queue_work(g, Q.items, t, task);
         const TaskSource ts = SRC == kSrcSignal ? task_source(w, task, 2LL * N1 * N2) : TaskSource{};
-        column_unit<Ar, SRC>(FWD ? g.fs1 : g.is1, N1, N2, F, qu.unit * F,
+        column_unit<Ar, SRC>(sp, N1, N2, F, qu.unit * F,
                              static_cast<const CxW<Ar>*>(FWD ? g.ftw_stage : g.itw_stage),
                              static_cast<const CxW<Ar>*>(FWD ? g.ftw4 : g.itw4), Q.odd, x, x, ts, nullptr, smem);
     }
@@ -759,20 +806,22 @@ template <class Ar, int DST, bool FWD>
 __global__ void __launch_bounds__(Ar::kMaxThreads, Ar::kMinBlocks)
     k_row_q(const __grid_constant__ QueueParams<typename Ar::W> Q) {
     extern __shared__ __align__(16) unsigned char smem[];
-    __shared__ int next;
+    __shared__ QueueSlot slot;
+    __shared__ SubPlan sp;
     using C = CxR<Ar>;
-    for (;;) {
-        const int u = queue_next(Q.counter, &next);
-        if (u >= Q.nunits) break;
-        const QueueUnit qu = Q.units[u];
-        const QueueTask t = Q.tasks[qu.task];
+    QueueCursor<typename Ar::W> qc{Q, slot};
+    for (qc.start(); slot.u < Q.nunits; qc.advance()) {
+        const QueueUnit qu = slot.qu;
+        const QueueTask t = slot.t;
+        qc.prefetch();
         const QueueGroup& g = Q.groups[t.group];
+        queue_plan(FWD ? g.fs2 : g.is2, sp);
         const int N1 = FWD ? g.fN1 : g.iN1, N2 = FWD ? g.fN2 : g.iN2, F = FWD ? g.frF : g.irF;
         long long task;
         const Work w = queue_work(g, Q.items, t, task);
         const C* src = static_cast<const C*>(FWD ? Q.A : Q.B) + t.slot;
         C* dst = static_cast<C*>(Q.B) + t.slot;
-        row_unit<Ar, DST>(FWD ? g.fs2 : g.is2, N1, N2, F, qu.unit * F,
+        row_unit<Ar, DST>(sp, N1, N2, F, qu.unit * F,
                           static_cast<const CxW<Ar>*>(FWD ? g.ftw_stage : g.itw_stage), Q.odd, src, dst, w, task, smem);
     }
 }
@@ -790,13 +839,13 @@ __device__ __forceinline__ SpecParams<Ar> queue_spec(const QueueGroup& g) {
 // Real-FFT split (buffer B to A, bins of one unit) or spectrum multiply and merge (buffer A to B).
 template <class Ar, bool SPLIT>
 __global__ void __launch_bounds__(kQueueBinThreads) k_bins_q(const __grid_constant__ QueueParams<typename Ar::W> Q) {
-    __shared__ int next;
+    __shared__ QueueSlot slot;
     using C = CxR<Ar>;
-    for (;;) {
-        const int u = queue_next(Q.counter, &next);
-        if (u >= Q.nunits) break;
-        const QueueUnit qu = Q.units[u];
-        const QueueTask t = Q.tasks[qu.task];
+    QueueCursor<typename Ar::W> qc{Q, slot};
+    for (qc.start(); slot.u < Q.nunits; qc.advance()) {
+        const QueueUnit qu = slot.qu;
+        const QueueTask t = slot.t;
+        qc.prefetch();
         const QueueGroup& g = Q.groups[t.group];
         const SpecParams<Ar> sp = queue_spec<Ar>(g);
         const int k0 = qu.unit * kQueueBins, last = split_last<Ar>(SPLIT ? g.h : g.hi);
@@ -2586,13 +2635,62 @@ int queue_ctas(K kernel, int threads, size_t smem, int sms, int& ctas) {
 // buffers, each pass's units. The other groups run their own launches after the queue.
 int build_queue(kbsrc_gpu_batch& b) {
     if (b.groups.empty() || !env_int("KBSRC_GPU_QUEUE", 1)) return KBSRC_GPU_OK;
+    int first = -1;
+    for (size_t i = 0; i < b.groups.size() && first < 0; i++)
+        if (queue_eligible(*b.groups[i])) first = (int)i;
+    if (first < 0) return KBSRC_GPU_OK;
+    const bool exact = b.groups[first]->exact;
+    const size_t es = b.groups[first]->esize();
+    // Every group shares each pass's launch shape, so a group's sequences per unit are cut (launch shapes only: the
+    // bytes do not change) until its shared memory leaves room for as many CTAs per SM as the kernel is compiled
+    // for; the largest of those then sizes the launch. A group that fits no such shape runs on its own launches.
+    int per_sm = 0;
+    KB_CUDA(cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, b.device));
+    const int colT = exact ? KB_MAXT_DD_COL : KB_MAXT_F64, rowT = exact ? KB_MAXT_DD : KB_MAXT_F64;
+    const int colB = exact ? KB_MINB_DD_COL : KB_MINB_F64, rowB = exact ? KB_MINB_DD : KB_MINB_F64;
+    const int pass[4] = {0, 1, 4, 5}, maxT[4] = {colT, rowT, colT, rowT};
+    size_t limit[4];
+    for (int k = 0; k < 4; k++) limit[k] = (size_t)per_sm / (k & 1 ? rowB : colB) - 2048;
+    auto fit = [&](const SubPlan& sp, int F, int kk, Shape& out) {  // the largest F' <= F within limit[kk]
+        const size_t tw = es == 32 ? (size_t)sp.twn * es : 0;
+        for (int f = F; f >= 1; f--) {
+            const size_t sm = 2 * (size_t)sp.n * f * es + tw;
+            if (sm > limit[kk]) continue;
+            int t = ((max_bfly(sp) * f + 31) / 32) * 32;
+            out = Shape{f, std::max(64, std::min(maxT[kk], t)), sm};
+            return true;
+        }
+        return false;
+    };
+    // A group with enough units to fill the GPU on every pass runs on its own launches, whose shapes are its own
+    // (a queue launch shares one thread count and one shared-memory size among its groups: C4's 54 groups, all
+    // large, took 500 ms per step through the queue against 384 ms on their own launches); the queue gathers the
+    // groups whose own launches would leave SMs idle. KBSRC_GPU_QUEUE_FILL sets the threshold in units per pass.
+    int sms_q = 0;
+    KB_CUDA(cudaDeviceGetAttribute(&sms_q, cudaDevAttrMultiProcessorCount, b.device));
+    const long long fill = env_int("KBSRC_GPU_QUEUE_FILL", 8 * sms_q);
+    auto fills = [&](const BatchGroup& g) {
+        const long long col = std::min((g.fw.host.N2 + g.fw.col.F - 1) / g.fw.col.F,
+                                       (g.iv.host.N2 + g.iv.col.F - 1) / g.iv.col.F);
+        const long long row = std::min((g.fw.host.N1 + g.fw.row.F - 1) / g.fw.row.F,
+                                       (g.iv.host.N1 + g.iv.row.F - 1) / g.iv.row.F);
+        return g.tasks * std::min(col, row) >= fill;
+    };
     std::vector<int> qi;  // queued groups in the batch's group order
-    for (size_t i = 0; i < b.groups.size(); i++)
-        if (queue_eligible(*b.groups[i]) && (qi.empty() || b.groups[i]->exact == b.groups[qi[0]]->exact))
-            qi.push_back((int)i);
+    std::vector<std::array<Shape, 4>> qs;
+    for (size_t i = 0; i < b.groups.size(); i++) {
+        const BatchGroup& g = *b.groups[i];
+        if (!queue_eligible(g) || g.exact != exact || fills(g)) continue;
+        const SubPlan* sp[4] = {&g.fw.host.s1, &g.fw.host.s2, &g.iv.host.s1, &g.iv.host.s2};
+        const Shape sh[4] = {g.fw.col, g.fw.row, g.iv.col, g.iv.row};
+        std::array<Shape, 4> q;
+        bool ok = true;
+        for (int k = 0; k < 4 && ok; k++) ok = fit(*sp[k], sh[k].F, k, q[k]);
+        if (!ok) continue;
+        qi.push_back((int)i);
+        qs.push_back(q);
+    }
     if (qi.empty()) return KBSRC_GPU_OK;
-    const bool exact = b.groups[qi[0]]->exact;
-    const size_t es = b.groups[qi[0]]->esize();
     std::vector<QueueGroup> qg(qi.size());
     int T[6] = {}, sms = 0;
     size_t S[6] = {};
@@ -2601,16 +2699,14 @@ int build_queue(kbsrc_gpu_batch& b) {
         QueueGroup& q = qg[i];
         q.fs1 = g.fw.host.s1; q.fs2 = g.fw.host.s2; q.is1 = g.iv.host.s1; q.is2 = g.iv.host.s2;
         q.fN1 = g.fw.host.N1; q.fN2 = g.fw.host.N2; q.iN1 = g.iv.host.N1; q.iN2 = g.iv.host.N2;
-        q.fcF = g.fw.col.F; q.frF = g.fw.row.F; q.icF = g.iv.col.F; q.irF = g.iv.row.F;
+        q.fcF = qs[i][0].F; q.frF = qs[i][1].F; q.icF = qs[i][2].F; q.irF = qs[i][3].F;
         q.ftw_stage = g.fw.tw_stage.p; q.ftw4 = g.fw.tw4.p; q.itw_stage = g.iv.tw_stage.p; q.itw4 = g.iv.tw4.p;
         q.w_fw = g.w_fw.p; q.w_iv = g.w_iv.p; q.H = g.H.p;
         q.h = g.hf; q.hi = g.hi; q.Nb = g.Nb; q.Mb = g.Mb; q.up = g.d.up; q.Jg = g.d.Jg;
         q.hopQ = (long long)g.hop * g.d.Q; q.hopP = (long long)g.hop * g.d.P; q.margP = (long long)g.d.marg * g.d.P;
-        const Shape sh[4] = {g.fw.col, g.fw.row, g.iv.col, g.iv.row};
-        const int pass[4] = {0, 1, 4, 5};
         for (int k = 0; k < 4; k++) {
-            T[pass[k]] = std::max(T[pass[k]], sh[k].T);
-            S[pass[k]] = std::max(S[pass[k]], sh[k].smem);
+            T[pass[k]] = std::max(T[pass[k]], qs[i][k].T);
+            S[pass[k]] = std::max(S[pass[k]], qs[i][k].smem);
         }
     }
     T[2] = T[3] = kQueueBinThreads;
