@@ -210,11 +210,16 @@ __device__ __forceinline__ CxR<Ar> czero() {
     return CxR<Ar>{Ar::zero(), Ar::zero()};
 }
 
-// Loads per thread issued together before their shared-memory stores (memory-level parallelism)
+// Loads per thread issued together before their shared-memory stores (memory-level parallelism), for the wide
+// types (double-double, extended) and for float64
 #ifndef KB_LOAD_BATCH
 #define KB_LOAD_BATCH 4
 #endif
-constexpr int kLoadBatch = KB_LOAD_BATCH;
+#ifndef KB_LOAD_BATCH_F64
+#define KB_LOAD_BATCH_F64 4
+#endif
+template <class Ar>
+constexpr int kLoadBatch = Ar::kWide ? KB_LOAD_BATCH : KB_LOAD_BATCH_F64;
 
 // Shared memory of a pass: two plane pairs of n*F values, then (double-double) the sub-FFT's stage twiddles.
 template <class Ar>
@@ -240,29 +245,29 @@ __device__ __forceinline__ void column_unit(const SubPlan& sp, int N1, int N2, i
     Planes<Ar> A, B;
     unsigned char* rest = carve<Ar>(smem, total, A, B);
     const CxW<Ar>* tws = stage_twiddles<Ar>(sp, tw_stage, twiddle_smem<Ar>(rest));
-    for (int e0 = threadIdx.x; e0 < total; e0 += kLoadBatch * blockDim.x) {
-        C v[kLoadBatch];
+    for (int e0 = threadIdx.x; e0 < total; e0 += kLoadBatch<Ar> * blockDim.x) {
+        C v[kLoadBatch<Ar>];
 #pragma unroll
-        for (int j = 0; j < kLoadBatch; j++) {
+        for (int j = 0; j < kLoadBatch<Ar>; j++) {
             const int e = e0 + j * blockDim.x, r = (int)fdiv(e, dF), n2 = c0 + (e - r * F);
             if (e < total) v[j] = n2 < N2 ? load_input<Ar, SRC>(ddreal, ts, src, (long long)r * N2 + n2) : czero<Ar>();
         }
 #pragma unroll
-        for (int j = 0; j < kLoadBatch; j++)
+        for (int j = 0; j < kLoadBatch<Ar>; j++)
             if (e0 + j * blockDim.x < total) A.st(e0 + j * blockDim.x, v[j]);
     }
     __syncthreads();
     const Planes<Ar> res = stockham<Ar>(sp, A, B, F, tws, odd);
     // four-step twiddle and store; the table loads of a batch are issued before any of its products
-    for (int e0 = threadIdx.x; e0 < total; e0 += kLoadBatch * blockDim.x) {
-        CxW<Ar> w[kLoadBatch];
+    for (int e0 = threadIdx.x; e0 < total; e0 += kLoadBatch<Ar> * blockDim.x) {
+        CxW<Ar> w[kLoadBatch<Ar>];
 #pragma unroll
-        for (int j = 0; j < kLoadBatch; j++) {
+        for (int j = 0; j < kLoadBatch<Ar>; j++) {
             const int e = e0 + j * blockDim.x, k1 = (int)fdiv(e, dF), n2 = c0 + (e - k1 * F);
             if (e < total && n2 < N2 && k1 && (Ar::kLanes || n2)) w[j] = ld_tw(tw4 + (long long)k1 * N2 + n2);
         }
 #pragma unroll
-        for (int j = 0; j < kLoadBatch; j++) {
+        for (int j = 0; j < kLoadBatch<Ar>; j++) {
             const int e = e0 + j * blockDim.x, k1 = (int)fdiv(e, dF), n2 = c0 + (e - k1 * F);
             if (e >= total || n2 >= N2) continue;
             C v = res.ld(e);
@@ -291,28 +296,28 @@ __global__ void __launch_bounds__(Ar::kColMaxThreads, Ar::kColMinBlocks) k_colum
     C* dst = P.dst + slot * P.stride;
     const TaskSource ts = SRC == kSrcSignal ? task_source(P.work, task, 2LL * N1 * N2) : TaskSource{};
     const CxW<Ar>* tws = stage_twiddles<Ar>(P.sp, P.tw_stage, twiddle_smem<Ar>(rest));
-    for (int e0 = threadIdx.x; e0 < total; e0 += kLoadBatch * blockDim.x) {
-        C v[kLoadBatch];
+    for (int e0 = threadIdx.x; e0 < total; e0 += kLoadBatch<Ar> * blockDim.x) {
+        C v[kLoadBatch<Ar>];
 #pragma unroll
-        for (int j = 0; j < kLoadBatch; j++) {
+        for (int j = 0; j < kLoadBatch<Ar>; j++) {
             const int e = e0 + j * blockDim.x, r = (int)fdiv(e, dF), n2 = c0 + (e - r * F);
             if (e < total) v[j] = n2 < N2 ? load_input<Ar, SRC>(P, ts, src, (long long)r * N2 + n2) : czero<Ar>();
         }
 #pragma unroll
-        for (int j = 0; j < kLoadBatch; j++)
+        for (int j = 0; j < kLoadBatch<Ar>; j++)
             if (e0 + j * blockDim.x < total) A.st(e0 + j * blockDim.x, v[j]);
     }
     __syncthreads();
     const Planes<Ar> res = stockham<Ar>(P.sp, A, B, F, tws, P.odd);
-    for (int e0 = threadIdx.x; e0 < total; e0 += kLoadBatch * blockDim.x) {
-        CxW<Ar> w[kLoadBatch];
+    for (int e0 = threadIdx.x; e0 < total; e0 += kLoadBatch<Ar> * blockDim.x) {
+        CxW<Ar> w[kLoadBatch<Ar>];
 #pragma unroll
-        for (int j = 0; j < kLoadBatch; j++) {
+        for (int j = 0; j < kLoadBatch<Ar>; j++) {
             const int e = e0 + j * blockDim.x, k1 = (int)fdiv(e, dF), n2 = c0 + (e - k1 * F);
             if (e < total && n2 < N2 && k1 && (Ar::kLanes || n2)) w[j] = ld_tw(P.tw4 + (long long)k1 * N2 + n2);
         }
 #pragma unroll
-        for (int j = 0; j < kLoadBatch; j++) {
+        for (int j = 0; j < kLoadBatch<Ar>; j++) {
             const int e = e0 + j * blockDim.x, k1 = (int)fdiv(e, dF), n2 = c0 + (e - k1 * F);
             if (e >= total || n2 >= N2) continue;
             C v = res.ld(e);
@@ -338,15 +343,15 @@ __device__ __forceinline__ void row_unit(const SubPlan& sp, int N1, int N2, int 
     Planes<Ar> A, B;
     unsigned char* rest = carve<Ar>(smem, total, A, B);
     const CxW<Ar>* tws = stage_twiddles<Ar>(sp, tw_stage, twiddle_smem<Ar>(rest));
-    for (int e0 = threadIdx.x; e0 < total; e0 += kLoadBatch * blockDim.x) {
-        C v[kLoadBatch];
+    for (int e0 = threadIdx.x; e0 < total; e0 += kLoadBatch<Ar> * blockDim.x) {
+        C v[kLoadBatch<Ar>];
 #pragma unroll
-        for (int j = 0; j < kLoadBatch; j++) {
+        for (int j = 0; j < kLoadBatch<Ar>; j++) {
             const int e = e0 + j * blockDim.x, f = (int)fdiv(e, dN2), i = e - f * N2, row = r0 + f;
             if (e < total) v[j] = row < N1 ? src[(long long)row * N2 + i] : czero<Ar>();
         }
 #pragma unroll
-        for (int j = 0; j < kLoadBatch; j++) {
+        for (int j = 0; j < kLoadBatch<Ar>; j++) {
             const int e = e0 + j * blockDim.x, f = (int)fdiv(e, dN2), i = e - f * N2;
             if (e < total) A.st(i * F + f, v[j]);
         }
@@ -383,15 +388,15 @@ __global__ void __launch_bounds__(Ar::kMaxThreads, Ar::kMinBlocks) k_row(const _
     const int r0 = blockIdx.x * F;
     const C* src = P.src + blockIdx.y * P.stride;
     const CxW<Ar>* tws = stage_twiddles<Ar>(P.sp, P.tw_stage, twiddle_smem<Ar>(rest));
-    for (int e0 = threadIdx.x; e0 < total; e0 += kLoadBatch * blockDim.x) {
-        C v[kLoadBatch];
+    for (int e0 = threadIdx.x; e0 < total; e0 += kLoadBatch<Ar> * blockDim.x) {
+        C v[kLoadBatch<Ar>];
 #pragma unroll
-        for (int j = 0; j < kLoadBatch; j++) {
+        for (int j = 0; j < kLoadBatch<Ar>; j++) {
             const int e = e0 + j * blockDim.x, f = (int)fdiv(e, dN2), i = e - f * N2, row = r0 + f;
             if (e < total) v[j] = row < N1 ? src[(long long)row * N2 + i] : czero<Ar>();
         }
 #pragma unroll
-        for (int j = 0; j < kLoadBatch; j++) {
+        for (int j = 0; j < kLoadBatch<Ar>; j++) {
             const int e = e0 + j * blockDim.x, f = (int)fdiv(e, dN2), i = e - f * N2;
             if (e < total) A.st(i * F + f, v[j]);
         }
@@ -565,9 +570,40 @@ __device__ __forceinline__ x80 ld_w<x80>(const x80* p) {
     return x80{(unsigned long long)a.x, (int)a.y, 0};
 }
 
-// Y[k]: spectrum multiply with fold (down) or periodic extension (up) (resampler.cpp:64-78)
+// The forward spectrum X[j] (j <= h) as the spectrum step reads it: from the split pass's output buffer ...
 template <class Ar>
-__device__ __forceinline__ CxR<Ar> spectrum_bin(const SpecParams<Ar>& P, const CxR<Ar>* X, int k) {
+struct SpectrumBuf {
+    const CxR<Ar>* X;
+    __device__ __forceinline__ CxR<Ar> operator()(int j) const { return X[j]; }
+};
+
+// ... or, in float64, computed from the complex spectrum Z where it is needed: the float64 split computes every bin
+// alone by the same operations (fft.hpp:377-407), so a bin's value does not depend on the pass that computes it,
+// and the spectrum step can read Z directly instead of a stored copy of X (one pass and 2 x (h+1) values of HBM
+// traffic per task fewer).
+template <class Ar>
+struct SpectrumFromZ {
+    static_assert(!Ar::kWide, "the wide types split conjugate pairs together");
+    const CxR<Ar>* Z;
+    const CxW<Ar>* w_fw;
+    int h;
+    __device__ __forceinline__ CxR<Ar> operator()(int k) const {
+        using C = CxR<Ar>;
+        if (k == 0 || k == h) {
+            const C z0 = Z[0];
+            return C{k ? Ar::sub(z0.re, z0.im) : Ar::add(z0.re, z0.im), Ar::zero()};
+        }
+        const C a = Z[k], bb = c_conj<Ar>(Z[h - k]);
+        const C E = c_add<Ar>(a, bb), O = c_mul_mi<Ar>(c_sub<Ar>(a, bb));
+        const C v = c_add<Ar>(E, c_mulw<Ar>(O, ld_tw(w_fw + k)));
+        return c_scale<Ar>(v, Ar::from_f64(0.5));
+    }
+};
+
+// Y[k]: spectrum multiply with fold (down) or periodic extension (up) (resampler.cpp:64-78); X(j) is the forward
+// spectrum (SpectrumBuf or SpectrumFromZ).
+template <class Ar, class XS>
+__device__ __forceinline__ CxR<Ar> spectrum_bin(const SpecParams<Ar>& P, const XS& X, int k) {
     using C = CxR<Ar>;
     const int Nb = P.Nb, Mb = P.Mb;
     if (P.Jg) {
@@ -578,7 +614,7 @@ __device__ __forceinline__ CxR<Ar> spectrum_bin(const SpecParams<Ar>& P, const C
         C y = czero<Ar>();
         auto take = [&](long long j, bool mirrored) {
             const int jj = (int)(j % Nb);
-            const C x = jj <= Nb / 2 ? X[jj] : c_conj<Ar>(X[Nb - jj]);
+            const C x = jj <= Nb / 2 ? X(jj) : c_conj<Ar>(X(Nb - jj));
             const C v = c_scale<Ar>(x, Ar::from_w(ld_w(P.H + j)));
             if (j == 0) y = c_add<Ar>(y, v);
             else if (edge) y.re = Ar::add(y.re, Ar::mul(Ar::from_f64(2.0), v.re));
@@ -593,17 +629,17 @@ __device__ __forceinline__ CxR<Ar> spectrum_bin(const SpecParams<Ar>& P, const C
     }
     if (P.up) {
         const int kk = k % Nb;
-        const C v = kk <= Nb / 2 ? X[kk] : c_conj<Ar>(X[Nb - kk]);
+        const C v = kk <= Nb / 2 ? X(kk) : c_conj<Ar>(X(Nb - kk));
         C y = c_scale<Ar>(v, Ar::from_w(ld_w(P.H + k)));
         if (2 * k == Mb) y.im = Ar::zero();
         return y;
     }
     if (2 * k == Mb)
-        return C{Ar::mul(Ar::mul(Ar::from_f64(2.0), X[k].re), Ar::from_w(ld_w(P.H + k))), Ar::zero()};
-    C y = c_scale<Ar>(X[k], Ar::from_w(ld_w(P.H + k)));
+        return C{Ar::mul(Ar::mul(Ar::from_f64(2.0), X(k).re), Ar::from_w(ld_w(P.H + k))), Ar::zero()};
+    C y = c_scale<Ar>(X(k), Ar::from_w(ld_w(P.H + k)));
     const int j = Mb - k, jmax = min(Nb / 2, Mb - 1);
     if (k >= 1 && j <= jmax) {  // j >= Mb/2 + 1 = K holds for every k < Mb/2
-        const C v = c_scale<Ar>(X[j], Ar::from_w(ld_w(P.H + j)));
+        const C v = c_scale<Ar>(X(j), Ar::from_w(ld_w(P.H + j)));
         y = c_add<Ar>(y, c_conj<Ar>(v));
     }
     return y;
@@ -611,8 +647,8 @@ __device__ __forceinline__ CxR<Ar> spectrum_bin(const SpecParams<Ar>& P, const C
 
 // Inverse merge z[k] = conj(E + i D), E = Y[k] + conj Y[hi-k], D = (Y[k] - conj Y[hi-k]) conj w[k]
 // (fft.hpp:411-458); pairs in dd, each k alone in f64.
-template <class Ar>
-__device__ __forceinline__ void merge_range(const SpecParams<Ar>& P, const CxR<Ar>* X, CxR<Ar>* Zi, int k0, int k_end,
+template <class Ar, class XS>
+__device__ __forceinline__ void merge_range(const SpecParams<Ar>& P, const XS& X, CxR<Ar>* Zi, int k0, int k_end,
                                             int step) {
     using C = CxR<Ar>;
     const int hi = P.hi;
@@ -636,8 +672,16 @@ __device__ __forceinline__ void merge_range(const SpecParams<Ar>& P, const CxR<A
 
 template <class Ar>
 __global__ void k_merge(const __grid_constant__ SpecParams<Ar> P) {
-    merge_range<Ar>(P, P.X + blockIdx.y * P.stride, P.Zi + blockIdx.y * P.stride, blockIdx.x * blockDim.x + threadIdx.x,
-                    split_last<Ar>(P.hi), gridDim.x * blockDim.x);
+    merge_range<Ar>(P, SpectrumBuf<Ar>{P.X + blockIdx.y * P.stride}, P.Zi + blockIdx.y * P.stride,
+                    blockIdx.x * blockDim.x + threadIdx.x, split_last<Ar>(P.hi), gridDim.x * blockDim.x);
+}
+
+// Float64 split, spectrum multiply and merge in one pass: Z (forward complex FFT) -> Zi (inverse input), with the
+// forward spectrum computed from Z bin by bin as the spectrum step needs it. Zi must not alias Z.
+template <class Ar>
+__global__ void k_spectrum_z(const __grid_constant__ SpecParams<Ar> P) {
+    merge_range<Ar>(P, SpectrumFromZ<Ar>{P.Z + blockIdx.y * P.stride, P.w_fw, P.h}, P.Zi + blockIdx.y * P.stride,
+                    blockIdx.x * blockDim.x + threadIdx.x, split_last<Ar>(P.hi), gridDim.x * blockDim.x);
 }
 
 // dd / double (double_double.hpp:80-84) with IEEE division
@@ -854,7 +898,7 @@ __global__ void __launch_bounds__(kQueueBinThreads) k_bins_q(const __grid_consta
             split_range<Ar>(sp, static_cast<const C*>(Q.B) + t.slot, static_cast<C*>(Q.A) + t.slot,
                             k0 + (int)threadIdx.x, k_end, blockDim.x);
         else
-            merge_range<Ar>(sp, static_cast<const C*>(Q.A) + t.slot, static_cast<C*>(Q.B) + t.slot,
+            merge_range<Ar>(sp, SpectrumBuf<Ar>{static_cast<const C*>(Q.A) + t.slot}, static_cast<C*>(Q.B) + t.slot,
                             k0 + (int)threadIdx.x, k_end, blockDim.x);
     }
 }
@@ -1914,12 +1958,20 @@ int enqueue_plan(const PlanCore& pc, const Work& work, long long t_begin, long l
         s.w_iv = static_cast<const CxW<ArS>*>(pc.w_iv.p);
         s.H = static_cast<const WS*>(pc.H.p);
         s.h = pc.hf; s.hi = pc.hi; s.Nb = pc.Nb; s.Mb = pc.Mb; s.up = d.up; s.Jg = d.Jg;
-        k_split<ArS><<<dim3(grid_for(pc.hf / 2 + 1 + (ArS::kWide ? 0 : pc.hf / 2), 256), sl.nt), 256, 0, st>>>(s);
-        if ((rc = tr.mark(st, kSplit)) != KBSRC_GPU_OK) return rc;
-        k_merge<ArS><<<dim3(grid_for(pc.hi / 2 + 1 + (ArS::kWide ? 0 : pc.hi / 2), 256), sl.nt), 256, 0, st>>>(s);
+        const dim3 gmerge(grid_for(pc.hi / 2 + 1 + (ArS::kWide ? 0 : pc.hi / 2), 256), sl.nt);
+        int zi = z;  // the buffer that holds the inverse FFT's input
+        if constexpr (ArS::kWide) {
+            k_split<ArS><<<dim3(grid_for(pc.hf / 2 + 1, 256), sl.nt), 256, 0, st>>>(s);
+            if ((rc = tr.mark(st, kSplit)) != KBSRC_GPU_OK) return rc;
+            k_merge<ArS><<<gmerge, 256, 0, st>>>(s);
+        } else {  // float64: one pass from Z (buf[z]) to the inverse input in buf[1-z]
+            zi = 1 - z;
+            s.Zi = static_cast<CS*>(buf[zi]);
+            k_spectrum_z<ArS><<<gmerge, 256, 0, st>>>(s);
+        }
         if ((rc = tr.mark(st, kMerge)) != KBSRC_GPU_OK) return rc;
-        // inverse complex FFT of buf[z] and the output epilogue
-        rc = launch_cfft<ArL, ArS, kSrcComplex, kDstOutput>(pc.iv, sl, buf[z], buf[1 - z], buf[z], nullptr, st, tr,
+        // inverse complex FFT of buf[zi] and the output epilogue
+        rc = launch_cfft<ArL, ArS, kSrcComplex, kDstOutput>(pc.iv, sl, buf[zi], buf[1 - zi], buf[zi], nullptr, st, tr,
                                                              kInvA, kInvB);
         if (rc) return rc;
     }
@@ -1989,20 +2041,18 @@ int enqueue_split(const PlanCore& pc, const Work& work, long long t_begin, long 
         sl.nt = (unsigned)std::min(wave, t_end - t0);
         if ((rc = launch_tc<S, kSrcSignal, kDstComplex>(pc.tfw, sl, a, b, err, st, tr, kFwdA, kFwdB)) != KBSRC_GPU_OK)
             return rc;
+        // float64 split, spectrum and merge in one pass: Z in b, the inverse input to a
         SpecParams<ArF64> s{};
         s.Z = static_cast<CxR<ArF64>*>(b);
-        s.X = static_cast<CxR<ArF64>*>(a);
-        s.Zi = static_cast<CxR<ArF64>*>(b);
+        s.Zi = static_cast<CxR<ArF64>*>(a);
         s.stride = stride;
         s.w_fw = static_cast<const CxW<ArF64>*>(pc.w_fw.p);
         s.w_iv = static_cast<const CxW<ArF64>*>(pc.w_iv.p);
         s.H = static_cast<const double*>(pc.H.p);
         s.h = pc.hf; s.hi = pc.hi; s.Nb = pc.Nb; s.Mb = pc.Mb; s.up = d.up; s.Jg = d.Jg;
-        k_split<ArF64><<<dim3(grid_for(pc.hf, 256), sl.nt), 256, 0, st>>>(s);
-        if ((rc = tr.mark(st, kSplit)) != KBSRC_GPU_OK) return rc;
-        k_merge<ArF64><<<dim3(grid_for(pc.hi, 256), sl.nt), 256, 0, st>>>(s);
+        k_spectrum_z<ArF64><<<dim3(grid_for(pc.hi, 256), sl.nt), 256, 0, st>>>(s);
         if ((rc = tr.mark(st, kMerge)) != KBSRC_GPU_OK) return rc;
-        if ((rc = launch_tc<S, kSrcComplex, kDstOutput>(pc.tiv, sl, b, nullptr, err, st, tr, kInvA, kInvB)) !=
+        if ((rc = launch_tc<S, kSrcComplex, kDstOutput>(pc.tiv, sl, a, nullptr, err, st, tr, kInvA, kInvB)) !=
             KBSRC_GPU_OK)
             return rc;
     }
@@ -2048,8 +2098,9 @@ size_t cfft_bytes(const DevCfft& c) {
 
 // Kernel launches of one wave, and the device bytes of the plan's tables
 long long plan_launches(const PlanCore& pc) {
-    if (pc.split) return (pc.tfw.N2 > 1 ? 2 : 1) + 2 + (pc.tiv.N2 > 1 ? 2 : 1);
-    return cfft_launches(pc.fw) + 2 + cfft_launches(pc.iv);
+    if (pc.split) return (pc.tfw.N2 > 1 ? 2 : 1) + 1 + (pc.tiv.N2 > 1 ? 2 : 1);
+    const int spectrum = pc.exact || pc.tab == kTabX80 ? 2 : 1;  // float64 fuses split, spectrum and merge
+    return cfft_launches(pc.fw) + spectrum + cfft_launches(pc.iv);
 }
 size_t plan_table_bytes(const PlanCore& pc) {
     return cfft_bytes(pc.fw) + cfft_bytes(pc.iv) + pc.tfw.bytes() + pc.tiv.bytes() + pc.w_fw.bytes + pc.w_iv.bytes +

@@ -123,7 +123,8 @@ def conversion_work(plan, channels, exact):
 
 
 def pass_bytes(plan, exact):
-    """Bytes each pass must move per task (its inputs and outputs; complex dd 32 B, f64 16 B)."""
+    """Bytes each pass must move per task (its inputs and outputs; complex dd 32 B, f64 16 B). In float64 the split,
+    spectrum and merge are one pass timed as "merge" (it reads Z, e*hf, and writes the inverse input, e*hi)."""
     e = 32 if exact else 16
     hf, hi = plan["Nb"] // 2, plan["Mb"] // 2
     four_f, four_i = hf > 2048, hi > 2048
@@ -131,7 +132,7 @@ def pass_bytes(plan, exact):
     return {"fwd_column": 8 * plan["Nb"] + e * hf,
             "fwd_row": 2 * e * hf if four_f else 0,
             "split": e * hf + e * (hf + 1),
-            "merge": e * (hf + 1) + e * hi,
+            "merge": e * (hf + 1) + e * hi if exact else e * hf + e * hi,
             "inv_column": 2 * e * hi if four_i else e * hi + out,
             "inv_row": e * hi + out if four_i else 0}
 
