@@ -514,6 +514,7 @@ def product_arm(args, w, world, rank, local, pg):
     extra = {}
     if tuned is not None:
         extra["tuned_shapes"] = tuned
+        extra["twiddles_in_shared_memory"] = cv.staging()
     if (w.get("pcm24") or not args.no_cpu) and not args.seconds and world == 1 and not split:
         extra["cli_e2e"] = cli_e2e(w, x)  # the tool a user runs, on the workload's file, ours and the reference's
     if args.workload in ("c2_exact", "c5_exact") and world == 1 and not args.seconds and not args.no_forms:

@@ -146,7 +146,8 @@ int kbsrc_gpu_engine_run_host_packed(kbsrc_gpu_engine* e, const double* in, cons
 int kbsrc_gpu_pack(const double* d_planar, int channels, long long frames, long long stride, int format, int dither,
                    unsigned char* d_out, long long* clipped, void* stream);
 
-/* Autotuner: picks the launch shape (sequences per CTA, threads per CTA, hence shared-memory staging) of each
+/* Autotuner: picks the launch shape (sequences per CTA, threads per CTA, and for double-double and extended
+ * passes whether the stage twiddles are staged in shared memory; see kbsrc_gpu_engine_staging) of each
  * four-step pass (forward column and row, inverse column and row) by timing whole device-resident runs on the
  * given buffers: every candidate shape is applied to all passes at once, each pass keeps its fastest. The radix
  * order and the block size are never changed, so the output bytes are the same under every shape. Runs the
@@ -155,6 +156,13 @@ int kbsrc_gpu_pack(const double* d_planar, int channels, long long frames, long 
  * Not in the reference (its engines have no launch shapes). */
 int kbsrc_gpu_engine_tune(kbsrc_gpu_engine* e, const double* d_in, const double* d_head, const double* d_tail,
                           double* d_out, void* stream, int* shapes);
+
+/* Where the four four-step passes (forward column and row, inverse column and row) read their stage twiddles:
+ * 4 ints out, 1 = a copy in each CTA's shared memory, 0 = the global table through the read-only cache, -1 = not a
+ * four-step pass. Float64 passes always read the global table; the double-double and extended passes stage by
+ * default (KBSRC_GPU_TW_GLOBAL=1 reads the table) and the autotuner chooses per pass. The bytes do not depend on it.
+ * Not in the reference (its engines run on the CPU). */
+int kbsrc_gpu_engine_staging(const kbsrc_gpu_engine* e, int* staged);
 
 /* Number of (channel, block) tasks, kernel launches per run, and the engine's device bytes. */
 int kbsrc_gpu_engine_info(const kbsrc_gpu_engine* e, long long* tasks, long long* launches,

@@ -97,6 +97,7 @@ GPU_SYMBOLS = {
     "kbsrc_gpu_engine_name": (ctypes.c_char_p, []),
     "kbsrc_gpu_engine_tune": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                              ctypes.c_void_p, ctypes.c_void_p, _P(ctypes.c_int)]),
+    "kbsrc_gpu_engine_staging": (ctypes.c_int, [ctypes.c_void_p, _P(ctypes.c_int)]),
     "kbsrc_gpu_init": (ctypes.c_int, []),
     "kbsrc_gpu_shard_plan": (ctypes.c_int, [_P(GpuDesc), ctypes.c_int, _P(GpuShard)]),
     "kbsrc_gpu_use_device": (ctypes.c_int, [ctypes.c_int]),
@@ -308,6 +309,16 @@ class Conversion:
             raise RuntimeError(f"kbsrc_gpu_engine_tune: {rc} {gpu_error()}")
         names = ["fwd_column", "fwd_row", "inv_column", "inv_row"]
         return {names[i]: (sh[2 * i], sh[2 * i + 1]) for i in range(4) if sh[2 * i]}
+
+    def staging(self):
+        """kbsrc_gpu_engine_staging: {pass: True when its stage twiddles are staged in shared memory, False when
+        read from the global table} for the four-step passes."""
+        st = (ctypes.c_int * 4)()
+        rc = gpu_lib().kbsrc_gpu_engine_staging(self.engine, st)
+        if rc:
+            raise RuntimeError(f"kbsrc_gpu_engine_staging: {rc} {gpu_error()}")
+        names = ["fwd_column", "fwd_row", "inv_column", "inv_row"]
+        return {names[i]: bool(st[i]) for i in range(4) if st[i] >= 0}
 
     def run_host_raw(self, x_ptr, head_ptr, tail_ptr, out_ptr):
         """Engine run on host pointers (ints), e.g. pinned buffers; synchronous."""

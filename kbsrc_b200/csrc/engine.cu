@@ -244,7 +244,7 @@ __device__ __forceinline__ void column_unit(const SubPlan& sp, int N1, int N2, i
     const FastDiv dF = fast_div(F);
     Planes<Ar> A, B;
     unsigned char* rest = carve<Ar>(smem, total, A, B);
-    const CxW<Ar>* tws = stage_twiddles<Ar>(sp, tw_stage, twiddle_smem<Ar>(rest));
+    const auto tws = stage_twiddles<Ar>(sp, tw_stage, twiddle_smem<Ar>(rest));
     for (int e0 = threadIdx.x; e0 < total; e0 += kLoadBatch<Ar> * blockDim.x) {
         C v[kLoadBatch<Ar>];
 #pragma unroll
@@ -280,8 +280,9 @@ __device__ __forceinline__ void column_unit(const SubPlan& sp, int N1, int N2, i
 
 // The per-plan grid kernel runs the same loop as column_unit with every plan value read straight from its
 // parameters: a reference to the parameter block would turn those reads into generic loads (C2 exact: forward
-// column 1.05 -> 1.10 ms).
-template <class Ar, int SRC>
+// column 1.05 -> 1.10 ms). TWG (double-double and extended): read the stage twiddles from the global table instead
+// of a shared-memory copy (the launch shape's choice).
+template <class Ar, int SRC, bool TWG>
 __global__ void __launch_bounds__(Ar::kColMaxThreads, Ar::kColMinBlocks) k_column(const __grid_constant__ PassParams<Ar> P) {
     extern __shared__ __align__(16) unsigned char smem[];
     using C = CxR<Ar>;
@@ -295,7 +296,7 @@ __global__ void __launch_bounds__(Ar::kColMaxThreads, Ar::kColMinBlocks) k_colum
     const C* src = P.src + slot * P.stride;
     C* dst = P.dst + slot * P.stride;
     const TaskSource ts = SRC == kSrcSignal ? task_source(P.work, task, 2LL * N1 * N2) : TaskSource{};
-    const CxW<Ar>* tws = stage_twiddles<Ar>(P.sp, P.tw_stage, twiddle_smem<Ar>(rest));
+    const auto tws = stage_twiddles<Ar, TWG || !Ar::kWide>(P.sp, P.tw_stage, twiddle_smem<Ar>(rest));
     for (int e0 = threadIdx.x; e0 < total; e0 += kLoadBatch<Ar> * blockDim.x) {
         C v[kLoadBatch<Ar>];
 #pragma unroll
@@ -342,7 +343,7 @@ __device__ __forceinline__ void row_unit(const SubPlan& sp, int N1, int N2, int 
     const FastDiv dF = fast_div(F), dN2 = fast_div(N2);
     Planes<Ar> A, B;
     unsigned char* rest = carve<Ar>(smem, total, A, B);
-    const CxW<Ar>* tws = stage_twiddles<Ar>(sp, tw_stage, twiddle_smem<Ar>(rest));
+    const auto tws = stage_twiddles<Ar>(sp, tw_stage, twiddle_smem<Ar>(rest));
     for (int e0 = threadIdx.x; e0 < total; e0 += kLoadBatch<Ar> * blockDim.x) {
         C v[kLoadBatch<Ar>];
 #pragma unroll
@@ -376,7 +377,7 @@ __device__ __forceinline__ void row_unit(const SubPlan& sp, int N1, int N2, int 
 }
 
 // The per-plan grid kernel: row_unit's loop with the plan read straight from the parameters (see k_column).
-template <class Ar, int DST>
+template <class Ar, int DST, bool TWG>
 __global__ void __launch_bounds__(Ar::kMaxThreads, Ar::kMinBlocks) k_row(const __grid_constant__ PassParams<Ar> P) {
     extern __shared__ __align__(16) unsigned char smem[];
     using C = CxR<Ar>;
@@ -387,7 +388,7 @@ __global__ void __launch_bounds__(Ar::kMaxThreads, Ar::kMinBlocks) k_row(const _
     const long long task = P.task0 + blockIdx.y;
     const int r0 = blockIdx.x * F;
     const C* src = P.src + blockIdx.y * P.stride;
-    const CxW<Ar>* tws = stage_twiddles<Ar>(P.sp, P.tw_stage, twiddle_smem<Ar>(rest));
+    const auto tws = stage_twiddles<Ar, TWG || !Ar::kWide>(P.sp, P.tw_stage, twiddle_smem<Ar>(rest));
     for (int e0 = threadIdx.x; e0 < total; e0 += kLoadBatch<Ar> * blockDim.x) {
         C v[kLoadBatch<Ar>];
 #pragma unroll
@@ -432,7 +433,7 @@ __global__ void __launch_bounds__(Ar::kMaxThreads, Ar::kMinBlocks) k_direct(cons
     const long long task = P.task0 + blockIdx.y;
     const C* src = P.src + blockIdx.y * P.stride;
     const TaskSource ts = SRC == kSrcSignal ? task_source(P.work, task, 2LL * n) : TaskSource{};
-    const CxW<Ar>* tws = stage_twiddles<Ar>(P.sp, P.tw_stage, twiddle_smem<Ar>(rest));
+    const auto tws = stage_twiddles<Ar>(P.sp, P.tw_stage, twiddle_smem<Ar>(rest));
     for (int i = threadIdx.x; i < n; i += blockDim.x) A.st(i, load_input<Ar, SRC>(P, ts, src, i));
     __syncthreads();
     const Planes<Ar> res = stockham<Ar>(P.sp, A, B, 1, tws, P.odd);
@@ -1251,6 +1252,7 @@ constexpr int kThreadsF64 = 128;
 struct Shape {
     int F, T;
     size_t smem;
+    bool twg = false;  // double-double / extended: stage twiddles read from global memory, not staged in shared
 };
 
 int max_bfly(const SubPlan& sp) {
@@ -1265,7 +1267,8 @@ int env_int(const char* name, int dflt);
 // block also holds the sub-FFT's twiddles in double-double.
 Shape pick_shape(const SubPlan& sp, int count, size_t esize, int fmax, int maxT) {
     const size_t budget = (size_t)env_int("KBSRC_GPU_SMEM_KB", 100) * 1024;
-    const size_t tw = esize == 32 ? (size_t)sp.twn * esize : 0;
+    const bool twg = esize == 32 && env_int("KBSRC_GPU_TW_GLOBAL", 0) != 0;
+    const size_t tw = esize == 32 && !twg ? (size_t)sp.twn * esize : 0;
     int F = 1;
     for (int f = fmax; f >= 1; f--) {
         if (2 * (size_t)sp.n * f * esize + tw > budget) continue;
@@ -1274,7 +1277,7 @@ Shape pick_shape(const SubPlan& sp, int count, size_t esize, int fmax, int maxT)
     }
     int T = ((max_bfly(sp) * F + 31) / 32) * 32;
     T = std::max(64, std::min(std::min(env_int("KBSRC_GPU_THREADS", maxT), maxT), T));
-    return Shape{F, T, 2 * (size_t)sp.n * F * esize + tw};
+    return Shape{F, T, 2 * (size_t)sp.n * F * esize + tw, twg};
 }
 
 Shape direct_shape(const SubPlan& sp, size_t esize) {
@@ -1708,17 +1711,24 @@ int allow_large_smem() {
         KB_CUDA(cudaFuncSetAttribute((const void*)(k), cudaFuncAttributeMaxDynamicSharedMemorySize,          \
                                      mx - (int)ka.sharedSizeBytes));                                        \
     } while (0)
-    KB_SMEM((k_column<ArF64, kSrcSignal>));
-    KB_SMEM((k_column<ArF64, kSrcComplex>));
-    KB_SMEM((k_column<ArDDShort, kSrcSignal>));
-    KB_SMEM((k_column<ArDDShort, kSrcComplex>));
-    KB_SMEM((k_column<ArDDAccurate, kSrcDDReal>));
-    KB_SMEM((k_column<ArDDAccurate, kSrcComplex>));
-    KB_SMEM((k_row<ArF64, kDstComplex>));
-    KB_SMEM((k_row<ArF64, kDstOutput>));
-    KB_SMEM((k_row<ArDDShort, kDstComplex>));
-    KB_SMEM((k_row<ArDDShort, kDstOutput>));
-    KB_SMEM((k_row<ArDDAccurate, kDstComplex>));
+    KB_SMEM((k_column<ArF64, kSrcSignal, false>));
+    KB_SMEM((k_column<ArF64, kSrcComplex, false>));
+    KB_SMEM((k_column<ArDDShort, kSrcSignal, false>));
+    KB_SMEM((k_column<ArDDShort, kSrcSignal, true>));
+    KB_SMEM((k_column<ArDDShort, kSrcComplex, false>));
+    KB_SMEM((k_column<ArDDShort, kSrcComplex, true>));
+    KB_SMEM((k_column<ArDDAccurate, kSrcDDReal, false>));
+    KB_SMEM((k_column<ArDDAccurate, kSrcDDReal, true>));
+    KB_SMEM((k_column<ArDDAccurate, kSrcComplex, false>));
+    KB_SMEM((k_column<ArDDAccurate, kSrcComplex, true>));
+    KB_SMEM((k_row<ArF64, kDstComplex, false>));
+    KB_SMEM((k_row<ArF64, kDstOutput, false>));
+    KB_SMEM((k_row<ArDDShort, kDstComplex, false>));
+    KB_SMEM((k_row<ArDDShort, kDstComplex, true>));
+    KB_SMEM((k_row<ArDDShort, kDstOutput, false>));
+    KB_SMEM((k_row<ArDDShort, kDstOutput, true>));
+    KB_SMEM((k_row<ArDDAccurate, kDstComplex, false>));
+    KB_SMEM((k_row<ArDDAccurate, kDstComplex, true>));
     KB_SMEM((k_direct<ArF64, kSrcSignal, kDstComplex>));
     KB_SMEM((k_direct<ArF64, kSrcComplex, kDstComplex>));
     KB_SMEM((k_direct<ArF64, kSrcComplex, kDstOutput>));
@@ -1726,10 +1736,14 @@ int allow_large_smem() {
     KB_SMEM((k_direct<ArDDAccurate, kSrcComplex, kDstComplex>));
     KB_SMEM((k_direct<ArDDAccurate, kSrcComplex, kDstOutput>));
     KB_SMEM((k_direct<ArDDAccurate, kSrcDDReal, kDstComplex>));
-    KB_SMEM((k_column<ArX80, kSrcSignal>));
-    KB_SMEM((k_column<ArX80, kSrcComplex>));
-    KB_SMEM((k_row<ArX80, kDstComplex>));
-    KB_SMEM((k_row<ArX80, kDstOutput>));
+    KB_SMEM((k_column<ArX80, kSrcSignal, false>));
+    KB_SMEM((k_column<ArX80, kSrcSignal, true>));
+    KB_SMEM((k_column<ArX80, kSrcComplex, false>));
+    KB_SMEM((k_column<ArX80, kSrcComplex, true>));
+    KB_SMEM((k_row<ArX80, kDstComplex, false>));
+    KB_SMEM((k_row<ArX80, kDstComplex, true>));
+    KB_SMEM((k_row<ArX80, kDstOutput, false>));
+    KB_SMEM((k_row<ArX80, kDstOutput, true>));
     KB_SMEM((k_direct<ArX80, kSrcSignal, kDstComplex>));
     KB_SMEM((k_direct<ArX80, kSrcComplex, kDstComplex>));
     KB_SMEM((k_direct<ArX80, kSrcComplex, kDstOutput>));
@@ -1831,11 +1845,22 @@ int launch_smooth(const DevCfft& c, const Slots& sl, void* x, void* y, cudaStrea
         PassParams<ArL> p = pass_params<ArL>(sl, c, x, x);
         p.sp = h.s1; p.N1 = h.N1; p.N2 = h.N2; p.F = c.col.F;
         const unsigned groups = (unsigned)((h.N2 + p.F - 1) / p.F);
-        k_column<ArL, SRC><<<SRC == kSrcSignal ? dim3((unsigned)sl.nt, groups) : dim3(groups, (unsigned)sl.nt), c.col.T,
-                             c.col.smem, st>>>(p);
+        const dim3 gc = SRC == kSrcSignal ? dim3((unsigned)sl.nt, groups) : dim3(groups, (unsigned)sl.nt);
+        if constexpr (ArL::kWide) {
+            if (c.col.twg) k_column<ArL, SRC, true><<<gc, c.col.T, c.col.smem, st>>>(p);
+            else k_column<ArL, SRC, false><<<gc, c.col.T, c.col.smem, st>>>(p);
+        } else {
+            k_column<ArL, SRC, false><<<gc, c.col.T, c.col.smem, st>>>(p);
+        }
         if ((rc = tr.mark(st, kA)) != KBSRC_GPU_OK) return rc;
         p.sp = h.s2; p.F = c.row.F; p.src = static_cast<CxR<ArL>*>(x); p.dst = static_cast<CxR<ArL>*>(y);
-        k_row<ArL, DST><<<dim3((h.N1 + p.F - 1) / p.F, sl.nt), c.row.T, c.row.smem, st>>>(p);
+        const dim3 gr((h.N1 + p.F - 1) / p.F, sl.nt);
+        if constexpr (ArL::kWide) {
+            if (c.row.twg) k_row<ArL, DST, true><<<gr, c.row.T, c.row.smem, st>>>(p);
+            else k_row<ArL, DST, false><<<gr, c.row.T, c.row.smem, st>>>(p);
+        } else {
+            k_row<ArL, DST, false><<<gr, c.row.T, c.row.smem, st>>>(p);
+        }
         return tr.mark(st, kB);
     }
     PassParams<ArS> p = pass_params<ArS>(sl, c, x, y);
@@ -3382,11 +3407,13 @@ int kbsrc_gpu_engine_tune(kbsrc_gpu_engine* e, const double* d_in, const double*
         for (int p = 0; p < 4; p++) {
             if (!pass[p]) continue;
             const size_t tw = esize == 32 ? (size_t)sub[p]->twn * esize : 0;
-            for (int F : {1, 2, 3, 4, 5, 6, 8, 10, 12, 16}) {
-                const size_t sm = 2 * (size_t)sub[p]->n * F * esize + tw;
-                if (F > count[p] || sm > (size_t)smem_max) continue;
-                for (int T = 64; T <= maxT[p]; T += 32) cand[p].push_back(Shape{F, T, sm});
-            }
+            for (int F : {1, 2, 3, 4, 5, 6, 8, 10, 12, 16})
+                for (bool twg : {false, true}) {  // wide types: stage twiddles in shared memory, or read them
+                    if (twg && esize != 32) continue;
+                    const size_t sm = 2 * (size_t)sub[p]->n * F * esize + (twg ? 0 : tw);
+                    if (F > count[p] || sm > (size_t)smem_max) continue;
+                    for (int T = 64; T <= maxT[p]; T += 32) cand[p].push_back(Shape{F, T, sm, twg});
+                }
             cand[p].push_back(*pass[p]);  // the default stays a candidate
         }
         size_t rounds = 0;
@@ -3432,6 +3459,17 @@ int kbsrc_gpu_engine_tune(kbsrc_gpu_engine* e, const double* d_in, const double*
     } catch (const std::exception& x) {
         return fail(KBSRC_GPU_E_CUDA, x.what());
     }
+}
+
+int kbsrc_gpu_engine_staging(const kbsrc_gpu_engine* e, int* staged) {
+    if (!e || !staged) return fail(KBSRC_GPU_E_ARG, "null engine or output");
+    const DevCfft* c[2] = {&e->fw, &e->iv};
+    for (int i = 0; i < 2; i++) {
+        const bool four = !e->split && !c[i]->m && c[i]->host.four, wide = e->esize() == 32;
+        staged[2 * i] = four ? (wide && !c[i]->col.twg ? 1 : 0) : -1;
+        staged[2 * i + 1] = four ? (wide && !c[i]->row.twg ? 1 : 0) : -1;
+    }
+    return KBSRC_GPU_OK;
 }
 
 int kbsrc_gpu_engine_run_host(kbsrc_gpu_engine* e, const double* in, const double* head, const double* tail,
@@ -3775,9 +3813,12 @@ int kbsrc_gpu_kernel_spectrum_static(const double* d_taps, int L, int n, double 
             p.sp = c.s1; p.N1 = c.N1; p.N2 = c.N2; p.F = sc.F;
             p.tw4 = reinterpret_cast<const CxW<ArDDAccurate>*>(base + off_t4);
             p.src = A; p.dst = A;
-            k_column<ArDDAccurate, kSrcDDReal><<<dim3((c.N2 + sc.F - 1) / sc.F, 1), sc.T, sc.smem, st>>>(p);
+            const dim3 gc((c.N2 + sc.F - 1) / sc.F, 1), gr((c.N1 + sr.F - 1) / sr.F, 1);
+            if (sc.twg) k_column<ArDDAccurate, kSrcDDReal, true><<<gc, sc.T, sc.smem, st>>>(p);
+            else k_column<ArDDAccurate, kSrcDDReal, false><<<gc, sc.T, sc.smem, st>>>(p);
             p.sp = c.s2; p.F = sr.F; p.src = A; p.dst = B;
-            k_row<ArDDAccurate, kDstComplex><<<dim3((c.N1 + sr.F - 1) / sr.F, 1), sr.T, sr.smem, st>>>(p);
+            if (sr.twg) k_row<ArDDAccurate, kDstComplex, true><<<gr, sr.T, sr.smem, st>>>(p);
+            else k_row<ArDDAccurate, kDstComplex, false><<<gr, sr.T, sr.smem, st>>>(p);
         } else {
             const Shape sd = direct_shape(c.sd, esize);
             p.sp = c.sd; p.F = 1; p.dst = B;

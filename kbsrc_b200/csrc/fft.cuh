@@ -65,13 +65,19 @@ __device__ __forceinline__ cx<x80> ld_tw<x80>(const cx<x80>* p) {
     return cx<x80>{x80{(unsigned long long)a.x, (int)a.y, 0}, x80{(unsigned long long)b.x, (int)b.y, 0}};
 }
 
-// Stage twiddles are read from shared memory (double-double and extended: staged once per CTA) or straight from
-// the global table through the read-only path (f64: a CTA's work is too short to amortise the copy).
-template <class Ar>
-__device__ __forceinline__ CxW<Ar> tw_at(const CxW<Ar>* p) {
-    if constexpr (Ar::kWide) return *p;
-    else return ld_tw(p);
-}
+// A pass's stage twiddles: entry i is table entry sp.tw0 + i, read from the CTA's shared-memory copy (double-double
+// and extended by default: copied once per CTA) or, with GLOBAL, straight from the global table through the
+// read-only path (float64 always: a CTA's work is too short to amortise the copy; the wide types when the launch
+// shape says so, which leaves the shared memory to the sequences). A compile-time choice, so neither form pays for
+// the other.
+template <class Ar, bool GLOBAL = !Ar::kWide>
+struct Twiddles {
+    const CxW<Ar>* p;  // GLOBAL: the table at entry sp.tw0; else the shared copy
+    __device__ __forceinline__ CxW<Ar> at(int i) const {
+        if constexpr (GLOBAL) return ld_tw(p + i);
+        else return p[i];
+    }
+};
 
 // Shared-memory view of F sequences in split planes: element i = j*F + f (sample j of sequence f) has its real
 // part at re[i] and its imaginary part at im[i], so consecutive threads (consecutive f) read consecutive
@@ -97,17 +103,17 @@ __device__ __forceinline__ unsigned char* carve(unsigned char* smem, int nF, Pla
     return reinterpret_cast<unsigned char*>(p + 4 * nF);
 }
 
-template <class Ar>
+template <class Ar, class TW>
 __device__ __forceinline__ void bfly2(const Planes<Ar>& a, int ia, int sin, const Planes<Ar>& b, int ib, int sout,
-                                      const CxW<Ar>* tw, bool p0) {
+                                      const TW& tw, int tk, bool p0) {
     const CxR<Ar> a0 = a.ld(ia), a1 = a.ld(ia + sin);
     b.st(ib, c_add<Ar>(a0, a1));
-    b.st(ib + sout, p0 ? c_sub<Ar>(a0, a1) : c_mulw<Ar>(c_sub<Ar>(a0, a1), tw_at<Ar>(tw)));
+    b.st(ib + sout, p0 ? c_sub<Ar>(a0, a1) : c_mulw<Ar>(c_sub<Ar>(a0, a1), tw.at(tk)));
 }
 
-template <class Ar>
+template <class Ar, class TW>
 __device__ __forceinline__ void bfly4(const Planes<Ar>& a, int ia, int sin, const Planes<Ar>& b, int ib, int sout,
-                                      const CxW<Ar>* tw, bool p0) {
+                                      const TW& tw, int tk, bool p0) {
     using C = CxR<Ar>;
     const C a0 = a.ld(ia), a1 = a.ld(ia + sin), a2 = a.ld(ia + 2 * sin), a3 = a.ld(ia + 3 * sin);
     const C t0 = c_add<Ar>(a0, a2), t1 = c_sub<Ar>(a0, a2), t2 = c_add<Ar>(a1, a3);
@@ -118,17 +124,17 @@ __device__ __forceinline__ void bfly4(const Planes<Ar>& a, int ia, int sin, cons
         b.st(ib + 2 * sout, c_sub<Ar>(t0, t2));
         b.st(ib + 3 * sout, c_sub<Ar>(t1, t3));
     } else {
-        b.st(ib + sout, c_mulw<Ar>(c_add<Ar>(t1, t3), tw_at<Ar>(tw)));
-        b.st(ib + 2 * sout, c_mulw<Ar>(c_sub<Ar>(t0, t2), tw_at<Ar>(tw + 1)));
-        b.st(ib + 3 * sout, c_mulw<Ar>(c_sub<Ar>(t1, t3), tw_at<Ar>(tw + 2)));
+        b.st(ib + sout, c_mulw<Ar>(c_add<Ar>(t1, t3), tw.at(tk)));
+        b.st(ib + 2 * sout, c_mulw<Ar>(c_sub<Ar>(t0, t2), tw.at(tk + 1)));
+        b.st(ib + 3 * sout, c_mulw<Ar>(c_sub<Ar>(t1, t3), tw.at(tk + 2)));
     }
 }
 
 // Odd radix R: x_u = a0 + sum_t S_t cos(2pi tu/R) -/+ i sum_t D_t sin(2pi tu/R) (fft.hpp:62-84)
-template <class Ar, int R>
+template <class Ar, int R, class TW>
 __device__ __forceinline__ void bfly_odd(const Planes<Ar>& a, int ia, int sin, const Planes<Ar>& b, int ib,
-                                         int sout, const CxW<Ar>* tw, bool p0, const typename Ar::W* cr,
-                                         const typename Ar::W* sr) {
+                                         int sout, const TW& tw, int tk, bool p0,
+                                         const typename Ar::W* cr, const typename Ar::W* sr) {
     using C = CxR<Ar>;
     constexpr int H = (R - 1) / 2;
     const C a0 = a.ld(ia);
@@ -159,46 +165,46 @@ __device__ __forceinline__ void bfly_odd(const Planes<Ar>& a, int ia, int sin, c
             b.st(ib + u * sout, xu);
             b.st(ib + (R - u) * sout, xr);
         } else {
-            b.st(ib + u * sout, c_mulw<Ar>(xu, tw_at<Ar>(tw + u - 1)));
-            b.st(ib + (R - u) * sout, c_mulw<Ar>(xr, tw_at<Ar>(tw + R - u - 1)));
+            b.st(ib + u * sout, c_mulw<Ar>(xu, tw.at(tk + u - 1)));
+            b.st(ib + (R - u) * sout, c_mulw<Ar>(xr, tw.at(tk + R - u - 1)));
         }
     }
 }
 
-// Twiddles a pass reads: for the wide types, the plan's stage twiddles copied to shared memory (tws, sp.twn
-// entries; the caller synchronises before use); for f64, the global table itself.
-template <class Ar>
-__device__ __forceinline__ const CxW<Ar>* stage_twiddles(const SubPlan& sp, const CxW<Ar>* __restrict__ tw,
-                                                         CxW<Ar>* tws) {
-    if constexpr (!Ar::kWide) {
-        return tw + sp.tw0;
+// Twiddles a pass reads: for the wide types unless GLOBAL, the plan's stage twiddles copied to shared memory (tws,
+// sp.twn entries; the caller synchronises before use); otherwise the global table itself.
+template <class Ar, bool GLOBAL = !Ar::kWide>
+__device__ __forceinline__ Twiddles<Ar, GLOBAL> stage_twiddles(const SubPlan& sp, const CxW<Ar>* __restrict__ tw,
+                                                               CxW<Ar>* tws) {
+    if constexpr (GLOBAL) {
+        return Twiddles<Ar, GLOBAL>{tw + sp.tw0};
     } else {
         for (int i = threadIdx.x; i < sp.twn; i += blockDim.x) tws[i] = ld_tw(tw + sp.tw0 + i);
-        return tws;
+        return Twiddles<Ar, GLOBAL>{tws};
     }
 }
 
 // Runs every stage of `sp` on F sequences held in `a` (element j of sequence f at j*F + f); `b` is the other
 // plane pair; `tws` the plan's twiddles from stage_twiddles (entry 0 = table entry sp.tw0). Returns the planes
 // that hold the result. Ends with the CTA synchronised.
-template <class Ar>
+template <class Ar, class TW>
 __device__ __forceinline__ Planes<Ar> stockham(const SubPlan& sp, Planes<Ar> a, Planes<Ar> b, int F,
-                                               const CxW<Ar>* tws, const OddRoots<typename Ar::W>& odd) {
+                                               const TW& tws, const OddRoots<typename Ar::W>& odd) {
     for (int g = 0; g < sp.nst; g++) {
         const int r = sp.st[g].r, m = sp.st[g].m, s = sp.st[g].s;
-        const CxW<Ar>* twg = tws + (sp.st[g].tw - sp.tw0);
+        const int twg = sp.st[g].tw - sp.tw0;
         const int total = m * s * F, sin = s * m * F, sout = s * F;
         const FastDiv dF = fast_div(F), ds = fast_div(s);
         for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
             const int bf = (int)fdiv(idx, dF), f = idx - bf * F, p = (int)fdiv(bf, ds), q = bf - p * s;
             const int ia = (s * p + q) * F + f, ib = (s * r * p + q) * F + f;
-            const CxW<Ar>* t = twg + p * (r - 1);
+            const int t = twg + p * (r - 1);
             const bool p0 = p == 0;
-            if (r == 4) bfly4<Ar>(a, ia, sin, b, ib, sout, t, p0);
-            else if (r == 2) bfly2<Ar>(a, ia, sin, b, ib, sout, t, p0);
-            else if (r == 3) bfly_odd<Ar, 3>(a, ia, sin, b, ib, sout, t, p0, odd.c[0], odd.s[0]);
-            else if (r == 5) bfly_odd<Ar, 5>(a, ia, sin, b, ib, sout, t, p0, odd.c[1], odd.s[1]);
-            else bfly_odd<Ar, 7>(a, ia, sin, b, ib, sout, t, p0, odd.c[2], odd.s[2]);
+            if (r == 4) bfly4<Ar, TW>(a, ia, sin, b, ib, sout, tws, t, p0);
+            else if (r == 2) bfly2<Ar, TW>(a, ia, sin, b, ib, sout, tws, t, p0);
+            else if (r == 3) bfly_odd<Ar, 3, TW>(a, ia, sin, b, ib, sout, tws, t, p0, odd.c[0], odd.s[0]);
+            else if (r == 5) bfly_odd<Ar, 5, TW>(a, ia, sin, b, ib, sout, tws, t, p0, odd.c[1], odd.s[1]);
+            else bfly_odd<Ar, 7, TW>(a, ia, sin, b, ib, sout, tws, t, p0, odd.c[2], odd.s[2]);
         }
         __syncthreads();
         const Planes<Ar> t = a;

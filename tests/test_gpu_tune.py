@@ -32,3 +32,21 @@ def test_tuned_engine_keeps_reference_bytes(golden, name):
     assert hashlib.sha256(y.astype("<f8").tobytes()).hexdigest() == golden[name]["sha256"]
     z = cv.run(x)  # the host path with the tuned shapes
     assert hashlib.sha256(z.astype("<f8").tobytes()).hexdigest() == golden[name]["sha256"]
+
+
+@pytest.mark.parametrize("name", ["c1_96k_44k1_exact", "s_44k1_48k_exact_30000", "c1_96k_44k1_ld"])
+def test_twiddles_from_global_memory_keep_reference_bytes(golden, monkeypatch, name):
+    """KBSRC_GPU_TW_GLOBAL=1: the double-double and extended passes read their stage twiddles from the global table
+    instead of a shared-memory copy (a choice the autotuner also makes per pass); the bytes do not change."""
+    if name not in CASES:
+        pytest.skip(f"no case {name}")
+    recipe, fi, fo, opts = CASES[name]
+    monkeypatch.setenv("KBSRC_GPU_TW_GLOBAL", "1")
+    x = make_input(recipe)
+    cv = kbsrc_b200.Conversion(x, fi, fo, mode=opts.get("mode", "exact"))
+    try:
+        assert cv.staging() and not any(cv.staging().values())
+        y = cv.run(x)
+    finally:
+        cv.close()
+    assert hashlib.sha256(y.astype("<f8").tobytes()).hexdigest() == golden[name]["sha256"]
