@@ -160,7 +160,8 @@ int kbsrc_gpu_engine_tune(kbsrc_gpu_engine* e, const double* d_in, const double*
 /* Where the four four-step passes (forward column and row, inverse column and row) read their stage twiddles:
  * 4 ints out, 1 = a copy in each CTA's shared memory, 0 = the global table through the read-only cache, -1 = not a
  * four-step pass. Float64 passes always read the global table; the double-double and extended passes stage by
- * default (KBSRC_GPU_TW_GLOBAL=1 reads the table) and the autotuner chooses per pass. The bytes do not depend on it.
+ * default unless a CTA holds a single sequence (KBSRC_GPU_TW_GLOBAL=1 reads the table in every pass, =0 stages in
+ * every pass), and the autotuner chooses per pass. The bytes do not depend on it.
  * Not in the reference (its engines run on the CPU). */
 int kbsrc_gpu_engine_staging(const kbsrc_gpu_engine* e, int* staged);
 

@@ -1264,16 +1264,24 @@ int max_bfly(const SubPlan& sp) {
 int env_int(const char* name, int dflt);
 
 // F sequences per CTA (a divisor of `count` when one fits) and T threads, within a shared-memory budget; the
-// block also holds the sub-FFT's twiddles in double-double.
+// block also holds the sub-FFT's twiddles in double-double, except where it holds a single sequence: those read
+// the global table instead (a copy made for one sequence costs about a fifth of the CTA's shared memory for little
+// reuse; the autotuner's choice on C5's 960- and 1008-point forward passes, 4.43 -> 3.96 and 4.04 -> 3.50 ms per
+// wave). KBSRC_GPU_TW_GLOBAL=1 reads the table in every wide pass, =0 stages in every one.
 Shape pick_shape(const SubPlan& sp, int count, size_t esize, int fmax, int maxT) {
     const size_t budget = (size_t)env_int("KBSRC_GPU_SMEM_KB", 100) * 1024;
-    const bool twg = esize == 32 && env_int("KBSRC_GPU_TW_GLOBAL", 0) != 0;
-    const size_t tw = esize == 32 && !twg ? (size_t)sp.twn * esize : 0;
+    const int force = env_int("KBSRC_GPU_TW_GLOBAL", -1);
+    bool twg = esize == 32 && force == 1;
+    size_t tw = esize == 32 && !twg ? (size_t)sp.twn * esize : 0;
     int F = 1;
     for (int f = fmax; f >= 1; f--) {
         if (2 * (size_t)sp.n * f * esize + tw > budget) continue;
         if (F == 1) F = f;
         if (count % f == 0) { F = f; break; }
+    }
+    if (esize == 32 && F == 1 && force == -1) {
+        twg = true;
+        tw = 0;
     }
     int T = ((max_bfly(sp) * F + 31) / 32) * 32;
     T = std::max(64, std::min(std::min(env_int("KBSRC_GPU_THREADS", maxT), maxT), T));

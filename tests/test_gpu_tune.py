@@ -50,3 +50,29 @@ def test_twiddles_from_global_memory_keep_reference_bytes(golden, monkeypatch, n
     finally:
         cv.close()
     assert hashlib.sha256(y.astype("<f8").tobytes()).hexdigest() == golden[name]["sha256"]
+
+
+def test_one_sequence_ctas_read_global_twiddles(monkeypatch):
+    """With one sequence per CTA (forced here by a 60 KB shared-memory budget on 625- and 640-point sub-FFTs) the
+    double-double passes read their stage twiddles from the global table by default; the bytes equal the staged
+    form and the default shapes."""
+    x = np.random.default_rng(41).uniform(-0.5, 0.5, (10 * 192000, 1))
+    args = dict(mode="exact", length=1.0, beta=60.0)
+    want = kbsrc_b200.resample(x, 192000, 44100, **args)
+    monkeypatch.setenv("KBSRC_GPU_SMEM_KB", "60")
+    cv = kbsrc_b200.Conversion(x, 192000, 44100, **args)
+    try:
+        st = cv.staging()
+        assert st["fwd_column"] is False and st["fwd_row"] is False
+        one = cv.run(x).copy()
+    finally:
+        cv.close()
+    monkeypatch.setenv("KBSRC_GPU_TW_GLOBAL", "0")
+    cv = kbsrc_b200.Conversion(x, 192000, 44100, **args)
+    try:
+        assert cv.staging() and all(cv.staging().values())
+        staged = cv.run(x).copy()
+    finally:
+        cv.close()
+    assert one.tobytes() == want.tobytes()
+    assert staged.tobytes() == want.tobytes()
